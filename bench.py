@@ -1,0 +1,369 @@
+#!/usr/bin/env python
+"""Benchmark of the propagation hot path (object-steps/s at 70x70 gravity, mixed vs FP64).
+
+Workload (the mixed-precision configuration): 65,536 seeded synthetic objects (70% LEO, 20% MEO,
+10% GEO), 70x70 JGM3 gravity, 30 s GJ8 step with RK8 startup, epoch 2024-01-01T00:00:00 UTC.
+A bench step propagates every object through --prop-steps GJ8 steps (default 64) of a continuing
+propagation (startup runs in the warm-up). `value` is the mixed-precision throughput; the FP64
+build is measured on the same workload and reported beside it. `e2e` times the public call a user
+makes (gpop_propagate with pinned host buffers: upload, frame tables, startup, steps, download).
+
+Multi-GPU (torchrun): every rank propagates its own 65,536 objects (weak scaling, no collective on
+the data path); the time is the max over ranks.
+
+--impl reference times the CPU FP64 restatement of the reference method (the oracle port; the
+reference has no CPU implementation of this path) on the host cores, on a bounded sample.
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_OBJECTS = 65536
+H = 30.0
+DEGREE = 70
+START = (2024, 1, 1, 0, 0, 0.0)
+SEED = 20240101
+
+# Algorithmic work (FMA = 2 flops): gravity evaluation W(L) = 24 T(L) + 15 L + 60, T(L) the number
+# of (n, m) terms with 2 <= n <= L; an object-step is 7 distinct evaluations plus ~500 flops of
+# GJ8 predictor/corrector arithmetic.
+def terms(L):
+    return (L + 1) * (L + 2) // 2 - 3
+
+
+def flops_per_object_step(L=DEGREE):
+    return 7 * (24 * terms(L) + 15 * L + 60) + 500
+
+
+def fp32_flops_per_object_step(L=DEGREE):
+    # the mixed build runs the degree > 8 terms in FP32
+    return 7 * 24 * (terms(L) - terms(8))
+
+
+def env_int(k, d):
+    try:
+        return int(os.environ.get(k, d))
+    except ValueError:
+        return d
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax = float(p[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, p[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def cpu_baseline(seconds_target=15.0):
+    """Oracle (CPU FP64 restatement of the reference method, OpenMP over objects) on a bounded
+    sample of the same workload; returns object-steps/s and a description."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_api as O
+    from opengpop_b200 import orbits
+    data = O.Data(degree=DEGREE)
+    cores = cpu_cores()
+    n = max(32, 8 * cores)
+    r0, v0 = orbits.mixed_population(N_OBJECTS, SEED)
+    r0, v0 = r0[:n], v0[:n]
+    # calibrate: two lengths, so the startup cost cancels out of the per-step rate
+    t0 = time.perf_counter()
+    O.propagate(data, "gravity", START, H, 8, r0, v0, threads=cores)
+    t8 = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    O.propagate(data, "gravity", START, H, 40, r0, v0, threads=cores)
+    t40 = time.perf_counter() - t0
+    per_step = max((t40 - t8) / 32.0, 1e-6)
+    steps = int(min(4000, max(40, seconds_target / per_step)))
+    t0 = time.perf_counter()
+    O.propagate(data, "gravity", START, H, steps, r0, v0, threads=cores)
+    dt = time.perf_counter() - t0
+    rate = n * steps / dt
+    return rate, cores, ("%d of the %d objects x %d steps (30 s, 70x70, startup included), "
+                         "%.1f s of CPU work" % (n, N_OBJECTS, steps, dt))
+
+
+def run_reference(args):
+    rank = env_int("RANK", 0)
+    if rank != 0:
+        return 0
+    rates = []
+    cores = cpu_cores()
+    desc = ""
+    for i in range(args.warmup + args.steps):
+        rate, cores, desc = cpu_baseline(seconds_target=max(2.0, 30.0 / (args.steps + args.warmup)))
+        if i >= args.warmup:
+            rates.append(rate)
+    value = float(np.mean(rates)) if rates else 0.0
+    line = {
+        "impl": "reference", "metric": "object-steps/s @70x70", "value": value,
+        "unit": "object-steps/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "65,536 objects (70% LEO / 20% MEO / 10% GEO), 70x70, 30 s step",
+                   "sample": desc},
+        "cpu_baseline": {"value": value, "unit": "object-steps/s", "cores": cores, "kind": "port",
+                         "sample": desc},
+        "e2e": {"value": value, "unit": "object-steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def probe_peak(torch, fp64, dev):
+    """Measured FMA throughput (TFLOP/s) of this GPU: independent FMA chains on every SM."""
+    lib = C.CDLL(os.path.join(ROOT, "opengpop_b200", "lib", "libgpop_probe.so"))
+    lib.gpop_probe_fma.restype = C.c_int
+    lib.gpop_probe_fma.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
+                                   C.POINTER(C.c_double)]
+    scratch = torch.zeros(16, dtype=torch.float64, device=dev)
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    stream = torch.cuda.current_stream()
+    flops = C.c_double()
+    best = 0.0
+    for it in range(4):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        rc = lib.gpop_probe_fma(int(fp64), sms * 8, 2000, C.c_void_p(scratch.data_ptr()),
+                                C.c_void_p(stream.cuda_stream), C.byref(flops))
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if rc != 0:
+            return None
+        if it:
+            best = max(best, flops.value / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+    return best
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--prop-steps", type=int, default=64, help="GJ8 steps per bench step")
+    ap.add_argument("--objects", type=int, default=N_OBJECTS)
+    ap.add_argument("--e2e-steps", type=int, default=960, help="GJ8 steps per e2e call")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import torch.distributed as dist
+    import opengpop_b200 as G
+    from opengpop_b200 import orbits
+
+    rank = env_int("RANK", 0)
+    world = env_int("WORLD_SIZE", 1)
+    local = env_int("LOCAL_RANK", 0)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=dev)
+    n = args.objects
+    r0, v0 = orbits.mixed_population(n, SEED + rank)
+    total_steps = (args.warmup + args.steps) * args.prop_steps + 1
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def run(precision):
+        ctx = G.Context(device=local, precision=precision)
+        r = torch.tensor(r0, dtype=torch.float64, device=dev)
+        v = torch.tensor(v0, dtype=torch.float64, device=dev)
+        prop = ctx.propagator(START, H, total_steps, r, v)
+        stream = torch.cuda.current_stream()
+        flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+        prop.step(1)  # startup (RK8 + 7 corrector passes) + step 1
+        for _ in range(args.warmup):
+            prop.step(args.prop_steps)
+        torch.cuda.synchronize()
+        barrier()
+        launches0 = ctx.kernel_launches
+        times = []
+        for _ in range(args.steps):
+            flush.fill_(1.0)  # L2 flush between timed steps (256 MB > 126 MB L2)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            prop.step(args.prop_steps)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1) * 1e-3)
+        barrier()
+        launches = ctx.kernel_launches - launches0
+        rv = float(r.abs().sum().item())
+        prop.close()
+        ctx.close()
+        return times, launches, rv
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    times_mixed, launches_mixed, chk_m = run(G.MIXED)
+    times_fp64, launches_fp64, chk_d = run(G.FP64)
+    clocks = sampler.stop()
+
+    t_mixed = max_over_ranks(sum(times_mixed))
+    t_fp64 = max_over_ranks(sum(times_fp64))
+    osteps = n * args.prop_steps * args.steps
+    value = world * osteps / t_mixed
+    value_fp64 = world * osteps / t_fp64
+
+    # ---- end to end through the public call (host pinned in/out) ----
+    ctx = G.Context(device=local, precision=G.MIXED)
+    rin = torch.tensor(r0, dtype=torch.float64).pin_memory()
+    vin = torch.tensor(v0, dtype=torch.float64).pin_memory()
+    rout = torch.empty_like(rin).pin_memory()
+    vout = torch.empty_like(vin).pin_memory()
+    rin_np, vin_np, rout_np, vout_np = (x.numpy() for x in (rin, vin, rout, vout))
+    e2e_steps = args.e2e_steps
+    ctx.propagate(START, H, e2e_steps, rin_np, vin_np)  # warm-up call
+    barrier()
+    e2e_calls = max(1, min(args.steps, 3))
+    t0 = time.perf_counter()
+    for _ in range(e2e_calls):
+        lib = G.load_library()
+        st = lib.gpop_propagate(ctx._h, C.byref(G.as_time(START)), H, e2e_steps, n,
+                                rin_np.ctypes.data_as(C.c_void_p), vin_np.ctypes.data_as(C.c_void_p),
+                                rout_np.ctypes.data_as(C.c_void_p),
+                                vout_np.ctypes.data_as(C.c_void_p))
+        ctx._check(st)
+    t_e2e = max_over_ranks(time.perf_counter() - t0)
+    e2e_value = world * n * e2e_steps * e2e_calls / t_e2e
+    ctx.close()
+
+    # ---- roofline of the dominant kernel (the mixed GJ8 kernel) ----
+    peak64 = probe_peak(torch, True, dev)
+    peak32 = probe_peak(torch, False, dev)
+    launch_t = sum(times_mixed) / max(1, launches_mixed)
+    steps_per_launch = args.prop_steps * args.steps / max(1, launches_mixed)
+    f_total = flops_per_object_step() * n * steps_per_launch
+    f32 = fp32_flops_per_object_step() * n * steps_per_launch
+    f64 = f_total - f32
+    achieved = f_total / launch_t / 1e12
+    t_min = f64 / (peak64 * 1e12) + f32 / (peak32 * 1e12) if peak64 and peak32 else None
+    eff_peak = f_total / t_min / 1e12 if t_min else None
+    fp64_launch_t = sum(times_fp64) / max(1, launches_fp64)
+    fp64_achieved = flops_per_object_step() * n * steps_per_launch / fp64_launch_t / 1e12
+
+    if rank == 0:
+        cpu = None
+        if not args.no_cpu_baseline:
+            rate, cores, desc = cpu_baseline()
+            cpu = {"value": rate, "unit": "object-steps/s", "cores": cores, "kind": "port",
+                   "sample": desc}
+        line = {
+            "metric": "object-steps/s @70x70 (mixed precision)",
+            "value": value, "unit": "object-steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * t_mixed / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32",
+            "data": "synthetic",
+            "config": {"workload": "65,536 objects (70%% LEO / 20%% MEO / 10%% GEO, seed %d), "
+                                   "70x70 JGM3, 30 s GJ8 step, %d GJ8 steps per bench step"
+                                   % (SEED, args.prop_steps),
+                       "objects_per_gpu": n, "degree": DEGREE, "step_s": H,
+                       "l2": "flushed (256 MB write) between timed steps",
+                       "parallelism": "replicas" if world == 1 else "object shards x%d" % world},
+            "fp64": {"value": value_fp64, "unit": "object-steps/s",
+                     "ms_per_step": 1e3 * t_fp64 / args.steps,
+                     "roofline": {"bound": "fp64", "achieved": fp64_achieved, "peak": peak64,
+                                  "unit": "TFLOP/s",
+                                  "frac": fp64_achieved / peak64 if peak64 else None}},
+            "mixed_vs_fp64": value / value_fp64,
+            "e2e": {"value": e2e_value, "unit": "object-steps/s",
+                    "h2d_bytes_per_step": 2 * n * 3 * 8, "d2h_bytes_per_step": 2 * n * 3 * 8,
+                    "call": "gpop_propagate, %d GJ8 steps per call incl. startup" % e2e_steps},
+            "roofline": {"bound": "fp64+fp32", "achieved": achieved, "peak": eff_peak,
+                         "unit": "TFLOP/s", "frac": achieved / eff_peak if eff_peak else None,
+                         "traffic": None,
+                         "peaks_measured": {"fp64_tflops": peak64, "fp32_tflops": peak32,
+                                            "how": "live FMA-chain probe (libgpop_probe.so)"}},
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+            "gpu_launches": launches_mixed,
+            "checksum": [chk_m, chk_d],
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

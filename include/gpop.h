@@ -1,0 +1,183 @@
+/*
+ * gpop.h -- C ABI of the B200 propagation + closest-approach library (libgpop.so).
+ *
+ * Plain C types only: host or device pointers, sizes, status codes. Every entry point names the
+ * reference interface it replaces (file:line relative to the reference project root). Device
+ * pointers are caller-owned; the context owns all scratch memory. Errors are returned as status
+ * codes (the reference calls exit()); gpop_last_error() gives the message. A context is used from
+ * one host thread at a time; distinct contexts are independent.
+ */
+#ifndef GPOP_H
+#define GPOP_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+typedef struct gpop_ctx gpop_ctx;
+typedef struct gpop_propagator gpop_propagator;
+typedef struct gpop_ca gpop_ca;
+
+typedef enum {
+    GPOP_OK = 0,
+    GPOP_ERR_INVALID_ARG = 1,
+    GPOP_ERR_CUDA = 2,
+    GPOP_ERR_DATA = 3, /* a model data file is missing or malformed */
+    GPOP_ERR_NOMEM = 4,
+    GPOP_ERR_TIMEOUT = 5, /* a bounded device wait gave up */
+    GPOP_ERR_UNSUPPORTED = 6,
+    GPOP_ERR_STATE = 7, /* call out of order (e.g. find before propagate) */
+} gpop_status;
+
+/* TimeData (lib/common/types/types/Parameters.hpp:19-22) */
+typedef struct {
+    int32_t year, month, day, hour, min;
+    double sec;
+} gpop_time;
+
+typedef enum { GPOP_FP64 = 0, GPOP_MIXED = 1 } gpop_precision;
+
+/* Reference quirks (kept by default so results match the reference build; a set bit fixes it). */
+enum {
+    GPOP_FIX_BACKWARD_RK8_EPOCH = 1u << 0, /* Q1: force_model.cu:69-71 uses (-i + c_k) h */
+    GPOP_FIX_STARTUP_EXPORT_ACC = 1u << 1, /* Q3: gpu_propagator.cu:48-53,68-72 exports column 8 */
+    GPOP_FIX_PHASE_EPOCH = 1u << 2, /* closest_approach.cu:134: each phase restarts the epoch */
+};
+
+/* Analytic force models of the reference's test suite (unit_tests/include/gpu_test_helpers.cuh) */
+typedef enum {
+    GPOP_FORCE_GRAVITY = 0,
+    GPOP_FORCE_ZERO = 1,
+    GPOP_FORCE_CONST = 2,
+    GPOP_FORCE_POLY7 = 3,
+    GPOP_FORCE_POLY8 = 4,
+    GPOP_FORCE_POLY9 = 5,
+    GPOP_FORCE_EXP = 6,
+    GPOP_FORCE_DAMPED = 7,
+} gpop_force_kind;
+
+typedef struct {
+    const char* data_dir; /* directory with JGM3.gfc, nutation, EOP and leap-second files */
+    int32_t device; /* CUDA device ordinal (the reference hard-wires 0: force_model.cu:25) */
+    int32_t gravity_degree; /* <= 0: max_degree of the gfc header (dataset_loaders.cu:245-248) */
+    int32_t n_corrections; /* corrector passes; the reference uses 7 (exec/runner.cu:36) */
+    int32_t precision; /* gpop_precision */
+    uint32_t flags; /* GPOP_FIX_* */
+} gpop_config;
+
+/* ---- context ---- */
+void gpop_config_default(gpop_config* cfg);
+/* Replaces ForceModel(...) + PreInitialize (force_model.cuh:30-40, force_model.cu:23-45):
+ * loads the data sets once and uploads the gravity table. */
+gpop_status gpop_create(const gpop_config* cfg, gpop_ctx** out);
+void gpop_destroy(gpop_ctx* ctx);
+const char* gpop_last_error(const gpop_ctx* ctx);
+const char* gpop_status_string(int32_t status);
+int32_t gpop_gravity_degree(const gpop_ctx* ctx);
+/* Number of device kernels this context has launched (monotonic). */
+int64_t gpop_kernel_launches(const gpop_ctx* ctx);
+
+/* ---- propagation ---- */
+/* exec propagate (exec/runner.cu:11-70) / GpuPropagator::Step x steps + CopyStateToHost
+ * (gpu_propagator.cu:28-84): host AoS buffers [n][3] in metres and m/s (GCRS). */
+gpop_status gpop_propagate(gpop_ctx* ctx, const gpop_time* start, double h, int32_t steps, int64_t n,
+    const double* r_in, const double* v_in, double* r_out, double* v_out);
+/* Device-pointer variant: r_dev/v_dev ([n][3] AoS) are updated in place, like the caller-owned
+ * buffers of GpuPropagator (gpu_propagator.cu:128-129). stream may be NULL (legacy default). */
+gpop_status gpop_propagate_device(gpop_ctx* ctx, const gpop_time* start, double h, int32_t steps,
+    int64_t n, double* r_dev, double* v_dev, void* stream);
+/* Same, also writing the per-step trajectory (device, [steps][3][n] SoA each; any may be NULL):
+ * positions, velocities and the acceleration the reference exports after each Step()
+ * (MoveColumnToVectorKernel, gpu_propagator/src/device/dev_functions.cu:71-82). */
+gpop_status gpop_propagate_trajectory(gpop_ctx* ctx, const gpop_time* start, double h,
+    int32_t steps, int64_t n, double* r_dev, double* v_dev, double* traj_r, double* traj_v,
+    double* traj_a, void* stream);
+/* GpuPropagator (lib/gpu_propagator/include/gpu_propagator/gpu_propagator.cuh:26-59): binds the
+ * caller-owned device buffers r_dev/v_dev ([n][3] AoS, updated in place after every step call);
+ * max_steps sizes the epoch table like the reference's maxSteps argument. */
+gpop_status gpop_propagator_create(gpop_ctx* ctx, const gpop_time* start, double h,
+    int32_t max_steps, int64_t n, double* r_dev, double* v_dev, gpop_propagator** out);
+/* GpuPropagator::Step (gpu_propagator.cu:28-77) called `steps` times: the first call runs the
+ * startup. traj_* ([steps][3][n] SoA, may be NULL) are indexed from this call's first step. */
+gpop_status gpop_propagator_step(gpop_propagator* p, int32_t steps, double* traj_r, double* traj_v,
+    double* traj_a, void* stream);
+/* Steps taken so far. */
+int32_t gpop_propagator_steps_done(const gpop_propagator* p);
+void gpop_propagator_destroy(gpop_propagator* p);
+/* Analytic test forces through the same integrator kernels (MockForceModel,
+ * unit_tests/include/mock_force_model.cuh:46-112). Times follow the mock: (idx - 4) h. */
+gpop_status gpop_propagate_analytic(gpop_ctx* ctx, int32_t kind, double h, int32_t steps,
+    int32_t n_corrections, int64_t n, double* r_dev, double* v_dev, double* traj_r, double* traj_v,
+    double* traj_a, void* stream);
+
+/* ---- startup and integrator pieces (device buffers, one object each) ---- */
+/* GpuStartup::Startup (gpu_startup.cu:55-68). Outputs 9 columns x 3 (column 4 = epoch):
+ * r27, v27, a27, s27, S27 (device). n_corrections = 0 returns the RK8 guess only. */
+gpop_status gpop_startup(gpop_ctx* ctx, int32_t kind, const gpop_time* start, double h,
+    int32_t n_corrections, const double* r0_dev, const double* v0_dev, double* r27, double* v27,
+    double* a27, double* s27, double* S27, void* stream);
+/* StartupCorrector on given matrices (gpu_startup.cu:170-294): op 0 = acceleration matrix only,
+ * 1 = + CalculateS0, 2 = + one Correct(). In place on device buffers. */
+gpop_status gpop_corrector_unit(gpop_ctx* ctx, int32_t kind, double h, int32_t op, double* r27,
+    double* v27, double* a27, double* s27, double* S27, void* stream);
+/* Predictor::Predict (prediction.cu:49-74) at `step`, in place. */
+gpop_status gpop_predict_unit(gpop_ctx* ctx, int32_t kind, double h, int32_t step, double* r3,
+    double* v3, double* a27, double* s3, double* S3, void* stream);
+/* FinalizeCorrectionKernel (gpu_propagator/src/device/dev_functions.cu:52-69), in place. */
+gpop_status gpop_finalize_correction_unit(gpop_ctx* ctx, double h, double* r3, double* v3,
+    const double* a27, const double* s3, const double* S3, void* stream);
+
+/* ---- force model ---- */
+/* GravitySource::ComputeAcceleration (gravity_source.cu:168-211): r_dev, a_dev [n][3] GCRS;
+ * frame9_dev = ITRS->GCRS column-major 3x3 (NULL = identity). precision: gpop_precision. */
+gpop_status gpop_gravity(gpop_ctx* ctx, int64_t n, const double* r_dev, const double* frame9_dev,
+    double* a_dev, int32_t precision, void* stream);
+/* FMTimePoints::CalculateParameters (time_points.cu:126-201): count ITRS->GCRS matrices
+ * (column-major, 9 each) and UTC MJDs for epochs start - before_epoch h + i h (or the RK8
+ * midpoints when use_midpoints). Device outputs; mjd_dev may be NULL. */
+gpop_status gpop_frame_matrices(gpop_ctx* ctx, const gpop_time* start, double h, int32_t count,
+    int32_t use_midpoints, int32_t before_epoch, double* m_dev, double* mjd_dev, void* stream);
+
+/* ---- closest approach (lib/closest_approach) ---- */
+/* One record per cross-set pair i < j (exec/runner.cu:96-106, ClosestApproachData::Get). */
+typedef struct {
+    uint32_t object_index1, object_index2;
+    double distance; /* m */
+    double time; /* s from the start of the first phase */
+    double position_a[3], position_b[3];
+} gpop_ca_record;
+
+/* ClosestApproach::Initialize (closest_approach.cu:47-127). set_ids: start at 0, non-decreasing by
+ * at most 1, at least two sets. Host buffers. */
+gpop_status gpop_ca_create(gpop_ctx* ctx, const gpop_time* start, double h, int64_t n,
+    const double* r_in, const double* v_in, const uint32_t* set_ids, gpop_ca** out);
+/* ClosestApproach::Propagate (closest_approach.cu:129-157): steps more steps; running minima
+ * persist across calls. */
+gpop_status gpop_ca_propagate(gpop_ca* ca, int32_t steps);
+/* ClosestApproach::FindClosest (closest_approach.cu:159-209) + the runner's record loop. Writes
+ * the records whose distance < threshold_m (threshold_m < 0: every pair, reference semantics),
+ * sorted by (object_index1, object_index2). out may be NULL to query the count. */
+gpop_status gpop_ca_find(gpop_ca* ca, double threshold_m, gpop_ca_record* out, int64_t capacity,
+    int64_t* n_out);
+/* Per-pair results in the reference's pair order (PartitionParameters map), host buffers of
+ * num_pairs entries (any may be NULL): refined distance, time, positions, closest step. */
+gpop_status gpop_ca_pairs(gpop_ca* ca, double* dist, double* time, double* pos_a, double* pos_b,
+    uint32_t* closest_step);
+int64_t gpop_ca_num_pairs(const gpop_ca* ca);
+/* Device trajectory of the propagated phases ([steps][3][n] SoA), for inspection and tests. */
+gpop_status gpop_ca_trajectory(gpop_ca* ca, double* r_host, double* v_host, double* a_host,
+    int32_t* steps_out);
+void gpop_ca_destroy(gpop_ca* ca);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+#ifdef __cplusplus
+}
+#endif
+#endif /* GPOP_H */

@@ -1,0 +1,372 @@
+"""opengpop_b200 -- B200 (sm_100a) propagation and closest-approach library.
+
+Python binding of the C ABI in include/gpop.h (libgpop.so, built in-tree into
+opengpop_b200/lib/). Device memory for the *_device calls comes from torch tensors (plumbing only);
+every computation runs in the library's own CUDA kernels. Importing works without a GPU; creating a
+Context needs the built library and a CUDA device, and fails loudly otherwise.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+PKG_DIR = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG_DIR, "lib", "libgpop.so")
+DATA_DIR = os.path.join(PKG_DIR, "data")
+
+OK = 0
+STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "model data error",
+          4: "out of memory", 5: "device wait timed out", 6: "unsupported", 7: "call out of order"}
+FP64, MIXED = 0, 1
+FIX_BACKWARD_RK8_EPOCH = 1
+FIX_STARTUP_EXPORT_ACC = 2
+FIX_PHASE_EPOCH = 4
+FORCE = {"gravity": 0, "zero": 1, "const": 2, "poly7": 3, "poly8": 4, "poly9": 5, "exp": 6,
+         "damped": 7}
+
+# Every symbol include/gpop.h declares (checked by the test suite against the built library).
+EXPORTS = (
+    "gpop_config_default", "gpop_create", "gpop_destroy", "gpop_last_error", "gpop_status_string",
+    "gpop_gravity_degree", "gpop_kernel_launches", "gpop_propagate", "gpop_propagate_device",
+    "gpop_propagate_trajectory", "gpop_propagator_create", "gpop_propagator_step",
+    "gpop_propagator_steps_done", "gpop_propagator_destroy", "gpop_propagate_analytic", "gpop_startup", "gpop_corrector_unit",
+    "gpop_predict_unit", "gpop_finalize_correction_unit", "gpop_gravity", "gpop_frame_matrices",
+    "gpop_ca_create", "gpop_ca_propagate", "gpop_ca_find", "gpop_ca_pairs", "gpop_ca_num_pairs",
+    "gpop_ca_trajectory", "gpop_ca_destroy",
+)
+
+
+class GpopError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__("%s (%d): %s" % (STATUS.get(status, "?"), status, message))
+        self.status = status
+
+
+class Time(C.Structure):
+    """TimeData of the reference (lib/common/types/types/Parameters.hpp:19-22)."""
+    _fields_ = [("year", C.c_int32), ("month", C.c_int32), ("day", C.c_int32),
+                ("hour", C.c_int32), ("min", C.c_int32), ("sec", C.c_double)]
+
+
+class Config(C.Structure):
+    _fields_ = [("data_dir", C.c_char_p), ("device", C.c_int32), ("gravity_degree", C.c_int32),
+                ("n_corrections", C.c_int32), ("precision", C.c_int32), ("flags", C.c_uint32)]
+
+
+class CaRecord(C.Structure):
+    _fields_ = [("object_index1", C.c_uint32), ("object_index2", C.c_uint32),
+                ("distance", C.c_double), ("time", C.c_double),
+                ("position_a", C.c_double * 3), ("position_b", C.c_double * 3)]
+
+
+_lib = None
+_VP = C.c_void_p
+
+
+def load_library(path=LIB_PATH):
+    """Loads libgpop.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise OSError("libgpop.so not built (%s): run __graft_entry__.build() or make -C "
+                      "opengpop_b200/csrc" % path)
+    lib = C.CDLL(path)
+    i32, i64, f64 = C.c_int32, C.c_int64, C.c_double
+    sig = {
+        "gpop_config_default": (None, [C.POINTER(Config)]),
+        "gpop_create": (i32, [C.POINTER(Config), C.POINTER(_VP)]),
+        "gpop_destroy": (None, [_VP]),
+        "gpop_last_error": (C.c_char_p, [_VP]),
+        "gpop_status_string": (C.c_char_p, [i32]),
+        "gpop_gravity_degree": (i32, [_VP]),
+        "gpop_kernel_launches": (i64, [_VP]),
+        "gpop_propagate": (i32, [_VP, C.POINTER(Time), f64, i32, i64, _VP, _VP, _VP, _VP]),
+        "gpop_propagate_device": (i32, [_VP, C.POINTER(Time), f64, i32, i64, _VP, _VP, _VP]),
+        "gpop_propagate_trajectory": (i32, [_VP, C.POINTER(Time), f64, i32, i64] + [_VP] * 6),
+        "gpop_propagator_create": (i32, [_VP, C.POINTER(Time), f64, i32, i64, _VP, _VP,
+                                         C.POINTER(_VP)]),
+        "gpop_propagator_step": (i32, [_VP, i32, _VP, _VP, _VP, _VP]),
+        "gpop_propagator_steps_done": (i32, [_VP]),
+        "gpop_propagator_destroy": (None, [_VP]),
+        "gpop_propagate_analytic": (i32, [_VP, i32, f64, i32, i32, i64] + [_VP] * 6),
+        "gpop_startup": (i32, [_VP, i32, C.POINTER(Time), f64, i32] + [_VP] * 8),
+        "gpop_corrector_unit": (i32, [_VP, i32, f64, i32] + [_VP] * 6),
+        "gpop_predict_unit": (i32, [_VP, i32, f64, i32] + [_VP] * 6),
+        "gpop_finalize_correction_unit": (i32, [_VP, f64] + [_VP] * 6),
+        "gpop_gravity": (i32, [_VP, i64, _VP, _VP, _VP, i32, _VP]),
+        "gpop_frame_matrices": (i32, [_VP, C.POINTER(Time), f64, i32, i32, i32, _VP, _VP, _VP]),
+        "gpop_ca_create": (i32, [_VP, C.POINTER(Time), f64, i64, _VP, _VP, _VP, C.POINTER(_VP)]),
+        "gpop_ca_propagate": (i32, [_VP, i32]),
+        "gpop_ca_find": (i32, [_VP, f64, _VP, i64, C.POINTER(i64)]),
+        "gpop_ca_pairs": (i32, [_VP] * 6),
+        "gpop_ca_num_pairs": (i64, [_VP]),
+        "gpop_ca_trajectory": (i32, [_VP] * 4 + [C.POINTER(i32)]),
+        "gpop_ca_destroy": (None, [_VP]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def as_time(t):
+    if isinstance(t, Time):
+        return t
+    y, mo, d, hh, mi, s = t
+    return Time(int(y), int(mo), int(d), int(hh), int(mi), float(s))
+
+
+def _host(a, shape=None):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    return a.reshape(shape) if shape is not None else a
+
+
+def _dptr(t):
+    """Device pointer of a CUDA torch tensor (or None)."""
+    if t is None:
+        return None
+    if not t.is_cuda or not t.is_contiguous():
+        raise ValueError("expected a contiguous CUDA tensor")
+    return C.c_void_p(t.data_ptr())
+
+
+def _stream_ptr(stream):
+    if stream is None:
+        import torch
+        stream = torch.cuda.current_stream()
+    return C.c_void_p(stream.cuda_stream) if hasattr(stream, "cuda_stream") else C.c_void_p(stream)
+
+
+class Context:
+    """A loaded force model and device tables (replaces ForceModel + PreInitialize)."""
+
+    def __init__(self, data_dir=DATA_DIR, device=0, gravity_degree=0, n_corrections=7,
+                 precision=FP64, flags=0):
+        lib = load_library()
+        cfg = Config()
+        lib.gpop_config_default(C.byref(cfg))
+        self._dir = data_dir.encode()
+        cfg.data_dir = self._dir
+        cfg.device = device
+        cfg.gravity_degree = gravity_degree
+        cfg.n_corrections = n_corrections
+        cfg.precision = precision
+        cfg.flags = flags
+        h = _VP()
+        st = lib.gpop_create(C.byref(cfg), C.byref(h))
+        self._h = h.value
+        if st != OK:
+            msg = lib.gpop_last_error(self._h).decode() if self._h else ""
+            if self._h:
+                lib.gpop_destroy(self._h)
+                self._h = None
+            raise GpopError(st, msg)
+        self.device = device
+        self.precision = precision
+
+    def close(self):
+        if getattr(self, "_h", None):
+            load_library().gpop_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st):
+        if st != OK:
+            raise GpopError(st, load_library().gpop_last_error(self._h).decode())
+
+    @property
+    def degree(self):
+        return load_library().gpop_gravity_degree(self._h)
+
+    @property
+    def kernel_launches(self):
+        return load_library().gpop_kernel_launches(self._h)
+
+    # ---- propagation ----
+    def propagate(self, start, h, steps, r, v):
+        """Host in, host out (exec propagate): returns (r_end, v_end) as [n, 3] arrays."""
+        r = _host(r).reshape(-1, 3)
+        v = _host(v).reshape(-1, 3)
+        ro = np.empty_like(r)
+        vo = np.empty_like(v)
+        self._check(load_library().gpop_propagate(
+            self._h, C.byref(as_time(start)), float(h), int(steps), r.shape[0],
+            r.ctypes.data_as(_VP), v.ctypes.data_as(_VP), ro.ctypes.data_as(_VP),
+            vo.ctypes.data_as(_VP)))
+        return ro, vo
+
+    def propagate_device(self, start, h, steps, r, v, stream=None):
+        """In place on CUDA tensors r, v of shape [n, 3] (float64)."""
+        self._check(load_library().gpop_propagate_device(
+            self._h, C.byref(as_time(start)), float(h), int(steps), r.shape[0], _dptr(r), _dptr(v),
+            _stream_ptr(stream)))
+
+    def propagate_trajectory(self, start, h, steps, r, v, traj_r=None, traj_v=None, traj_a=None,
+                             stream=None):
+        self._check(load_library().gpop_propagate_trajectory(
+            self._h, C.byref(as_time(start)), float(h), int(steps), r.shape[0], _dptr(r), _dptr(v),
+            _dptr(traj_r), _dptr(traj_v), _dptr(traj_a), _stream_ptr(stream)))
+
+    def propagator(self, start, h, max_steps, r, v):
+        """GpuPropagator over CUDA tensors r, v [n, 3] (updated in place by step())."""
+        return Propagator(self, start, h, max_steps, r, v)
+
+    def propagate_analytic(self, kind, h, steps, r, v, n_corrections=7, traj_r=None,
+                           traj_v=None, traj_a=None, stream=None):
+        k = FORCE[kind] if isinstance(kind, str) else kind
+        self._check(load_library().gpop_propagate_analytic(
+            self._h, k, float(h), int(steps), int(n_corrections), r.shape[0], _dptr(r), _dptr(v),
+            _dptr(traj_r), _dptr(traj_v), _dptr(traj_a), _stream_ptr(stream)))
+
+    def startup(self, kind, start, h, n_corrections, r0, v0, out):
+        """out: five CUDA tensors [27] (r, v, a, s, S)."""
+        k = FORCE[kind] if isinstance(kind, str) else kind
+        t = as_time(start if start is not None else (2000, 1, 1, 0, 0, 0.0))
+        self._check(load_library().gpop_startup(
+            self._h, k, C.byref(t), float(h), int(n_corrections), _dptr(r0), _dptr(v0),
+            *[_dptr(x) for x in out], _stream_ptr(None)))
+
+    def corrector_unit(self, kind, h, op, r27, v27, a27, s27, S27):
+        k = FORCE[kind] if isinstance(kind, str) else kind
+        self._check(load_library().gpop_corrector_unit(
+            self._h, k, float(h), int(op), _dptr(r27), _dptr(v27), _dptr(a27), _dptr(s27),
+            _dptr(S27), _stream_ptr(None)))
+
+    def predict_unit(self, kind, h, step, r3, v3, a27, s3, S3):
+        k = FORCE[kind] if isinstance(kind, str) else kind
+        self._check(load_library().gpop_predict_unit(
+            self._h, k, float(h), int(step), _dptr(r3), _dptr(v3), _dptr(a27), _dptr(s3),
+            _dptr(S3), _stream_ptr(None)))
+
+    def finalize_correction_unit(self, h, r3, v3, a27, s3, S3):
+        self._check(load_library().gpop_finalize_correction_unit(
+            self._h, float(h), _dptr(r3), _dptr(v3), _dptr(a27), _dptr(s3), _dptr(S3),
+            _stream_ptr(None)))
+
+    # ---- force model ----
+    def gravity(self, r, a, frame9=None, precision=None, stream=None):
+        p = self.precision if precision is None else precision
+        self._check(load_library().gpop_gravity(
+            self._h, r.shape[0], _dptr(r), _dptr(frame9), _dptr(a), int(p), _stream_ptr(stream)))
+
+    def frame_matrices(self, start, h, count, m_out, mjd_out=None, use_midpoints=False,
+                       before_epoch=4, stream=None):
+        self._check(load_library().gpop_frame_matrices(
+            self._h, C.byref(as_time(start)), float(h), int(count), int(use_midpoints),
+            int(before_epoch), _dptr(m_out), _dptr(mjd_out), _stream_ptr(stream)))
+
+    # ---- closest approach ----
+    def closest_approach(self, start, h, r, v, set_ids):
+        return ClosestApproach(self, start, h, r, v, set_ids)
+
+
+class Propagator:
+    """GpuPropagator of the reference (gpu_propagator.cuh:26-59): step(k) = Step() k times."""
+
+    def __init__(self, ctx, start, h, max_steps, r, v):
+        lib = load_library()
+        self.ctx = ctx
+        self._keep = (r, v)
+        out = _VP()
+        ctx._check(lib.gpop_propagator_create(ctx._h, C.byref(as_time(start)), float(h),
+                                              int(max_steps), r.shape[0], _dptr(r), _dptr(v),
+                                              C.byref(out)))
+        self._h = out.value
+
+    def step(self, steps=1, traj_r=None, traj_v=None, traj_a=None, stream=None):
+        self.ctx._check(load_library().gpop_propagator_step(
+            self._h, int(steps), _dptr(traj_r), _dptr(traj_v), _dptr(traj_a),
+            _stream_ptr(stream)))
+
+    @property
+    def steps_done(self):
+        return load_library().gpop_propagator_steps_done(self._h)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            load_library().gpop_propagator_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class ClosestApproach:
+    """ClosestApproach of the reference (lib/closest_approach/closest_approach.cuh:36-88)."""
+
+    def __init__(self, ctx, start, h, r, v, set_ids):
+        lib = load_library()
+        self.ctx = ctx
+        r = _host(r).reshape(-1, 3)
+        v = _host(v).reshape(-1, 3)
+        ids = np.ascontiguousarray(set_ids, dtype=np.uint32)
+        if ids.shape[0] != r.shape[0]:
+            raise GpopError(1, "set_ids size mismatch")
+        out = _VP()
+        ctx._check(lib.gpop_ca_create(ctx._h, C.byref(as_time(start)), float(h), r.shape[0],
+                                      r.ctypes.data_as(_VP), v.ctypes.data_as(_VP),
+                                      ids.ctypes.data_as(_VP), C.byref(out)))
+        self._h = out.value
+        self.n = r.shape[0]
+
+    def close(self):
+        if getattr(self, "_h", None):
+            load_library().gpop_ca_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def num_pairs(self):
+        return load_library().gpop_ca_num_pairs(self._h)
+
+    def propagate(self, steps):
+        self.ctx._check(load_library().gpop_ca_propagate(self._h, int(steps)))
+
+    def find(self, threshold=-1.0):
+        lib = load_library()
+        cnt = C.c_int64()
+        self.ctx._check(lib.gpop_ca_find(self._h, float(threshold), None, 0, C.byref(cnt)))
+        recs = (CaRecord * max(cnt.value, 1))()
+        self.ctx._check(lib.gpop_ca_find(self._h, float(threshold), recs, cnt.value, C.byref(cnt)))
+        return [recs[i] for i in range(cnt.value)]
+
+    def pairs(self):
+        P = self.num_pairs
+        d = np.zeros(P)
+        t = np.zeros(P)
+        pa = np.zeros((P, 3))
+        pb = np.zeros((P, 3))
+        cs = np.zeros(P, np.uint32)
+        self.ctx._check(load_library().gpop_ca_pairs(
+            self._h, d.ctypes.data_as(_VP), t.ctypes.data_as(_VP), pa.ctypes.data_as(_VP),
+            pb.ctypes.data_as(_VP), cs.ctypes.data_as(_VP)))
+        return dict(distance=d, time=t, posA=pa, posB=pb, closest_step=cs)
+
+    def trajectory(self):
+        lib = load_library()
+        steps = C.c_int32()
+        self.ctx._check(lib.gpop_ca_trajectory(self._h, None, None, None, C.byref(steps)))
+        k = steps.value
+        r = np.zeros((k, 3, self.n))
+        v = np.zeros((k, 3, self.n))
+        a = np.zeros((k, 3, self.n))
+        self.ctx._check(lib.gpop_ca_trajectory(self._h, r.ctypes.data_as(_VP),
+                                               v.ctypes.data_as(_VP), a.ctypes.data_as(_VP),
+                                               C.byref(steps)))
+        return r, v, a

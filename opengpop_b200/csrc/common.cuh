@@ -1,0 +1,76 @@
+// common.cuh -- device constants and helpers shared by the propagation and screening kernels.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace gpop {
+
+// Error bits a kernel may raise in the context's device error word.
+enum : unsigned {
+    kErrTmaTimeout = 1u, // the bounded wait on the gravity-table bulk copy gave up
+    kErrBadInput = 2u, // non-finite or zero-radius position met by the force model
+};
+
+// ---- bulk-copy (TMA, cp.async.bulk) staging of a read-only table into shared memory ----
+__device__ __forceinline__ uint32_t smem_u32(const void* p)
+{
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Copies `bytes` (multiple of 16, both addresses 16-byte aligned) from global to shared memory with
+// one elected thread issuing cp.async.bulk chunks that complete on an mbarrier. Every thread of the
+// block waits with a bounded spin; on timeout the block's error bit is raised and false returned.
+__device__ __forceinline__ bool stage_to_smem(void* smem_dst, const void* gsrc, uint32_t bytes,
+    uint64_t* mbar, unsigned* err_word)
+{
+    const uint32_t bar = smem_u32(mbar);
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+                     : "memory");
+        const uint32_t chunk = 32768u;
+        uint32_t dst = smem_u32(smem_dst);
+        const char* src = static_cast<const char*>(gsrc);
+        for (uint32_t off = 0; off < bytes; off += chunk) {
+            uint32_t len = (bytes - off) < chunk ? (bytes - off) : chunk;
+            asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes "
+                         "[%0], [%1], %2, [%3];" ::"r"(dst + off),
+                         "l"(src + off), "r"(len), "r"(bar)
+                         : "memory");
+        }
+    }
+    // bounded wait on phase 0 (about a second at the sleep below before giving up)
+    uint32_t done = 0;
+    for (int it = 0; it < (1 << 22) && !done; ++it) {
+        asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n"
+                     " selp.u32 %0, 1, 0, p;\n}"
+                     : "=r"(done)
+                     : "r"(bar)
+                     : "memory");
+        if (!done)
+            __nanosleep(64);
+    }
+    if (!done) {
+        if (threadIdx.x == 0)
+            atomicOr(err_word, kErrTmaTimeout);
+        // give the copies in flight a second bounded window before the block leaves
+        for (int it = 0; it < (1 << 22) && !done; ++it) {
+            asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n"
+                         " selp.u32 %0, 1, 0, p;\n}"
+                         : "=r"(done)
+                         : "r"(bar)
+                         : "memory");
+            if (!done)
+                __nanosleep(64);
+        }
+        return false;
+    }
+    return true;
+}
+
+} // namespace gpop

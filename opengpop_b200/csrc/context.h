@@ -1,0 +1,116 @@
+// context.h -- the gpop_ctx object behind the C ABI.
+#pragma once
+#include "gpop.h"
+#include "kernels.h"
+#include "model.h"
+
+#include <cstring>
+#include <string>
+#include <vector>
+
+namespace gpop {
+
+// Grow-only device buffer owned by a context.
+struct DevBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t bytes)
+    {
+        if (bytes <= cap)
+            return cudaSuccess;
+        if (p)
+            cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        cudaError_t e = cudaMalloc(&p, bytes);
+        if (e == cudaSuccess)
+            cap = bytes;
+        return e;
+    }
+    void release()
+    {
+        if (p)
+            cudaFree(p);
+        p = nullptr;
+        cap = 0;
+    }
+    template <class T> T* as() const { return static_cast<T*>(p); }
+};
+
+} // namespace gpop
+
+struct gpop_ctx {
+    gpop_config cfg {};
+    std::string data_dir;
+    std::string err;
+    gpop::ModelData md;
+    int num_sms = 148;
+    int steps_per_launch = 64;
+    int block_override = 0; // GJ8 block size chosen by the tuner (0 = default policy)
+    // device-resident model data
+    gpop::DevBuf t64, mixed, nut, eop, leap, err_word;
+    uint32_t t64_bytes = 0, mixed_bytes = 0, mixed_off32 = 0;
+    gpop::FrameData frames {};
+    int64_t launches = 0;
+    // scratch
+    gpop::DevBuf state, gen_m, prop_m, gen_sec, prop_sec, io_r, io_v;
+
+    gpop::TableSrc table(bool mixed_mode) const
+    {
+        gpop::TableSrc ts;
+        ts.L = md.degree;
+        ts.radius = md.radius;
+        ts.gm = md.gm;
+        ts.mixed = mixed_mode;
+        if (mixed_mode) {
+            ts.src = mixed.p;
+            ts.bytes = mixed_bytes;
+            ts.off32 = mixed_off32;
+        } else {
+            ts.src = t64.p;
+            ts.bytes = t64_bytes;
+            ts.off32 = 0;
+        }
+        return ts;
+    }
+};
+
+// A propagation in progress (GpuPropagator): startup on the first step call, then GJ8 steps.
+// The buffers either belong to the object or are borrowed from the context's scratch.
+struct gpop_propagator {
+    gpop_ctx* ctx = nullptr;
+    int kind = 0;
+    gpop_time start {};
+    double h = 0;
+    int ncorr = 7;
+    int max_steps = 0;
+    int64_t n = 0;
+    double* r = nullptr;
+    double* v = nullptr;
+    int done = 0;
+    bool started = false;
+    bool mixed = false;
+    gpop::DevBuf own_state, own_gen, own_prop;
+    gpop::DevBuf *state = &own_state, *gen_m = &own_gen, *prop_m = &own_prop;
+    ~gpop_propagator()
+    {
+        own_state.release();
+        own_gen.release();
+        own_prop.release();
+    }
+};
+
+namespace gpop {
+gpop_status fail(gpop_ctx* ctx, gpop_status st, const std::string& msg);
+gpop_status cuda_fail(gpop_ctx* ctx, cudaError_t e, const char* what);
+// Builds and fills the generation (80) and propagation (4 + max(steps,4) + 1) epoch tables.
+gpop_status build_epoch_tables(gpop_ctx* ctx, const gpop_time* start, double h, int32_t steps,
+    DevBuf& gen_m, DevBuf& prop_m, cudaStream_t s);
+// Prepares a propagator (validates, builds epoch tables, sizes the state).
+gpop_status propagator_init(gpop_propagator* p, cudaStream_t s);
+// Runs `steps` more steps (startup first when needed).
+gpop_status propagator_step(gpop_propagator* p, int steps, double* traj_r, double* traj_v,
+    double* traj_a, cudaStream_t s);
+// Reads and clears the device error word (synchronises the stream).
+gpop_status check_device_errors(gpop_ctx* ctx, cudaStream_t s);
+} // namespace gpop

@@ -1,0 +1,598 @@
+// propagate.cu -- RK8 startup, fused GJ8 predict-evaluate-correct steps, and the gravity kernel.
+//
+// One thread owns one object for a whole range of steps (objects never interact), so a launch runs
+// many steps with no grid-wide synchronisation. The GJ8 acceleration history lives in a 9-slot
+// ring in global memory (SoA, coalesced); the working state of a step stays in registers.
+#include "common.cuh"
+#include "gravity.cuh"
+#include "gj8_tables.cuh"
+#include "kernels.h"
+
+#include <type_traits>
+
+namespace gpop {
+
+// ---- force models seen by the integrator (IForceModel, iforce_model.cuh:19-33) ----
+template <bool MIXED> struct ForceGravity {
+    static constexpr bool kTable = true;
+    GravSmem g;
+    const double* gen_m;
+    const double* prop_m;
+    // ForceModel::ComputePropagationAcceleration (force_model.cu:91-109): epoch index idx
+    __device__ __forceinline__ void prop(const double* r, const double*, int idx, double* a) const
+    {
+        gravity_gcrs<MIXED>(g, prop_m + (size_t)idx * 9, r, a);
+    }
+    // ForceModel::ComputeGenerationAcceleration (force_model.cu:59-89): table (s'+4)*10 + k
+    __device__ __forceinline__ void gen(const double* r, const double*, int step, int k, double* a) const
+    {
+        const int s = step > 0 ? step - 1 : step;
+        gravity_gcrs<MIXED>(g, gen_m + (size_t)((s + 4) * 10 + k) * 9, r, a);
+    }
+};
+
+// Analytic accelerations of the reference's tests (unit_tests/include/gpu_test_helpers.cuh) with the
+// mock's time rules (unit_tests/include/mock_force_model.cuh:65-106).
+struct ForceAnalytic {
+    static constexpr bool kTable = false;
+    int kind;
+    double h;
+    __device__ void eval(const double* p, const double* v, double t, double* a) const
+    {
+        double val = 0.0;
+        switch (kind) {
+        case 2:
+            a[0] = 1;
+            a[1] = 2;
+            a[2] = 3;
+            return;
+        case 3:
+            val = -3 * 2 * t + 7 * 6 * t * t * t * t * t;
+            break;
+        case 4:
+            val = 56 * pow(t, 6) - 42 * pow(t, 5) + 60 * pow(t, 4) - 100 * pow(t, 3)
+                - 120 * pow(t, 2) + 6 * t - 2;
+            break;
+        case 5:
+            val = 72 * pow(t, 7) + 56 * pow(t, 6) - 42 * pow(t, 5) + 60 * pow(t, 4)
+                - 100 * pow(t, 3) - 120 * pow(t, 2) + 6 * t - 2;
+            break;
+        case 6:
+            val = exp(-t);
+            break;
+        case 7:
+            for (int i = 0; i < 3; ++i)
+                a[i] = -2 * p[i] - 2 * v[i];
+            return;
+        default:
+            val = 0.0;
+        }
+        a[0] = a[1] = a[2] = val;
+    }
+    __device__ __forceinline__ void prop(const double* r, const double* v, int idx, double* a) const
+    {
+        eval(r, v, (double)(idx - 4) * h, a);
+    }
+    __device__ __forceinline__ void gen(const double* r, const double* v, int step, int k, double* a) const
+    {
+        const int dir = step > 0 ? -1 : 1;
+        eval(r, v, (double)(step + dir) * h + (-dir) * c_RKC[k] * h, a);
+    }
+};
+
+// ---- table staging ----
+size_t table_smem_bytes(const TableSrc& ts) { return 128 + (size_t)ts.bytes; }
+
+template <bool MIXED>
+__device__ __forceinline__ bool bind_table(uint8_t* smem, const TableSrc& ts, unsigned* err, GravSmem& g)
+{
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(smem);
+    uint8_t* tab = smem + 128;
+    bool ok = stage_to_smem(tab, ts.src, ts.bytes, mbar, err);
+    g.L = ts.L;
+    g.radius = ts.radius;
+    g.gm = ts.gm;
+    g.t64 = reinterpret_cast<const GravEntry64*>(tab);
+    g.t32 = reinterpret_cast<const GravEntry32*>(tab + ts.off32);
+    return ok;
+}
+
+// ---- RK8 startup and mid-corrector (lib/gpu_startup/src/gpu_startup.cu:55-318) ----
+struct StartupMats {
+    double r[9][3], v[9][3], a[9][3], s[9][3], S[9][3];
+};
+
+// RK8::step (gpu_startup.cu:108-144): stage state = base + h sum a_ki K_i; new column = base +
+// h sum b_k K_k, for both position (K = stage velocity) and velocity (K = acceleration).
+template <class F>
+__device__ void rk8_step(const F& f, double h, int step, StartupMats& m)
+{
+    const double hh = step > 0 ? h : -h;
+    const int base = 4 + step + (step > 0 ? -1 : 1);
+    double Kx[10][3], Kv[10][3];
+    double tx[3], tv[3];
+    for (int j = 0; j < 3; ++j) {
+        tx[j] = m.r[base][j];
+        tv[j] = m.v[base][j];
+        Kx[0][j] = tv[j];
+    }
+    f.gen(tx, tv, step, 0, Kv[0]);
+    for (int k = 1; k <= 9; ++k) {
+        for (int j = 0; j < 3; ++j) {
+            double sx = 0.0, sv = 0.0;
+            for (int i = 0; i < k; ++i) {
+                sx = fma(c_RKA[k - 1][i], Kx[i][j], sx);
+                sv = fma(c_RKA[k - 1][i], Kv[i][j], sv);
+            }
+            tx[j] = fma(hh, sx, m.r[base][j]);
+            tv[j] = fma(hh, sv, m.v[base][j]);
+        }
+        f.gen(tx, tv, step, k, Kv[k]);
+        for (int j = 0; j < 3; ++j)
+            Kx[k][j] = tv[j];
+    }
+    const int col = 4 + step;
+    for (int j = 0; j < 3; ++j) {
+        double sx = 0.0, sv = 0.0;
+        for (int k = 0; k < 10; ++k) {
+            sx = fma(Kx[k][j], c_RKB[k], sx);
+            sv = fma(Kv[k][j], c_RKB[k], sv);
+        }
+        m.v[col][j] = fma(hh, sv, m.v[base][j]);
+        m.r[col][j] = fma(hh, sx, m.r[base][j]);
+    }
+}
+
+// StartupCorrector::CalculateAccelerationMatrix (gpu_startup.cu:196-224)
+template <class F> __device__ void corrector_accel(const F& f, StartupMats& m, bool epoch)
+{
+    for (int i = 0; i < 9; ++i)
+        if (i != 4 || epoch)
+            f.prop(m.r[i], m.v[i], i, m.a[i]);
+}
+
+// StartupCorrector::CalculateS0 (gpu_startup.cu:170-195), Berry & Healy eqs. 73, 75, 86
+__device__ void corrector_s0(double h, StartupMats& m)
+{
+    const double hinv = 1 / h, h2inv = 1 / (h * h);
+    for (int j = 0; j < 3; ++j) {
+        double sb = 0.0, sa = 0.0;
+        for (int k = 0; k < 9; ++k) {
+            sb = fma(c_SA[4][k], m.a[k][j], sb);
+            sa = fma(c_GJ[4][k], m.a[k][j], sa);
+        }
+        m.s[4][j] = fma(hinv, m.v[4][j], -sb);
+        m.S[4][j] = fma(h2inv, m.r[4][j], -sa);
+    }
+}
+
+// CalculateAllSKernel (gpu_startup/src/device/calculate_all_s.cu:19-47)
+__device__ void corrector_all_s(StartupMats& m)
+{
+    for (int i = 1; i <= 4; ++i)
+        for (int j = 0; j < 3; ++j) {
+            m.s[4 + i][j] = m.s[4 + i - 1][j] + (m.a[4 + i - 1][j] + m.a[4 + i][j]) / 2;
+            m.s[4 - i][j] = m.s[4 - i + 1][j] - (m.a[4 - i + 1][j] + m.a[4 - i][j]) / 2;
+            m.S[4 + i][j] = m.s[4 + i - 1][j] + m.S[4 + i - 1][j] + m.a[4 + i - 1][j] / 2;
+            m.S[4 - i][j] = -m.s[4 - i + 1][j] + m.S[4 - i + 1][j] + m.a[4 - i + 1][j] / 2;
+        }
+}
+
+// StartupCorrector::Correct (gpu_startup.cu:247-294)
+template <class F> __device__ void corrector_correct(const F& f, double h, StartupMats& m)
+{
+    corrector_s0(h, m);
+    corrector_all_s(m);
+    const double h2 = h * h;
+    for (int c = 0; c < 9; ++c) {
+        if (c == 4)
+            continue; // the epoch column is restored
+        for (int j = 0; j < 3; ++j) {
+            double sv = 0.0, sr = 0.0;
+            for (int k = 0; k < 9; ++k) {
+                sv = fma(m.a[k][j], c_SA[c][k], sv);
+                sr = fma(m.a[k][j], c_GJ[c][k], sr);
+            }
+            m.v[c][j] = h * (sv + m.s[c][j]);
+            m.r[c][j] = h2 * (sr + m.S[c][j]);
+        }
+    }
+    corrector_accel(f, m, false);
+}
+
+template <class F>
+__device__ void run_startup(const F& f, double h, int ncorr, const double* r0, const double* v0, StartupMats& m)
+{
+    for (int c = 0; c < 9; ++c)
+        for (int j = 0; j < 3; ++j)
+            m.r[c][j] = m.v[c][j] = m.a[c][j] = m.s[c][j] = m.S[c][j] = 0.0;
+    for (int j = 0; j < 3; ++j) {
+        m.r[4][j] = r0[j];
+        m.v[4][j] = v0[j];
+    }
+    for (int i = 1; i <= 4; ++i) { // StartupPredictor::Predict (gpu_startup.cu:162-165)
+        rk8_step(f, h, i, m);
+        rk8_step(f, h, -i, m);
+    }
+    if (ncorr <= 0)
+        return;
+    corrector_accel(f, m, true);
+    for (int i = 0; i < ncorr; ++i)
+        corrector_correct(f, h, m);
+}
+
+template <class F>
+__global__ void __launch_bounds__(256) startup_kernel(F f, TableSrc ts, PropArgs a)
+{
+    extern __shared__ __align__(128) uint8_t smem[];
+    if constexpr (F::kTable) {
+        if (!bind_table<std::is_same<F, ForceGravity<true>>::value>(smem, ts, a.err, f.g))
+            return;
+    }
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n)
+        return;
+    double r0[3], v0[3];
+    for (int j = 0; j < 3; ++j) {
+        r0[j] = a.r0[i * 3 + j];
+        v0[j] = a.v0[i * 3 + j];
+    }
+    StartupMats m;
+    run_startup(f, a.h, a.ncorr, r0, v0, m);
+    if (a.out27[0]) {
+        for (int c = 0; c < 9; ++c)
+            for (int j = 0; j < 3; ++j) {
+                const int64_t o = i * 27 + c * 3 + j;
+                a.out27[0][o] = m.r[c][j];
+                a.out27[1][o] = m.v[c][j];
+                a.out27[2][o] = m.a[c][j];
+                a.out27[3][o] = m.s[c][j];
+                a.out27[4][o] = m.S[c][j];
+            }
+    }
+    if (a.state) {
+        const int64_t n = a.n;
+        double* st = a.state;
+        const bool fix_q3 = (a.flags & 2u) != 0;
+        for (int j = 0; j < 3; ++j) {
+            // GpuPropagator::Step at step 1 (gpu_propagator.cu:31-47): s, S from column 8; the
+            // caller's buffers hold column 8 after the corrector (gpu_startup.cu:59-61).
+            st[(kR + j) * n + i] = m.r[8][j];
+            st[(kV + j) * n + i] = m.v[8][j];
+            st[(kSs + j) * n + i] = m.s[8][j];
+            st[(kSb + j) * n + i] = m.S[8][j];
+            for (int c = 0; c < 9; ++c)
+                st[(kHist + c * 3 + j) * n + i] = m.a[c][j];
+            for (int k = 0; k < 4; ++k) { // replay of steps 1..4 (CopyStartupStateKernel)
+                st[(kRep + k * 6 + j) * n + i] = m.r[5 + k][j];
+                st[(kRep + k * 6 + 3 + j) * n + i] = m.v[5 + k][j];
+                st[(kRepA + k * 3 + j) * n + i] = fix_q3 ? m.a[5 + k][j] : m.a[8][j];
+            }
+        }
+    }
+}
+
+// ---- GJ8 step (prediction.cu:49-74 + gpu_propagator.cu:86-119) ----
+template <class F>
+__global__ void __launch_bounds__(512, 1) gj8_kernel(F f, TableSrc ts, PropArgs a)
+{
+    extern __shared__ __align__(128) uint8_t smem[];
+    if constexpr (F::kTable) {
+        if (!bind_table<std::is_same<F, ForceGravity<true>>::value>(smem, ts, a.err, f.g))
+            return;
+    }
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n)
+        return;
+    const int64_t n = a.n;
+    double* st = a.state;
+    const double h = a.h;
+    double r[3], v[3], s[3], S[3];
+    for (int j = 0; j < 3; ++j) {
+        r[j] = st[(kR + j) * n + i];
+        v[j] = st[(kV + j) * n + i];
+        s[j] = st[(kSs + j) * n + i];
+        S[j] = st[(kSb + j) * n + i];
+    }
+    for (int step = a.step_begin; step < a.step_end; ++step) {
+        double ae[3];
+        if (step <= 4) {
+            for (int j = 0; j < 3; ++j) {
+                r[j] = st[(kRep + (step - 1) * 6 + j) * n + i];
+                v[j] = st[(kRep + (step - 1) * 6 + 3 + j) * n + i];
+                ae[j] = st[(kRepA + (step - 1) * 3 + j) * n + i];
+            }
+        } else {
+            const int ring0 = (step - 5) % 9;
+            double hist[9][3];
+#pragma unroll
+            for (int k = 0; k < 9; ++k) {
+                int slot = ring0 + k;
+                slot -= slot >= 9 ? 9 : 0;
+#pragma unroll
+                for (int j = 0; j < 3; ++j)
+                    hist[k][j] = st[(kHist + slot * 3 + j) * n + i];
+            }
+            // Predictor (FinalizePredictionKernel, gpu_integrator/src/device/dev_functions.cu:34-50)
+            double s1[3], s2[3], prev[3], a7[3], a8[3];
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                double vt = 0.0, rt = 0.0;
+#pragma unroll
+                for (int k = 0; k < 9; ++k) {
+                    vt = fma(hist[k][j], c_SA[9][k], vt);
+                    rt = fma(hist[k][j], c_GJ[9][k], rt);
+                }
+                S[j] += s[j] + hist[8][j] / 2;
+                v[j] = (vt + s[j] + hist[8][j] / 2) * h;
+                r[j] = (rt + S[j]) * h * h;
+                // corrector partial sums over the shifted history (gpu_propagator.cu:92-100)
+                double c1 = 0.0, c2 = 0.0;
+#pragma unroll
+                for (int k = 0; k < 8; ++k) {
+                    c1 = fma(hist[k + 1][j], c_SA[8][k], c1);
+                    c2 = fma(hist[k + 1][j], c_GJ[8][k], c2);
+                }
+                s1[j] = c1;
+                s2[j] = c2;
+                prev[j] = s[j];
+                a7[j] = hist[8][j];
+            }
+            const int idx = step + 4;
+            f.prop(r, v, idx, a8);
+            // Corrector: the first pass reuses the predictor's evaluation at the unchanged
+            // position (bit-identical to the reference's repeated call).
+            for (int it = 0; it < a.ncorr; ++it) {
+                if (it > 0)
+                    f.prop(r, v, idx, a8);
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    s[j] = prev[j] + (a8[j] + a7[j]) / 2;
+                    v[j] = h * (s1[j] + a8[j] * c_SA[8][8] + s[j]);
+                    r[j] = h * h * (s2[j] + a8[j] * c_GJ[8][8] + S[j]);
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                st[(kHist + ring0 * 3 + j) * n + i] = a8[j];
+                ae[j] = a8[j];
+            }
+        }
+        const int64_t t = step - a.traj_step0;
+        if (a.traj_r)
+            for (int j = 0; j < 3; ++j)
+                a.traj_r[(t * 3 + j) * n + i] = r[j];
+        if (a.traj_v)
+            for (int j = 0; j < 3; ++j)
+                a.traj_v[(t * 3 + j) * n + i] = v[j];
+        if (a.traj_a)
+            for (int j = 0; j < 3; ++j)
+                a.traj_a[(t * 3 + j) * n + i] = ae[j];
+    }
+    for (int j = 0; j < 3; ++j) {
+        st[(kR + j) * n + i] = r[j];
+        st[(kV + j) * n + i] = v[j];
+        st[(kSs + j) * n + i] = s[j];
+        st[(kSb + j) * n + i] = S[j];
+        if (a.out_r)
+            a.out_r[i * 3 + j] = r[j];
+        if (a.out_v)
+            a.out_v[i * 3 + j] = v[j];
+    }
+}
+
+template <bool MIXED>
+__global__ void __launch_bounds__(512, 1) gravity_kernel(TableSrc ts, int64_t n, const double* r,
+    const double* m9, double* a, unsigned* err)
+{
+    extern __shared__ __align__(128) uint8_t smem[];
+    GravSmem g;
+    if (!bind_table<MIXED>(smem, ts, err, g))
+        return;
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    double p[3] = { r[i * 3], r[i * 3 + 1], r[i * 3 + 2] };
+    double acc[3];
+    if (m9) {
+        gravity_gcrs<MIXED>(g, m9, p, acc);
+    } else {
+        gravity_itrs<MIXED>(g, p[0], p[1], p[2], acc[0], acc[1], acc[2]);
+    }
+    a[i * 3] = acc[0];
+    a[i * 3 + 1] = acc[1];
+    a[i * 3 + 2] = acc[2];
+}
+
+// ---- single-object unit kernels for the integrator's known-answer tests ----
+__global__ void corrector_unit_kernel(ForceAnalytic f, int op, double* r27, double* v27,
+    double* a27, double* s27, double* S27)
+{
+    StartupMats m;
+    for (int c = 0; c < 9; ++c)
+        for (int j = 0; j < 3; ++j) {
+            m.r[c][j] = r27[c * 3 + j];
+            m.v[c][j] = v27[c * 3 + j];
+            m.a[c][j] = m.s[c][j] = m.S[c][j] = 0.0;
+        }
+    corrector_accel(f, m, true);
+    if (op == 1)
+        corrector_s0(f.h, m);
+    else if (op == 2)
+        corrector_correct(f, f.h, m);
+    for (int c = 0; c < 9; ++c)
+        for (int j = 0; j < 3; ++j) {
+            r27[c * 3 + j] = m.r[c][j];
+            v27[c * 3 + j] = m.v[c][j];
+            a27[c * 3 + j] = m.a[c][j];
+            s27[c * 3 + j] = m.s[c][j];
+            S27[c * 3 + j] = m.S[c][j];
+        }
+}
+
+__global__ void predict_unit_kernel(ForceAnalytic f, int step, double* r, double* v, double* a27,
+    double* s, double* S)
+{
+    const double h = f.h;
+    double vt[3], rt[3];
+    for (int j = 0; j < 3; ++j) {
+        double sv = 0.0, sr = 0.0;
+        for (int k = 0; k < 9; ++k) {
+            sv = fma(a27[k * 3 + j], c_SA[9][k], sv);
+            sr = fma(a27[k * 3 + j], c_GJ[9][k], sr);
+        }
+        vt[j] = sv;
+        rt[j] = sr;
+    }
+    for (int j = 0; j < 3; ++j) {
+        S[j] += s[j] + a27[24 + j] / 2;
+        v[j] = (vt[j] + s[j] + a27[24 + j] / 2) * h;
+        r[j] = (rt[j] + S[j]) * h * h;
+    }
+    for (int k = 0; k < 8; ++k)
+        for (int j = 0; j < 3; ++j)
+            a27[k * 3 + j] = a27[(k + 1) * 3 + j];
+    double a8[3];
+    f.prop(r, v, step + 4, a8);
+    for (int j = 0; j < 3; ++j)
+        a27[24 + j] = a8[j];
+}
+
+__global__ void finalize_unit_kernel(double h, double* r, double* v, const double* a27,
+    const double* s, const double* S)
+{
+    for (int j = 0; j < 3; ++j) {
+        v[j] = h * (v[j] + a27[24 + j] * c_SA[8][8] + s[j]);
+        r[j] = h * h * (r[j] + a27[24 + j] * c_GJ[8][8] + S[j]);
+    }
+}
+
+// ---- launchers ----
+LaunchShape pick_shape(int64_t n, int max_block, int num_sms)
+{
+    LaunchShape ls;
+    int64_t per_sm = (n + num_sms - 1) / num_sms;
+    int64_t block = ((per_sm + 31) / 32) * 32;
+    if (block < 32)
+        block = 32;
+    if (block > max_block)
+        block = max_block;
+    ls.block = (int)block;
+    ls.grid = (int)((n + block - 1) / block);
+    return ls;
+}
+
+template <class K> static cudaError_t set_smem(K kernel, size_t bytes)
+{
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+cudaError_t launch_startup(const TableSrc& ts, const PropArgs& a, int num_sms, cudaStream_t s)
+{
+    if (a.n <= 0)
+        return cudaSuccess;
+    LaunchShape ls = pick_shape(a.n, 256, num_sms);
+    if (a.kind == 0) {
+        size_t smem = table_smem_bytes(ts);
+        if (ts.mixed) {
+            ForceGravity<true> f {};
+            f.gen_m = a.gen_m;
+            f.prop_m = a.prop_m;
+            cudaError_t e = set_smem(startup_kernel<ForceGravity<true>>, smem);
+            if (e != cudaSuccess)
+                return e;
+            startup_kernel<<<ls.grid, ls.block, smem, s>>>(f, ts, a);
+        } else {
+            ForceGravity<false> f {};
+            f.gen_m = a.gen_m;
+            f.prop_m = a.prop_m;
+            cudaError_t e = set_smem(startup_kernel<ForceGravity<false>>, smem);
+            if (e != cudaSuccess)
+                return e;
+            startup_kernel<<<ls.grid, ls.block, smem, s>>>(f, ts, a);
+        }
+    } else {
+        ForceAnalytic f { a.kind, a.h };
+        startup_kernel<<<ls.grid, ls.block, 0, s>>>(f, ts, a);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gj8(const TableSrc& ts, const PropArgs& a, int num_sms, cudaStream_t s, int block_override)
+{
+    if (a.n <= 0 || a.step_end <= a.step_begin)
+        return cudaSuccess;
+    LaunchShape ls = pick_shape(a.n, 512, num_sms);
+    if (block_override > 0) {
+        ls.block = block_override;
+        ls.grid = (int)((a.n + block_override - 1) / block_override);
+    }
+    if (a.kind == 0) {
+        size_t smem = table_smem_bytes(ts);
+        if (ts.mixed) {
+            ForceGravity<true> f {};
+            f.gen_m = a.gen_m;
+            f.prop_m = a.prop_m;
+            cudaError_t e = set_smem(gj8_kernel<ForceGravity<true>>, smem);
+            if (e != cudaSuccess)
+                return e;
+            gj8_kernel<<<ls.grid, ls.block, smem, s>>>(f, ts, a);
+        } else {
+            ForceGravity<false> f {};
+            f.gen_m = a.gen_m;
+            f.prop_m = a.prop_m;
+            cudaError_t e = set_smem(gj8_kernel<ForceGravity<false>>, smem);
+            if (e != cudaSuccess)
+                return e;
+            gj8_kernel<<<ls.grid, ls.block, smem, s>>>(f, ts, a);
+        }
+    } else {
+        ForceAnalytic f { a.kind, a.h };
+        gj8_kernel<<<ls.grid, ls.block, 0, s>>>(f, ts, a);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gravity(const TableSrc& ts, int64_t n, const double* r, const double* m9,
+    double* a, unsigned* err, int num_sms, cudaStream_t s)
+{
+    if (n <= 0)
+        return cudaSuccess;
+    LaunchShape ls = pick_shape(n, 512, num_sms);
+    size_t smem = table_smem_bytes(ts);
+    if (ts.mixed) {
+        cudaError_t e = set_smem(gravity_kernel<true>, smem);
+        if (e != cudaSuccess)
+            return e;
+        gravity_kernel<true><<<ls.grid, ls.block, smem, s>>>(ts, n, r, m9, a, err);
+    } else {
+        cudaError_t e = set_smem(gravity_kernel<false>, smem);
+        if (e != cudaSuccess)
+            return e;
+        gravity_kernel<false><<<ls.grid, ls.block, smem, s>>>(ts, n, r, m9, a, err);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_corrector_unit(int kind, double h, int op, double* r27, double* v27, double* a27,
+    double* s27, double* S27, cudaStream_t s)
+{
+    corrector_unit_kernel<<<1, 1, 0, s>>>(ForceAnalytic { kind, h }, op, r27, v27, a27, s27, S27);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_predict_unit(int kind, double h, int step, double* r3, double* v3, double* a27,
+    double* s3, double* S3, cudaStream_t s)
+{
+    predict_unit_kernel<<<1, 1, 0, s>>>(ForceAnalytic { kind, h }, step, r3, v3, a27, s3, S3);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_finalize_unit(double h, double* r3, double* v3, const double* a27,
+    const double* s3, const double* S3, cudaStream_t s)
+{
+    finalize_unit_kernel<<<1, 1, 0, s>>>(h, r3, v3, a27, s3, S3);
+    return cudaGetLastError();
+}
+
+} // namespace gpop

@@ -525,9 +525,9 @@ double leap_seconds(const Data& d, double mjd) // types.cuh:140-152
 }
 
 // time_points.cu:26-71 (one epoch) followed by the matrix chain of time_points.cu:160-201
-void frame_matrix(const Data& d, const or_time& st, double sec_offset, double* M, double* mjd_out)
+void frame_matrix(const Data& d, const or_time& st, double sec_arg, double* M, double* mjd_out)
 {
-    double mjd_utc = calendar_to_mjd(st.year, st.month, st.day, st.hour, st.min, st.sec + sec_offset);
+    double mjd_utc = calendar_to_mjd(st.year, st.month, st.day, st.hour, st.min, sec_arg);
     if (mjd_out)
         *mjd_out = mjd_utc;
     EopRec eop = eop_record(d, mjd_utc);
@@ -569,15 +569,15 @@ void frame_matrix(const Data& d, const or_time& st, double sec_offset, double* M
     matmul3(QR, W, M);
 }
 
-// time_points.cu:26-47 time of table entry idx
-double table_offset(double h, int idx, bool midpoints, int before)
+// time_points.cu:34-46: seconds argument of table entry idx, (sec - before h) + time from start
+double table_sec(const or_time& st, double h, int idx, bool midpoints, int before)
 {
     double from_start;
     if (midpoints)
         from_start = ((double)(idx / kRkStages) + kRkNodes[idx % kRkStages]) * h;
     else
         from_start = idx * h;
-    return -(double)before * h + from_start;
+    return (st.sec - (double)before * h) + from_start;
 }
 
 // ---------------- gravity (gravity_source.cu:168-262 + gravity_source_device.cu:63-239) ----------------
@@ -808,19 +808,19 @@ void build_tables(Force& f, const or_time& st, int steps)
         return;
     f.gen_m.assign(80 * 9, 0.0);
     for (int idx = 0; idx < 80; ++idx) {
-        double off = table_offset(f.h, idx, true, 4);
+        double sec = table_sec(st, f.h, idx, true, 4);
         if (f.flags & OR_FLAG_FIX_Q1) {
             int sp = idx / kRkStages - 4; // s'
             int k = idx % kRkStages;
-            if (sp < 0) // backward step -i with i = -sp: true stage time
-                off = (double)(sp + 1) * f.h - kRkNodes[k] * f.h;
+            if (sp < 0) // backward step -i with i = -sp: true stage time -(i-1) h - c_k h
+                sec = (st.sec - 4.0 * f.h) + (((double)(sp + 1) - kRkNodes[k]) * f.h + 4.0 * f.h);
         }
-        frame_matrix(*f.d, st, off, &f.gen_m[idx * 9], nullptr);
+        frame_matrix(*f.d, st, sec, &f.gen_m[idx * 9], nullptr);
     }
     int len = 4 + std::max(steps, 4) + 1;
     f.prop_m.assign((size_t)len * 9, 0.0);
     for (int idx = 0; idx < len; ++idx)
-        frame_matrix(*f.d, st, table_offset(f.h, idx, false, 4), &f.prop_m[idx * 9], nullptr);
+        frame_matrix(*f.d, st, table_sec(st, f.h, idx, false, 4), &f.prop_m[idx * 9], nullptr);
 }
 
 struct Startup {
@@ -1282,7 +1282,7 @@ void or_frame_matrices(const void* dv, const or_time* st, double h, int32_t coun
     const Data* d = static_cast<const Data*>(dv);
 #pragma omp parallel for schedule(dynamic, 16)
     for (int i = 0; i < count; ++i)
-        frame_matrix(*d, *st, table_offset(h, i, mid != 0, before), m_out + (size_t)i * 9,
+        frame_matrix(*d, *st, table_sec(*st, h, i, mid != 0, before), m_out + (size_t)i * 9,
             mjd_out ? mjd_out + i : nullptr);
 }
 
