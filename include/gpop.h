@@ -109,6 +109,18 @@ gpop_status gpop_propagator_step(gpop_propagator* p, int32_t steps, double* traj
 /* Steps taken so far. */
 int32_t gpop_propagator_steps_done(const gpop_propagator* p);
 void gpop_propagator_destroy(gpop_propagator* p);
+/* No counterpart in the reference. gpop_propagate_device for callers that may not allocate device
+ * memory while running (services that reserve their memory budget at start-up and forbid later
+ * allocation; hosts whose device memory is held by another allocator's pool). The scratch lives in
+ * one fixed device array of the library (about 4.1 MB on every GPU that loads it, until exit), so
+ * calls are limited to GPOP_NOALLOC_MAX_OBJECTS objects and GPOP_NOALLOC_MAX_STEPS steps; larger
+ * requests return GPOP_ERR_INVALID_ARG. All calls share that array: calls that overlap on the GPU
+ * race. The first call on a device looks the array up (cudaGetSymbolAddress) and should come
+ * before any stream capture. */
+#define GPOP_NOALLOC_MAX_OBJECTS 4096
+#define GPOP_NOALLOC_MAX_STEPS 20160
+gpop_status gpop_propagate_device_noalloc(gpop_ctx* ctx, const gpop_time* start, double h,
+    int32_t steps, int64_t n, double* r_dev, double* v_dev, void* stream);
 /* Analytic test forces through the same integrator kernels (MockForceModel,
  * unit_tests/include/mock_force_model.cuh:46-112). Times follow the mock: (idx - 4) h. */
 gpop_status gpop_propagate_analytic(gpop_ctx* ctx, int32_t kind, double h, int32_t steps,

@@ -28,7 +28,7 @@ FORCE = {"gravity": 0, "zero": 1, "const": 2, "poly7": 3, "poly8": 4, "poly9": 5
 EXPORTS = (
     "gpop_config_default", "gpop_create", "gpop_destroy", "gpop_last_error", "gpop_status_string",
     "gpop_gravity_degree", "gpop_kernel_launches", "gpop_propagate", "gpop_propagate_device",
-    "gpop_propagate_trajectory", "gpop_propagator_create", "gpop_propagator_step",
+    "gpop_propagate_device_noalloc", "gpop_propagate_trajectory", "gpop_propagator_create", "gpop_propagator_step",
     "gpop_propagator_steps_done", "gpop_propagator_destroy", "gpop_propagate_analytic", "gpop_startup", "gpop_corrector_unit",
     "gpop_predict_unit", "gpop_finalize_correction_unit", "gpop_gravity", "gpop_frame_matrices",
     "gpop_ca_create", "gpop_ca_propagate", "gpop_ca_find", "gpop_ca_pairs", "gpop_ca_num_pairs",
@@ -83,6 +83,8 @@ def load_library(path=LIB_PATH):
         "gpop_kernel_launches": (i64, [_VP]),
         "gpop_propagate": (i32, [_VP, C.POINTER(Time), f64, i32, i64, _VP, _VP, _VP, _VP]),
         "gpop_propagate_device": (i32, [_VP, C.POINTER(Time), f64, i32, i64, _VP, _VP, _VP]),
+        "gpop_propagate_device_noalloc": (i32, [_VP, C.POINTER(Time), f64, i32, i64, _VP, _VP,
+                                                _VP]),
         "gpop_propagate_trajectory": (i32, [_VP, C.POINTER(Time), f64, i32, i64] + [_VP] * 6),
         "gpop_propagator_create": (i32, [_VP, C.POINTER(Time), f64, i32, i64, _VP, _VP,
                                          C.POINTER(_VP)]),
