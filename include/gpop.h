@@ -168,6 +168,10 @@ typedef struct {
  * at most 1, at least two sets. Host buffers. */
 gpop_status gpop_ca_create(gpop_ctx* ctx, const gpop_time* start, double h, int64_t n,
     const double* r_in, const double* v_in, const uint32_t* set_ids, gpop_ca** out);
+/* ClosestApproach constructed over a MockForceModel (unit_tests/include/mock_force_model.cuh:46-112,
+ * used by unit_tests/closest_approach_test.cu): same screen and refinement, analytic force kind. */
+gpop_status gpop_ca_create_analytic(gpop_ctx* ctx, int32_t kind, double h, int64_t n,
+    const double* r_in, const double* v_in, const uint32_t* set_ids, gpop_ca** out);
 /* ClosestApproach::Propagate (closest_approach.cu:129-157): steps more steps; running minima
  * persist across calls. */
 gpop_status gpop_ca_propagate(gpop_ca* ca, int32_t steps);

@@ -31,7 +31,7 @@ EXPORTS = (
     "gpop_propagate_device_noalloc", "gpop_propagate_trajectory", "gpop_propagator_create", "gpop_propagator_step",
     "gpop_propagator_steps_done", "gpop_propagator_destroy", "gpop_propagate_analytic", "gpop_startup", "gpop_corrector_unit",
     "gpop_predict_unit", "gpop_finalize_correction_unit", "gpop_gravity", "gpop_frame_matrices",
-    "gpop_ca_create", "gpop_ca_propagate", "gpop_ca_find", "gpop_ca_pairs", "gpop_ca_num_pairs",
+    "gpop_ca_create", "gpop_ca_create_analytic", "gpop_ca_propagate", "gpop_ca_find", "gpop_ca_pairs", "gpop_ca_num_pairs",
     "gpop_ca_trajectory", "gpop_ca_destroy",
 )
 
@@ -99,6 +99,7 @@ def load_library(path=LIB_PATH):
         "gpop_gravity": (i32, [_VP, i64, _VP, _VP, _VP, i32, _VP]),
         "gpop_frame_matrices": (i32, [_VP, C.POINTER(Time), f64, i32, i32, i32, _VP, _VP, _VP]),
         "gpop_ca_create": (i32, [_VP, C.POINTER(Time), f64, i64, _VP, _VP, _VP, C.POINTER(_VP)]),
+        "gpop_ca_create_analytic": (i32, [_VP, i32, f64, i64, _VP, _VP, _VP, C.POINTER(_VP)]),
         "gpop_ca_propagate": (i32, [_VP, i32]),
         "gpop_ca_find": (i32, [_VP, f64, _VP, i64, C.POINTER(i64)]),
         "gpop_ca_pairs": (i32, [_VP] * 6),
@@ -266,8 +267,8 @@ class Context:
             int(before_epoch), _dptr(m_out), _dptr(mjd_out), _stream_ptr(stream)))
 
     # ---- closest approach ----
-    def closest_approach(self, start, h, r, v, set_ids):
-        return ClosestApproach(self, start, h, r, v, set_ids)
+    def closest_approach(self, start, h, r, v, set_ids, kind="gravity"):
+        return ClosestApproach(self, start, h, r, v, set_ids, kind)
 
 
 class Propagator:
@@ -307,7 +308,7 @@ class Propagator:
 class ClosestApproach:
     """ClosestApproach of the reference (lib/closest_approach/closest_approach.cuh:36-88)."""
 
-    def __init__(self, ctx, start, h, r, v, set_ids):
+    def __init__(self, ctx, start, h, r, v, set_ids, kind="gravity"):
         lib = load_library()
         self.ctx = ctx
         r = _host(r).reshape(-1, 3)
@@ -316,9 +317,15 @@ class ClosestApproach:
         if ids.shape[0] != r.shape[0]:
             raise GpopError(1, "set_ids size mismatch")
         out = _VP()
-        ctx._check(lib.gpop_ca_create(ctx._h, C.byref(as_time(start)), float(h), r.shape[0],
-                                      r.ctypes.data_as(_VP), v.ctypes.data_as(_VP),
-                                      ids.ctypes.data_as(_VP), C.byref(out)))
+        k = FORCE[kind] if isinstance(kind, str) else kind
+        if k == 0:
+            ctx._check(lib.gpop_ca_create(ctx._h, C.byref(as_time(start)), float(h), r.shape[0],
+                                          r.ctypes.data_as(_VP), v.ctypes.data_as(_VP),
+                                          ids.ctypes.data_as(_VP), C.byref(out)))
+        else:
+            ctx._check(lib.gpop_ca_create_analytic(ctx._h, k, float(h), r.shape[0],
+                                                   r.ctypes.data_as(_VP), v.ctypes.data_as(_VP),
+                                                   ids.ctypes.data_as(_VP), C.byref(out)))
         self._h = out.value
         self.n = r.shape[0]
 

@@ -1,0 +1,312 @@
+// screen.cu -- pairwise closest-approach screen and TCA refinement
+// (lib/closest_approach/src/device.cu:56-173, utility/interpolation.cuh:27-152).
+//
+// Screen: the reference launches one thread per pair per step (UpdateClosestApproachKernel), each
+// copying up to 54 doubles of node states on every new minimum and racing on a shared "last" array.
+// Here a block owns a 64 x 64 tile of (a, b) object pairs and walks every step of a phase: the
+// positions of its 128 objects are staged into shared memory 16 steps at a time from the
+// trajectory store, each thread keeps the running minimum of the squared distance and its step
+// for a 4 x 4 micro-tile in registers, and writes once at the end. Squared distances are compared
+// with the reference's strict "<", so the first step attaining the minimum wins as in the
+// reference (sqrt is monotonic). Node states for the refinement are read back from the trajectory
+// store, so "before" is always the previous step's state (no race).
+#include "kernels.h"
+#include "screen.h"
+
+#include <cfloat>
+#include <cstdint>
+
+namespace gpop {
+
+constexpr int kTile = 64; // objects per tile side
+constexpr int kSub = 4; // pairs per thread side
+constexpr int kStepChunk = 16; // steps staged per pass
+
+__global__ void __launch_bounds__(256) screen_kernel(ScreenArgs a)
+{
+    __shared__ __align__(16) double sa[kStepChunk][3][kTile];
+    __shared__ __align__(16) double sb[kStepChunk][3][kTile];
+    const int2 tile = a.tiles[blockIdx.x];
+    const int a0 = tile.x, b0 = tile.y;
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    const int64_t N = a.n;
+    // per-thread pairs: a = a0 + ty*4 + i, b = b0 + tx*4 + j
+    double best[kSub][kSub];
+    uint32_t bstep[kSub][kSub];
+    bool valid[kSub][kSub];
+    int64_t pidx[kSub][kSub];
+#pragma unroll
+    for (int i = 0; i < kSub; ++i) {
+        const int ai = a0 + ty * kSub + i;
+        const int bound = ai < N ? a.bound[ai] : (int)N;
+        const int64_t base = ai < N ? a.base[ai] : 0;
+#pragma unroll
+        for (int j = 0; j < kSub; ++j) {
+            const int bj = b0 + tx * kSub + j;
+            valid[i][j] = ai < N && bj < N && bj >= bound;
+            pidx[i][j] = base + bj;
+            best[i][j] = DBL_MAX;
+            bstep[i][j] = 0xFFFFFFFFu;
+            if (valid[i][j] && a.init == 0) {
+                best[i][j] = a.min_d2[pidx[i][j]];
+                bstep[i][j] = a.min_step[pidx[i][j]];
+            }
+        }
+    }
+    for (int k0 = a.step_lo; k0 < a.step_hi; k0 += kStepChunk) {
+        const int kc = min(kStepChunk, a.step_hi - k0);
+        __syncthreads();
+        // stage kc steps x 3 axes x 64 objects for the a and b tiles (coalesced rows of 64)
+        for (int e = threadIdx.x; e < kc * 3 * kTile; e += blockDim.x) {
+            const int o = e % kTile;
+            const int c = (e / kTile) % 3;
+            const int k = e / (3 * kTile);
+            const int64_t row = ((int64_t)(k0 + k) * 3 + c) * N;
+            sa[k][c][o] = (a0 + o < N) ? a.traj_r[row + a0 + o] : 0.0;
+            sb[k][c][o] = (b0 + o < N) ? a.traj_r[row + b0 + o] : 0.0;
+        }
+        __syncthreads();
+        for (int k = 0; k < kc; ++k) {
+            double ax[kSub], ay[kSub], az[kSub], bx[kSub], by[kSub], bz[kSub];
+#pragma unroll
+            for (int i = 0; i < kSub; ++i) {
+                ax[i] = sa[k][0][ty * kSub + i];
+                ay[i] = sa[k][1][ty * kSub + i];
+                az[i] = sa[k][2][ty * kSub + i];
+                bx[i] = sb[k][0][tx * kSub + i];
+                by[i] = sb[k][1][tx * kSub + i];
+                bz[i] = sb[k][2][tx * kSub + i];
+            }
+            const uint32_t step = (uint32_t)(a.step_offset + k0 + k);
+#pragma unroll
+            for (int i = 0; i < kSub; ++i)
+#pragma unroll
+                for (int j = 0; j < kSub; ++j) {
+                    const double dx = ax[i] - bx[j];
+                    const double dy = ay[i] - by[j];
+                    const double dz = az[i] - bz[j];
+                    const double d2 = dx * dx + dy * dy + dz * dz;
+                    if (d2 < best[i][j]) {
+                        best[i][j] = d2;
+                        bstep[i][j] = step;
+                    }
+                }
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < kSub; ++i)
+#pragma unroll
+        for (int j = 0; j < kSub; ++j)
+            if (valid[i][j]) {
+                a.min_d2[pidx[i][j]] = best[i][j];
+                a.min_step[pidx[i][j]] = bstep[i][j];
+            }
+}
+
+// ---- TCA refinement: HermitePolynomial / ApproachFunc / FindRoot of interpolation.cuh ----
+struct Herm {
+    double c[9];
+};
+
+// 9-coefficient confluent Hermite polynomial in Newton form through (p, v, a/2) at 0, dt, 2dt
+// (Kincaid & Cheney, ch. 6.3; interpolation.cuh:32-64).
+__device__ __forceinline__ void herm_build(Herm& H, double p0, double v0, double a0, double p1,
+    double v1, double a1, double p2, double v2, double a2, double dt)
+{
+    const double t[9] = { 0.0, 0.0, 0.0, dt, dt, dt, 2.0 * dt, 2.0 * dt, 2.0 * dt };
+    double* c = H.c;
+    c[0] = c[1] = c[2] = p0;
+    c[3] = c[4] = c[5] = p1;
+    c[6] = c[7] = c[8] = p2;
+#pragma unroll
+    for (int j = 1; j < 9; j++)
+#pragma unroll
+        for (int i = 8; i >= j; i--) {
+            if (t[i] == t[i - j]) {
+                if (j == 1)
+                    c[i] = (i < 3) ? v0 : (i < 6) ? v1 : v2;
+                else if (j == 2)
+                    c[i] = ((i < 3) ? a0 : (i < 6) ? a1 : a2) / 2.0;
+            } else {
+                c[i] = (c[i] - c[i - 1]) / (t[i] - t[i - j]);
+            }
+        }
+}
+
+__device__ __forceinline__ double herm_eval(const Herm& H, double dt, double t)
+{
+    const double z[9] = { 0.0, 0.0, 0.0, dt, dt, dt, 2.0 * dt, 2.0 * dt, 2.0 * dt };
+    double res = H.c[0], term = 1.0;
+#pragma unroll
+    for (int i = 1; i < 9; ++i) {
+        term *= (t - z[i - 1]);
+        res += H.c[i] * term;
+    }
+    return res;
+}
+
+__device__ __forceinline__ double herm_deriv(const Herm& H, double dt, double t)
+{
+    const double z[9] = { 0.0, 0.0, 0.0, dt, dt, dt, 2.0 * dt, 2.0 * dt, 2.0 * dt };
+    double res = 0.0, Nn = 1.0, dN = 0.0;
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+        res += H.c[i] * dN;
+        if (i < 8) {
+            dN = dN * (t - z[i]) + Nn;
+            Nn *= (t - z[i]);
+        }
+    }
+    return res;
+}
+
+struct Pair6 {
+    Herm A[3], B[3];
+    double dt;
+    __device__ double f(double t) const // ApproachFunc: (dr . dv)(t)
+    {
+        double s = 0.0;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const double d = herm_eval(A[c], dt, t) - herm_eval(B[c], dt, t);
+            const double dd = herm_deriv(A[c], dt, t) - herm_deriv(B[c], dt, t);
+            s += d * dd;
+        }
+        return s;
+    }
+};
+
+// Secant iteration of FindRoot (interpolation.cuh:126-152): tol 1e-7, at most 100 iterations.
+__device__ double find_root(const Pair6& P, double x0, double x1)
+{
+    const double tol = 1e-7;
+    double f0 = P.f(x0), f1 = P.f(x1);
+    for (int i = 0; i < 100; ++i) {
+        if (fabs(f1 - f0) < 1e-14)
+            return x1;
+        const double xn = x1 - f1 * (x1 - x0) / (f1 - f0);
+        const double fn = P.f(xn);
+        if (fabs(xn - x1) < tol || fabs(fn) < tol)
+            return xn;
+        x0 = x1;
+        f0 = f1;
+        x1 = xn;
+        f1 = fn;
+    }
+    return x1;
+}
+
+__global__ void __launch_bounds__(128) refine_kernel(RefineArgs a)
+{
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= a.num_pairs)
+        return;
+    // pair index -> (a, b): binary search of the set whose map range holds idx
+    // (inverse of PartitionParameters::GetPartitionMapIdx, partition_parameters.cuh:50-91)
+    int lo = 0, hi = a.num_sets - 2;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) / 2;
+        if (a.map_offsets[mid] <= (uint64_t)idx)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    const uint64_t rel = (uint64_t)idx - a.map_offsets[lo];
+    const int64_t oa = (int64_t)(rel / a.num_higher[lo]) + a.set_offsets[lo];
+    const int64_t ob = (int64_t)(rel % a.num_higher[lo]) + a.set_offsets[lo + 1];
+    const uint32_t cs = a.min_step[idx];
+    const int64_t N = a.n;
+    const double h = a.h;
+    double dist = sqrt(a.min_d2[idx]);
+    double tca;
+    double pa[3], pb[3];
+    // CalculateClosestApproachesKernel (device.cu:100-110): minimum on the first or last screened
+    // step is not refined; the sampled positions of that step are reported.
+    if (cs == 0 || cs == a.total_steps - 1 || cs == 0xFFFFFFFFu) {
+        tca = (cs == 0 || cs == 0xFFFFFFFFu) ? 0.0 : (double)a.total_steps * h;
+        const int64_t k = (cs == 0xFFFFFFFFu) ? 0 : cs;
+        for (int c = 0; c < 3; ++c) {
+            pa[c] = a.traj_r[(k * 3 + c) * N + oa];
+            pb[c] = a.traj_r[(k * 3 + c) * N + ob];
+        }
+    } else {
+        Pair6 P;
+        P.dt = h;
+        for (int c = 0; c < 3; ++c) {
+            double q[2][9];
+            for (int node = 0; node < 3; ++node) {
+                const int64_t k = (int64_t)cs - 1 + node;
+                const int64_t ra = (k * 3 + c) * N;
+                q[0][node * 3 + 0] = a.traj_r[ra + oa];
+                q[0][node * 3 + 1] = a.traj_v[ra + oa];
+                q[0][node * 3 + 2] = a.traj_a[ra + oa];
+                q[1][node * 3 + 0] = a.traj_r[ra + ob];
+                q[1][node * 3 + 1] = a.traj_v[ra + ob];
+                q[1][node * 3 + 2] = a.traj_a[ra + ob];
+            }
+            herm_build(P.A[c], q[0][0], q[0][1], q[0][2], q[0][3], q[0][4], q[0][5], q[0][6],
+                q[0][7], q[0][8], h);
+            herm_build(P.B[c], q[1][0], q[1][1], q[1][2], q[1][3], q[1][4], q[1][5], q[1][6],
+                q[1][7], q[1][8], h);
+        }
+        const double t = find_root(P, 0.0, h);
+        tca = t + (double)cs * h;
+        double d2 = 0.0;
+        for (int c = 0; c < 3; ++c) {
+            pa[c] = herm_eval(P.A[c], h, t);
+            pb[c] = herm_eval(P.B[c], h, t);
+            const double d = pa[c] - pb[c];
+            d2 += d * d;
+        }
+        dist = sqrt(d2);
+    }
+    a.dist[idx] = dist;
+    a.time[idx] = tca;
+    for (int c = 0; c < 3; ++c) {
+        a.pos_a[idx * 3 + c] = pa[c];
+        a.pos_b[idx * 3 + c] = pb[c];
+    }
+}
+
+// Pairs whose refined distance is below the threshold, appended in any order.
+__global__ void select_kernel(const double* dist, int64_t num_pairs, double threshold,
+    unsigned long long* count, int64_t* out, int64_t capacity)
+{
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= num_pairs)
+        return;
+    if (dist[idx] < threshold) {
+        const unsigned long long slot = atomicAdd(count, 1ull);
+        if ((int64_t)slot < capacity)
+            out[slot] = idx;
+    }
+}
+
+cudaError_t launch_screen(const ScreenArgs& a, int num_tiles, cudaStream_t s)
+{
+    if (num_tiles <= 0 || a.step_hi <= a.step_lo)
+        return cudaSuccess;
+    screen_kernel<<<num_tiles, 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_refine(const RefineArgs& a, cudaStream_t s)
+{
+    if (a.num_pairs <= 0)
+        return cudaSuccess;
+    const int64_t blocks = (a.num_pairs + 127) / 128;
+    refine_kernel<<<(unsigned)blocks, 128, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_select(const double* dist, int64_t num_pairs, double threshold,
+    unsigned long long* count, int64_t* out, int64_t capacity, cudaStream_t s)
+{
+    if (num_pairs <= 0)
+        return cudaSuccess;
+    select_kernel<<<(unsigned)((num_pairs + 255) / 256), 256, 0, s>>>(dist, num_pairs, threshold,
+        count, out, capacity);
+    return cudaGetLastError();
+}
+
+} // namespace gpop
