@@ -1,18 +1,20 @@
 // gravity.cuh -- fused normalised spherical-harmonic gravity (Gottlieb's derived-Legendre method,
-// as in lib/force_model/src/acceleration/gravity_source_device.cu:63-239), one object per thread.
+// as in lib/force_model/src/acceleration/gravity_source_device.cu:63-239) for K objects per thread.
 //
 // The reference builds the whole P-bar triangle, four N x T term arrays and two Thrust segment
 // reductions in HBM per evaluation (about 25 launches). Here each thread walks the triangle column
 // by column with a two-term recursion held in registers, reading the pre-scaled coefficient table
-// from shared memory by broadcast (every lane of a warp reads the same entry). Per (n, m) term:
-// 3 FP64 ops for the recursion and 6 FMAs into per-column sums; per column the sums are combined
-// with the cos/sin(m lambda) recursion of eq. 3-18. The (R/r)^n factor of eq. 4-12 rides in the
-// recursion variable, so no per-degree sums are needed.
+// from shared memory by broadcast (every lane of a warp reads the same entry). Per (n, m) term and
+// object: 3 FP64 ops for the recursion and 6 FMAs into per-column sums; per column the sums are
+// combined with the cos/sin(m lambda) recursion of eq. 3-18. The (R/r)^n factor of eq. 4-12 rides
+// in the recursion variable, so no per-degree sums are needed. With K objects per thread every
+// table entry loaded from shared memory feeds K independent chains.
 //
 // Mixed precision: terms of degree n <= 8 (and all per-column combining, the central term, frame
 // rotations and the final assembly) stay FP64; the n > 8 recursion and sums run in FP32 with
-// packed f32x2 FMAs, per column, and each column's FP32 sums are added into the FP64 totals
-// (two-level summation: at most 62 FP32 terms per partial sum).
+// packed f32x2 FMAs (for K = 2 the recursion of the two objects shares one packed instruction),
+// per column, and each column's FP32 sums are added into the FP64 totals (two-level summation: at
+// most 62 FP32 terms per partial sum).
 #pragma once
 #include "common.cuh"
 #include "model.h"
@@ -23,157 +25,283 @@ constexpr int kMixedSplit = 8; // highest degree kept in FP64 in the mixed mode
 
 struct GravSmem {
     const GravEntry64* t64; // FP64 mode: full table; mixed mode: head table (n <= 8)
-    const GravEntry32* t32; // mixed mode: full FP32 table
+    const GravEntry32* t32; // mixed mode: full FP32 table (recursion constant stored negated, twice)
     int L;
     double radius, gm;
 };
 
-__device__ __forceinline__ void col_accum64(const GravEntry64* __restrict__ e, double Q, double& g1,
-    double& g2, double& j1, double& j2, double& h1, double& h2)
-{
-    const double2* p = reinterpret_cast<const double2*>(e);
-    double2 g = p[1], j = p[2], h = p[3];
-    g1 = fma(g.x, Q, g1);
-    g2 = fma(g.y, Q, g2);
-    j1 = fma(j.x, Q, j1);
-    j2 = fma(j.y, Q, j2);
-    h1 = fma(h.x, Q, h1);
-    h2 = fma(h.y, Q, h2);
-}
+template <int K> struct ColSums64 {
+    double g1[K], g2[K], j1[K], j2[K], h1[K], h2[K];
+    __device__ __forceinline__ void zero()
+    {
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+            g1[k] = g2[k] = j1[k] = j2[k] = h1[k] = h2[k] = 0.0;
+    }
+    __device__ __forceinline__ void add(const GravEntry64* __restrict__ e, const double (&Q)[K])
+    {
+        const double2* p = reinterpret_cast<const double2*>(e);
+        const double2 g = p[1], j = p[2], h = p[3];
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            g1[k] = fma(g.x, Q[k], g1[k]);
+            g2[k] = fma(g.y, Q[k], g2[k]);
+            j1[k] = fma(j.x, Q[k], j1[k]);
+            j2[k] = fma(j.y, Q[k], j2[k]);
+            h1[k] = fma(h.x, Q[k], h1[k]);
+            h2[k] = fma(h.y, Q[k], h2[k]);
+        }
+    }
+};
 
-// Walks column entries e[first..last] (n = m + first .. m + last) in FP64, continuing the
-// recursion from (Q1, Q2) = (Q(n-1), Q(n-2)).
+// Walks column entries e[first..last] in FP64, continuing the recursion from Q1 = Q(n-1),
+// Q2 = Q(n-2) of each object.
+template <int K>
 __device__ __forceinline__ void column64(const GravEntry64* __restrict__ e, int first, int last,
-    double u, double w, double& Q1, double& Q2, double& g1, double& g2, double& j1, double& j2,
-    double& h1, double& h2)
+    const double (&u)[K], const double (&w)[K], double (&Q1)[K], double (&Q2)[K], ColSums64<K>& s)
 {
 #pragma unroll 2
-    for (int k = first; k <= last; ++k) {
-        double c = reinterpret_cast<const double2*>(e + k)[0].x;
-        double Q = fma(u, Q1, -(c * w) * Q2);
-        col_accum64(e + k, Q, g1, g2, j1, j2, h1, h2);
-        Q2 = Q1;
-        Q1 = Q;
+    for (int i = first; i <= last; ++i) {
+        const double c = reinterpret_cast<const double2*>(e + i)[0].x;
+        double Q[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            Q[k] = fma(u[k], Q1[k], -(c * w[k]) * Q2[k]);
+            Q2[k] = Q1[k];
+            Q1[k] = Q[k];
+        }
+        s.add(e + i, Q);
     }
 }
+
+// FP32 column walk; the table holds (-c, -c, g1, g2 | j1, j2, h1, h2).
+template <int K> struct ColSums32 {
+    float2 g[K], j[K], h[K];
+    __device__ __forceinline__ void zero()
+    {
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+            g[k] = j[k] = h[k] = make_float2(0.f, 0.f);
+    }
+};
 
 __device__ __forceinline__ void column32(const GravEntry32* __restrict__ e, int first, int last,
-    float u, float w, float& Q1, float& Q2, float2& g, float2& j, float2& h)
+    float u, float w, float& Q1, float& Q2, ColSums32<1>& s)
 {
 #pragma unroll 2
-    for (int k = first; k <= last; ++k) {
-        const float4* p = reinterpret_cast<const float4*>(e + k);
-        float4 a = p[0]; // c, pad, g1, g2
-        float4 b = p[1]; // j1, j2, h1, h2
-        float Q = fmaf(u, Q1, -(a.x * w) * Q2);
-        float2 QQ = make_float2(Q, Q);
-        g = __ffma2_rn(QQ, make_float2(a.z, a.w), g);
-        j = __ffma2_rn(QQ, make_float2(b.x, b.y), j);
-        h = __ffma2_rn(QQ, make_float2(b.z, b.w), h);
+    for (int i = first; i <= last; ++i) {
+        const float4* p = reinterpret_cast<const float4*>(e + i);
+        const float4 a = p[0], b = p[1];
+        const float Q = fmaf(u, Q1, (a.x * w) * Q2);
+        const float2 QQ = make_float2(Q, Q);
+        s.g[0] = __ffma2_rn(QQ, make_float2(a.z, a.w), s.g[0]);
+        s.j[0] = __ffma2_rn(QQ, make_float2(b.x, b.y), s.j[0]);
+        s.h[0] = __ffma2_rn(QQ, make_float2(b.z, b.w), s.h[0]);
         Q2 = Q1;
         Q1 = Q;
     }
 }
 
-// Acceleration in the Earth-fixed frame (eq. 4-13 of gravity_source_device.cu:212-239).
-template <bool MIXED>
-__device__ __forceinline__ void gravity_itrs(const GravSmem& gs, double x, double y, double z,
-    double& ax, double& ay, double& az)
+// Two objects: the recursion of both objects is one packed chain (Q = (Q_A, Q_B)).
+__device__ __forceinline__ void column32x2(const GravEntry32* __restrict__ e, int first, int last,
+    float2 u, float2 w, float2& Q1, float2& Q2, ColSums32<2>& s)
+{
+#pragma unroll 2
+    for (int i = first; i <= last; ++i) {
+        const float4* p = reinterpret_cast<const float4*>(e + i);
+        const float4 a = p[0], b = p[1];
+        const float2 t = __fmul2_rn(make_float2(a.x, a.y), w);
+        const float2 Q = __ffma2_rn(u, Q1, __fmul2_rn(t, Q2));
+        const float2 QA = make_float2(Q.x, Q.x), QB = make_float2(Q.y, Q.y);
+        const float2 cg = make_float2(a.z, a.w), cj = make_float2(b.x, b.y), ch = make_float2(b.z, b.w);
+        s.g[0] = __ffma2_rn(QA, cg, s.g[0]);
+        s.j[0] = __ffma2_rn(QA, cj, s.j[0]);
+        s.h[0] = __ffma2_rn(QA, ch, s.h[0]);
+        s.g[1] = __ffma2_rn(QB, cg, s.g[1]);
+        s.j[1] = __ffma2_rn(QB, cj, s.j[1]);
+        s.h[1] = __ffma2_rn(QB, ch, s.h[1]);
+        Q2 = Q1;
+        Q1 = Q;
+    }
+}
+
+template <int K>
+__device__ __forceinline__ void column32k(const GravEntry32* __restrict__ e, int first, int last,
+    const float (&u)[K], const float (&w)[K], float (&Q1)[K], float (&Q2)[K], ColSums32<K>& s)
+{
+    if constexpr (K == 1) {
+        column32(e, first, last, u[0], w[0], Q1[0], Q2[0], s);
+    } else {
+        static_assert(K == 2, "FP32 path packs one or two objects");
+        float2 U = make_float2(u[0], u[1]), W = make_float2(w[0], w[1]);
+        float2 A = make_float2(Q1[0], Q1[1]), B = make_float2(Q2[0], Q2[1]);
+        column32x2(e, first, last, U, W, A, B, s);
+        Q1[0] = A.x;
+        Q1[1] = A.y;
+        Q2[0] = B.x;
+        Q2[1] = B.y;
+    }
+}
+
+// Accelerations of K objects in the Earth-fixed frame (eq. 4-13 of gravity_source_device.cu:212-239).
+template <bool MIXED, int K>
+__device__ __forceinline__ void gravity_itrs(const GravSmem& gs, const double (&x)[K],
+    const double (&y)[K], const double (&z)[K], double (&ax)[K], double (&ay)[K], double (&az)[K])
 {
     const int L = gs.L;
-    const double r = sqrt(x * x + y * y + z * z);
-    const double eps = z / r; // eq. 3-3
-    const double q = gs.radius / r;
-    const double u = q * eps;
-    const double w = q * q;
-    const double C1 = x / r, S1 = y / r; // eq. 3-18 seeds
-    double Cm = 1.0, Sm = 0.0, Cp = 0.0, Sp = 0.0; // C_m, S_m and C_{m-1}, S_{m-1}
-    double qm = 1.0; // q^m
-    double G = 0.0, H = 0.0, J = 0.0, K = 0.0;
-    const float uf = (float)u, wf = (float)w;
+    double r[K], q[K], u[K], w[K], C1[K], S1[K], Cm[K], Sm[K], Cp[K], Sp[K], qm[K];
+    double G[K], H[K], J[K], KK[K];
+    float uf[K], wf[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        r[k] = sqrt(x[k] * x[k] + y[k] * y[k] + z[k] * z[k]);
+        const double eps = z[k] / r[k]; // eq. 3-3
+        q[k] = gs.radius / r[k];
+        u[k] = q[k] * eps;
+        w[k] = q[k] * q[k];
+        C1[k] = x[k] / r[k]; // eq. 3-18 seeds
+        S1[k] = y[k] / r[k];
+        Cm[k] = 1.0;
+        Sm[k] = 0.0;
+        Cp[k] = 0.0;
+        Sp[k] = 0.0;
+        qm[k] = 1.0;
+        G[k] = H[k] = J[k] = KK[k] = 0.0;
+        uf[k] = (float)u[k];
+        wf[k] = (float)w[k];
+    }
     for (int m = 0; m <= L; ++m) {
-        double g1 = 0, g2 = 0, j1 = 0, j2 = 0, h1 = 0, h2 = 0;
-        double Q1 = qm, Q2 = 0.0;
-        if (!MIXED) {
+        ColSums64<K> s;
+        s.zero();
+        double Q1[K], Q2[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            Q1[k] = qm[k];
+            Q2[k] = 0.0;
+        }
+        if constexpr (!MIXED) {
             const GravEntry64* e = gs.t64 + grav_col_offset(m, L);
-            col_accum64(e, Q1, g1, g2, j1, j2, h1, h2); // n = m
-            column64(e, 1, L - m, u, w, Q1, Q2, g1, g2, j1, j2, h1, h2);
+            s.add(e, Q1); // n = m
+            column64<K>(e, 1, L - m, u, w, Q1, Q2, s);
         } else {
-            float2 fg = make_float2(0.f, 0.f), fj = fg, fh = fg;
+            ColSums32<K> f;
+            f.zero();
             const GravEntry32* e32 = gs.t32 + grav_col_offset(m, L);
+            float Q1f[K], Q2f[K];
             if (m <= kMixedSplit) {
                 const int top = L < kMixedSplit ? L : kMixedSplit;
                 const GravEntry64* e = gs.t64 + grav_col_offset(m, kMixedSplit);
-                col_accum64(e, Q1, g1, g2, j1, j2, h1, h2);
-                column64(e, 1, top - m, u, w, Q1, Q2, g1, g2, j1, j2, h1, h2);
-                float Q1f = (float)Q1, Q2f = (float)Q2;
-                column32(e32, kMixedSplit + 1 - m, L - m, uf, wf, Q1f, Q2f, fg, fj, fh);
+                s.add(e, Q1);
+                column64<K>(e, 1, top - m, u, w, Q1, Q2, s);
+#pragma unroll
+                for (int k = 0; k < K; ++k) {
+                    Q1f[k] = (float)Q1[k];
+                    Q2f[k] = (float)Q2[k];
+                }
+                column32k<K>(e32, kMixedSplit + 1 - m, L - m, uf, wf, Q1f, Q2f, f);
             } else {
-                float Q1f = (float)qm, Q2f = 0.f;
+                // n = m term (Q = q^m), then the rest of the column with Q(m-1, m) = 0
                 const float4* p = reinterpret_cast<const float4*>(e32);
-                float4 a = p[0], b = p[1];
-                float2 QQ = make_float2(Q1f, Q1f);
-                fg = __ffma2_rn(QQ, make_float2(a.z, a.w), fg);
-                fj = __ffma2_rn(QQ, make_float2(b.x, b.y), fj);
-                fh = __ffma2_rn(QQ, make_float2(b.z, b.w), fh);
-                column32(e32, 1, L - m, uf, wf, Q1f, Q2f, fg, fj, fh);
+                const float4 a = p[0], b = p[1];
+#pragma unroll
+                for (int k = 0; k < K; ++k) {
+                    const float Qm = (float)qm[k];
+                    const float2 QQ = make_float2(Qm, Qm);
+                    f.g[k] = __ffma2_rn(QQ, make_float2(a.z, a.w), f.g[k]);
+                    f.j[k] = __ffma2_rn(QQ, make_float2(b.x, b.y), f.j[k]);
+                    f.h[k] = __ffma2_rn(QQ, make_float2(b.z, b.w), f.h[k]);
+                    Q1f[k] = Qm;
+                    Q2f[k] = 0.f;
+                }
+                column32k<K>(e32, 1, L - m, uf, wf, Q1f, Q2f, f);
             }
-            g1 += (double)fg.x;
-            g2 += (double)fg.y;
-            j1 += (double)fj.x;
-            j2 += (double)fj.y;
-            h1 += (double)fh.x;
-            h2 += (double)fh.y;
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                s.g1[k] += (double)f.g[k].x;
+                s.g2[k] += (double)f.g[k].y;
+                s.j1[k] += (double)f.j[k].x;
+                s.j2[k] += (double)f.j[k].y;
+                s.h1[k] += (double)f.h[k].x;
+                s.h2[k] += (double)f.h[k].y;
+            }
         }
         // eq. 4-11 per column: G with (C_m, S_m); J, K, H with (C_{m-1}, S_{m-1})
         const double dm = (double)m;
-        G += Cm * g1 + Sm * g2;
-        J += dm * (Cp * j1 + Sp * j2);
-        K -= dm * (Sp * j1 - Cp * j2);
-        H += Cp * h1 + Sp * h2;
-        Cp = Cm;
-        Sp = Sm;
-        const double Cn = C1 * Cm - S1 * Sm;
-        const double Sn = S1 * Cm + C1 * Sm;
-        Cm = Cn;
-        Sm = Sn;
-        qm *= q;
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            G[k] += Cm[k] * s.g1[k] + Sm[k] * s.g2[k];
+            J[k] += dm * (Cp[k] * s.j1[k] + Sp[k] * s.j2[k]);
+            KK[k] -= dm * (Sp[k] * s.j1[k] - Cp[k] * s.j2[k]);
+            H[k] += Cp[k] * s.h1[k] + Sp[k] * s.h2[k];
+            Cp[k] = Cm[k];
+            Sp[k] = Sm[k];
+            const double Cn = C1[k] * Cm[k] - S1[k] * Sm[k];
+            const double Sn = S1[k] * Cm[k] + C1[k] * Sm[k];
+            Cm[k] = Cn;
+            Sm[k] = Sn;
+            qm[k] *= q[k];
+        }
     }
-    // eq. 4-13
-    G = G + 1.0;
-    const double Lambda = G + z * H / r;
-    const double c = -gs.gm / (r * r);
-    ax = c * (Lambda * x / r - J);
-    ay = c * (Lambda * y / r - K);
-    az = c * (Lambda * z / r - H);
+#pragma unroll
+    for (int k = 0; k < K; ++k) { // eq. 4-13
+        const double Gk = G[k] + 1.0;
+        const double Lambda = Gk + z[k] * H[k] / r[k];
+        const double c = -gs.gm / (r[k] * r[k]);
+        ax[k] = c * (Lambda * x[k] / r[k] - J[k]);
+        ay[k] = c * (Lambda * y[k] / r[k] - KK[k]);
+        az[k] = c * (Lambda * z[k] / r[k] - H[k]);
+    }
 }
 
-// GCRS acceleration at GCRS position r with the ITRS->GCRS matrix M (column-major, 9 doubles):
-// r_itrs = M^T r, a = M a_itrs (the two cublasDgemvStridedBatched of gravity_source.cu:176-210).
-template <bool MIXED>
+// GCRS accelerations of K objects at GCRS positions r[k] with the ITRS->GCRS matrix M
+// (column-major): r_itrs = M^T r, a = M a_itrs (the two cublasDgemvStridedBatched of
+// gravity_source.cu:176-210).
+template <bool MIXED, int K>
 __device__ __forceinline__ void gravity_gcrs(const GravSmem& gs, const double* __restrict__ M,
-    const double* r, double* a)
+    const double (&r)[K][3], double (&a)[K][3])
 {
     double m[9];
 #pragma unroll
     for (int i = 0; i < 9; ++i)
         m[i] = __ldg(M + i);
-    const double px = m[0] * r[0] + m[1] * r[1] + m[2] * r[2];
-    const double py = m[3] * r[0] + m[4] * r[1] + m[5] * r[2];
-    const double pz = m[6] * r[0] + m[7] * r[1] + m[8] * r[2];
-    double ax, ay, az;
-    gravity_itrs<MIXED>(gs, px, py, pz, ax, ay, az);
-    a[0] = m[0] * ax + m[3] * ay + m[6] * az;
-    a[1] = m[1] * ax + m[4] * ay + m[7] * az;
-    a[2] = m[2] * ax + m[5] * ay + m[8] * az;
+    double px[K], py[K], pz[K], ax[K], ay[K], az[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        px[k] = m[0] * r[k][0] + m[1] * r[k][1] + m[2] * r[k][2];
+        py[k] = m[3] * r[k][0] + m[4] * r[k][1] + m[5] * r[k][2];
+        pz[k] = m[6] * r[k][0] + m[7] * r[k][1] + m[8] * r[k][2];
+    }
+    gravity_itrs<MIXED, K>(gs, px, py, pz, ax, ay, az);
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        a[k][0] = m[0] * ax[k] + m[3] * ay[k] + m[6] * az[k];
+        a[k][1] = m[1] * ax[k] + m[4] * ay[k] + m[7] * az[k];
+        a[k][2] = m[2] * ax[k] + m[5] * ay[k] + m[8] * az[k];
+    }
 }
 
-__device__ __forceinline__ void gravity_identity_fp64(const GravSmem& gs, const double* r, double* a, bool mixed)
+// One object (startup, single-evaluation and unit kernels).
+template <bool MIXED>
+__device__ __forceinline__ void gravity_gcrs1(const GravSmem& gs, const double* __restrict__ M,
+    const double* r, double* a)
 {
-    if (mixed)
-        gravity_itrs<true>(gs, r[0], r[1], r[2], a[0], a[1], a[2]);
-    else
-        gravity_itrs<false>(gs, r[0], r[1], r[2], a[0], a[1], a[2]);
+    double rr[1][3] = { { r[0], r[1], r[2] } };
+    double aa[1][3];
+    gravity_gcrs<MIXED, 1>(gs, M, rr, aa);
+    a[0] = aa[0][0];
+    a[1] = aa[0][1];
+    a[2] = aa[0][2];
+}
+
+template <bool MIXED>
+__device__ __forceinline__ void gravity_itrs1(const GravSmem& gs, double x, double y, double z,
+    double& ax, double& ay, double& az)
+{
+    double X[1] = { x }, Y[1] = { y }, Z[1] = { z }, AX[1], AY[1], AZ[1];
+    gravity_itrs<MIXED, 1>(gs, X, Y, Z, AX, AY, AZ);
+    ax = AX[0];
+    ay = AY[0];
+    az = AZ[0];
 }
 
 } // namespace gpop

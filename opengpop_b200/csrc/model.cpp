@@ -236,7 +236,7 @@ void build_gravity_tables(const ModelData& md, std::vector<GravEntry64>& t64, st
                 }
             }
             GravEntry32& f = t32[grav_col_offset(m, L) + (n - m)];
-            f.c = (float)e.c;
+            f.c = f.pad = (float)(-e.c); // the FP32 walk adds (-c w) Q(n-2), packed in pairs
             f.g1 = (float)e.g1;
             f.g2 = (float)e.g2;
             f.j1 = (float)e.j1;

@@ -50,6 +50,8 @@ bool load_model(const std::string& dir, int degree, ModelData& out, std::string&
 struct alignas(16) GravEntry64 {
     double c, pad, g1, g2, j1, j2, h1, h2;
 };
+// FP32 entry: the recursion constant is stored negated, twice ((-c, -c) is the packed operand of
+// the two-object recursion).
 struct alignas(16) GravEntry32 {
     float c, pad, g1, g2, j1, j2, h1, h2;
 };

@@ -21,13 +21,19 @@ template <bool MIXED> struct ForceGravity {
     // ForceModel::ComputePropagationAcceleration (force_model.cu:91-109): epoch index idx
     __device__ __forceinline__ void prop(const double* r, const double*, int idx, double* a) const
     {
-        gravity_gcrs<MIXED>(g, prop_m + (size_t)idx * 9, r, a);
+        gravity_gcrs1<MIXED>(g, prop_m + (size_t)idx * 9, r, a);
+    }
+    template <int K>
+    __device__ __forceinline__ void prop_k(const double (&r)[K][3], const double (&)[K][3], int idx,
+        double (&a)[K][3]) const
+    {
+        gravity_gcrs<MIXED, K>(g, prop_m + (size_t)idx * 9, r, a);
     }
     // ForceModel::ComputeGenerationAcceleration (force_model.cu:59-89): table (s'+4)*10 + k
     __device__ __forceinline__ void gen(const double* r, const double*, int step, int k, double* a) const
     {
         const int s = step > 0 ? step - 1 : step;
-        gravity_gcrs<MIXED>(g, gen_m + (size_t)((s + 4) * 10 + k) * 9, r, a);
+        gravity_gcrs1<MIXED>(g, gen_m + (size_t)((s + 4) * 10 + k) * 9, r, a);
     }
 };
 
@@ -72,6 +78,14 @@ struct ForceAnalytic {
     __device__ __forceinline__ void prop(const double* r, const double* v, int idx, double* a) const
     {
         eval(r, v, (double)(idx - 4) * h, a);
+    }
+    template <int K>
+    __device__ __forceinline__ void prop_k(const double (&r)[K][3], const double (&v)[K][3], int idx,
+        double (&a)[K][3]) const
+    {
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+            eval(r[k], v[k], (double)(idx - 4) * h, a[k]);
     }
     __device__ __forceinline__ void gen(const double* r, const double* v, int step, int k, double* a) const
     {
@@ -273,111 +287,147 @@ __global__ void __launch_bounds__(256) startup_kernel(F f, TableSrc ts, PropArgs
 }
 
 // ---- GJ8 step (prediction.cu:49-74 + gpu_propagator.cu:86-119) ----
-template <class F>
-__global__ void __launch_bounds__(512, 1) gj8_kernel(F f, TableSrc ts, PropArgs a)
+// K objects per thread: object k of thread g is g + k * (threads in the grid); every gravity
+// evaluation of a step runs the K objects in lockstep on the same table entries.
+template <class F, int K>
+__global__ void __launch_bounds__(K == 1 ? 512 : 256, 1) gj8_kernel(F f, TableSrc ts, PropArgs a)
 {
     extern __shared__ __align__(128) uint8_t smem[];
     if constexpr (F::kTable) {
         if (!bind_table<std::is_same<F, ForceGravity<true>>::value>(smem, ts, a.err, f.g))
             return;
     }
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= a.n)
-        return;
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t G = (int64_t)gridDim.x * blockDim.x;
     const int64_t n = a.n;
+    if (g >= n)
+        return;
+    int64_t obj[K];
+    bool live[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        const int64_t o = g + k * G;
+        live[k] = o < n;
+        obj[k] = live[k] ? o : g; // idle slots shadow object g and never store
+    }
     double* st = a.state;
     const double h = a.h;
-    double r[3], v[3], s[3], S[3];
-    for (int j = 0; j < 3; ++j) {
-        r[j] = st[(kR + j) * n + i];
-        v[j] = st[(kV + j) * n + i];
-        s[j] = st[(kSs + j) * n + i];
-        S[j] = st[(kSb + j) * n + i];
-    }
+    double r[K][3], v[K][3], s[K][3], S[K][3];
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            r[k][j] = st[(kR + j) * n + obj[k]];
+            v[k][j] = st[(kV + j) * n + obj[k]];
+            s[k][j] = st[(kSs + j) * n + obj[k]];
+            S[k][j] = st[(kSb + j) * n + obj[k]];
+        }
     for (int step = a.step_begin; step < a.step_end; ++step) {
-        double ae[3];
+        double ae[K][3];
         if (step <= 4) {
-            for (int j = 0; j < 3; ++j) {
-                r[j] = st[(kRep + (step - 1) * 6 + j) * n + i];
-                v[j] = st[(kRep + (step - 1) * 6 + 3 + j) * n + i];
-                ae[j] = st[(kRepA + (step - 1) * 3 + j) * n + i];
-            }
+#pragma unroll
+            for (int k = 0; k < K; ++k)
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    r[k][j] = st[(kRep + (step - 1) * 6 + j) * n + obj[k]];
+                    v[k][j] = st[(kRep + (step - 1) * 6 + 3 + j) * n + obj[k]];
+                    ae[k][j] = st[(kRepA + (step - 1) * 3 + j) * n + obj[k]];
+                }
         } else {
             const int ring0 = (step - 5) % 9;
-            double hist[9][3];
+            double s1[K][3], s2[K][3], prev[K][3], a7[K][3], a8[K][3];
 #pragma unroll
-            for (int k = 0; k < 9; ++k) {
-                int slot = ring0 + k;
-                slot -= slot >= 9 ? 9 : 0;
+            for (int k = 0; k < K; ++k) {
+                double hist[9][3];
 #pragma unroll
-                for (int j = 0; j < 3; ++j)
-                    hist[k][j] = st[(kHist + slot * 3 + j) * n + i];
-            }
-            // Predictor (FinalizePredictionKernel, gpu_integrator/src/device/dev_functions.cu:34-50)
-            double s1[3], s2[3], prev[3], a7[3], a8[3];
+                for (int c = 0; c < 9; ++c) {
+                    int slot = ring0 + c;
+                    slot -= slot >= 9 ? 9 : 0;
 #pragma unroll
-            for (int j = 0; j < 3; ++j) {
-                double vt = 0.0, rt = 0.0;
-#pragma unroll
-                for (int k = 0; k < 9; ++k) {
-                    vt = fma(hist[k][j], c_SA[9][k], vt);
-                    rt = fma(hist[k][j], c_GJ[9][k], rt);
+                    for (int j = 0; j < 3; ++j)
+                        hist[c][j] = st[(kHist + slot * 3 + j) * n + obj[k]];
                 }
-                S[j] += s[j] + hist[8][j] / 2;
-                v[j] = (vt + s[j] + hist[8][j] / 2) * h;
-                r[j] = (rt + S[j]) * h * h;
-                // corrector partial sums over the shifted history (gpu_propagator.cu:92-100)
-                double c1 = 0.0, c2 = 0.0;
+                // Predictor (FinalizePredictionKernel, gpu_integrator/src/device/dev_functions.cu:34-50)
 #pragma unroll
-                for (int k = 0; k < 8; ++k) {
-                    c1 = fma(hist[k + 1][j], c_SA[8][k], c1);
-                    c2 = fma(hist[k + 1][j], c_GJ[8][k], c2);
+                for (int j = 0; j < 3; ++j) {
+                    double vt = 0.0, rt = 0.0;
+#pragma unroll
+                    for (int c = 0; c < 9; ++c) {
+                        vt = fma(hist[c][j], c_SA[9][c], vt);
+                        rt = fma(hist[c][j], c_GJ[9][c], rt);
+                    }
+                    S[k][j] += s[k][j] + hist[8][j] / 2;
+                    v[k][j] = (vt + s[k][j] + hist[8][j] / 2) * h;
+                    r[k][j] = (rt + S[k][j]) * h * h;
+                    // corrector partial sums over the shifted history (gpu_propagator.cu:92-100)
+                    double c1 = 0.0, c2 = 0.0;
+#pragma unroll
+                    for (int c = 0; c < 8; ++c) {
+                        c1 = fma(hist[c + 1][j], c_SA[8][c], c1);
+                        c2 = fma(hist[c + 1][j], c_GJ[8][c], c2);
+                    }
+                    s1[k][j] = c1;
+                    s2[k][j] = c2;
+                    prev[k][j] = s[k][j];
+                    a7[k][j] = hist[8][j];
                 }
-                s1[j] = c1;
-                s2[j] = c2;
-                prev[j] = s[j];
-                a7[j] = hist[8][j];
             }
             const int idx = step + 4;
-            f.prop(r, v, idx, a8);
+            f.template prop_k<K>(r, v, idx, a8);
             // Corrector: the first pass reuses the predictor's evaluation at the unchanged
             // position (bit-identical to the reference's repeated call).
             for (int it = 0; it < a.ncorr; ++it) {
                 if (it > 0)
-                    f.prop(r, v, idx, a8);
+                    f.template prop_k<K>(r, v, idx, a8);
+#pragma unroll
+                for (int k = 0; k < K; ++k)
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) {
+                        s[k][j] = prev[k][j] + (a8[k][j] + a7[k][j]) / 2;
+                        v[k][j] = h * (s1[k][j] + a8[k][j] * c_SA[8][8] + s[k][j]);
+                        r[k][j] = h * h * (s2[k][j] + a8[k][j] * c_GJ[8][8] + S[k][j]);
+                    }
+            }
+#pragma unroll
+            for (int k = 0; k < K; ++k)
 #pragma unroll
                 for (int j = 0; j < 3; ++j) {
-                    s[j] = prev[j] + (a8[j] + a7[j]) / 2;
-                    v[j] = h * (s1[j] + a8[j] * c_SA[8][8] + s[j]);
-                    r[j] = h * h * (s2[j] + a8[j] * c_GJ[8][8] + S[j]);
+                    if (live[k])
+                        st[(kHist + ring0 * 3 + j) * n + obj[k]] = a8[k][j];
+                    ae[k][j] = a8[k][j];
                 }
-            }
-#pragma unroll
-            for (int j = 0; j < 3; ++j) {
-                st[(kHist + ring0 * 3 + j) * n + i] = a8[j];
-                ae[j] = a8[j];
-            }
         }
         const int64_t t = step - a.traj_step0;
-        if (a.traj_r)
-            for (int j = 0; j < 3; ++j)
-                a.traj_r[(t * 3 + j) * n + i] = r[j];
-        if (a.traj_v)
-            for (int j = 0; j < 3; ++j)
-                a.traj_v[(t * 3 + j) * n + i] = v[j];
-        if (a.traj_a)
-            for (int j = 0; j < 3; ++j)
-                a.traj_a[(t * 3 + j) * n + i] = ae[j];
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            if (!live[k])
+                continue;
+            if (a.traj_r)
+                for (int j = 0; j < 3; ++j)
+                    a.traj_r[(t * 3 + j) * n + obj[k]] = r[k][j];
+            if (a.traj_v)
+                for (int j = 0; j < 3; ++j)
+                    a.traj_v[(t * 3 + j) * n + obj[k]] = v[k][j];
+            if (a.traj_a)
+                for (int j = 0; j < 3; ++j)
+                    a.traj_a[(t * 3 + j) * n + obj[k]] = ae[k][j];
+        }
     }
-    for (int j = 0; j < 3; ++j) {
-        st[(kR + j) * n + i] = r[j];
-        st[(kV + j) * n + i] = v[j];
-        st[(kSs + j) * n + i] = s[j];
-        st[(kSb + j) * n + i] = S[j];
-        if (a.out_r)
-            a.out_r[i * 3 + j] = r[j];
-        if (a.out_v)
-            a.out_v[i * 3 + j] = v[j];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        if (!live[k])
+            continue;
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            st[(kR + j) * n + obj[k]] = r[k][j];
+            st[(kV + j) * n + obj[k]] = v[k][j];
+            st[(kSs + j) * n + obj[k]] = s[k][j];
+            st[(kSb + j) * n + obj[k]] = S[k][j];
+            if (a.out_r)
+                a.out_r[obj[k] * 3 + j] = r[k][j];
+            if (a.out_v)
+                a.out_v[obj[k] * 3 + j] = v[k][j];
+        }
     }
 }
 
@@ -395,9 +445,9 @@ __global__ void __launch_bounds__(512, 1) gravity_kernel(TableSrc ts, int64_t n,
     double p[3] = { r[i * 3], r[i * 3 + 1], r[i * 3 + 2] };
     double acc[3];
     if (m9) {
-        gravity_gcrs<MIXED>(g, m9, p, acc);
+        gravity_gcrs1<MIXED>(g, m9, p, acc);
     } else {
-        gravity_itrs<MIXED>(g, p[0], p[1], p[2], acc[0], acc[1], acc[2]);
+        gravity_itrs1<MIXED>(g, p[0], p[1], p[2], acc[0], acc[1], acc[2]);
     }
     a[i * 3] = acc[0];
     a[i * 3 + 1] = acc[1];
@@ -518,39 +568,57 @@ cudaError_t launch_startup(const TableSrc& ts, const PropArgs& a, int num_sms, c
     return cudaGetLastError();
 }
 
-cudaError_t launch_gj8(const TableSrc& ts, const PropArgs& a, int num_sms, cudaStream_t s, int block_override)
+template <class F, int K>
+static cudaError_t launch_gj8_k(F f, const TableSrc& ts, const PropArgs& a, int num_sms,
+    cudaStream_t s, int block_override)
+{
+    const int64_t threads = (a.n + K - 1) / K;
+    LaunchShape ls = pick_shape(threads, K == 1 ? 512 : 256, num_sms);
+    if (block_override > 0) {
+        ls.block = block_override;
+        ls.grid = (int)((threads + block_override - 1) / block_override);
+    }
+    size_t smem = 0;
+    if constexpr (F::kTable) {
+        smem = table_smem_bytes(ts);
+        cudaError_t e = set_smem(gj8_kernel<F, K>, smem);
+        if (e != cudaSuccess)
+            return e;
+    }
+    gj8_kernel<F, K><<<ls.grid, ls.block, smem, s>>>(f, ts, a);
+    return cudaGetLastError();
+}
+
+template <class F>
+static cudaError_t launch_gj8_f(F f, const TableSrc& ts, const PropArgs& a, int num_sms,
+    cudaStream_t s, int block_override, int objs_per_thread)
+{
+    if (objs_per_thread == 2)
+        return launch_gj8_k<F, 2>(f, ts, a, num_sms, s, block_override);
+    return launch_gj8_k<F, 1>(f, ts, a, num_sms, s, block_override);
+}
+
+cudaError_t launch_gj8(const TableSrc& ts, const PropArgs& a, int num_sms, cudaStream_t s,
+    int block_override, int objs_per_thread)
 {
     if (a.n <= 0 || a.step_end <= a.step_begin)
         return cudaSuccess;
-    LaunchShape ls = pick_shape(a.n, 512, num_sms);
-    if (block_override > 0) {
-        ls.block = block_override;
-        ls.grid = (int)((a.n + block_override - 1) / block_override);
-    }
+    if (objs_per_thread <= 0) // default: two objects per thread once every SM gets 64 threads
+        objs_per_thread = a.n >= (int64_t)num_sms * 128 ? 2 : 1;
     if (a.kind == 0) {
-        size_t smem = table_smem_bytes(ts);
         if (ts.mixed) {
             ForceGravity<true> f {};
             f.gen_m = a.gen_m;
             f.prop_m = a.prop_m;
-            cudaError_t e = set_smem(gj8_kernel<ForceGravity<true>>, smem);
-            if (e != cudaSuccess)
-                return e;
-            gj8_kernel<<<ls.grid, ls.block, smem, s>>>(f, ts, a);
-        } else {
-            ForceGravity<false> f {};
-            f.gen_m = a.gen_m;
-            f.prop_m = a.prop_m;
-            cudaError_t e = set_smem(gj8_kernel<ForceGravity<false>>, smem);
-            if (e != cudaSuccess)
-                return e;
-            gj8_kernel<<<ls.grid, ls.block, smem, s>>>(f, ts, a);
+            return launch_gj8_f(f, ts, a, num_sms, s, block_override, objs_per_thread);
         }
-    } else {
-        ForceAnalytic f { a.kind, a.h };
-        gj8_kernel<<<ls.grid, ls.block, 0, s>>>(f, ts, a);
+        ForceGravity<false> f {};
+        f.gen_m = a.gen_m;
+        f.prop_m = a.prop_m;
+        return launch_gj8_f(f, ts, a, num_sms, s, block_override, objs_per_thread);
     }
-    return cudaGetLastError();
+    ForceAnalytic f { a.kind, a.h };
+    return launch_gj8_f(f, ts, a, num_sms, s, block_override, objs_per_thread);
 }
 
 cudaError_t launch_gravity(const TableSrc& ts, int64_t n, const double* r, const double* m9,
