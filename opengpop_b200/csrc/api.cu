@@ -165,7 +165,7 @@ gpop_status propagator_step(gpop_propagator* p, int steps, double* traj_r, doubl
         const bool last = a.step_end == end;
         a.out_r = last ? p->r : nullptr;
         a.out_v = last ? p->v : nullptr;
-        if ((e = launch_gj8(ts, a, ctx->num_sms, s, ctx->block_override, ctx->objs_per_thread)) != cudaSuccess)
+        if ((e = launch_gj8(ts, a, ctx->num_sms, s, ctx->block_override, ctx->walk_mode)) != cudaSuccess)
             return cuda_fail(ctx, e, "GJ8 kernel");
         ctx->launches++;
     }
@@ -240,8 +240,8 @@ gpop_status gpop_create(const gpop_config* cfg_in, gpop_ctx** out)
         return fail(ctx, GPOP_ERR_DATA, err);
     if (const char* spl = std::getenv("GPOP_STEPS_PER_LAUNCH"))
         ctx->steps_per_launch = std::max(1, atoi(spl));
-    if (const char* opt = std::getenv("GPOP_OBJS_PER_THREAD"))
-        ctx->objs_per_thread = std::min(2, std::max(0, atoi(opt)));
+    if (const char* wm = std::getenv("GPOP_WALK_MODE"))
+        ctx->walk_mode = std::min(3, std::max(0, atoi(wm)));
     cudaError_t e = cudaSetDevice(cfg.device);
     if (e != cudaSuccess)
         return cuda_fail(ctx, e, "cudaSetDevice");

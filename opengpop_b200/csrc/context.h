@@ -47,7 +47,7 @@ struct gpop_ctx {
     int num_sms = 148;
     int steps_per_launch = 64;
     int block_override = 0; // GJ8 block size chosen by the tuner (0 = default policy)
-    int objs_per_thread = 0; // GJ8 objects per thread, 1 or 2 (0 = by problem size)
+    int walk_mode = 0; // GJ8 triangle walk (WalkMode; 0 = default)
     // device-resident model data
     gpop::DevBuf t64, mixed, nut, eop, leap, err_word;
     uint32_t t64_bytes = 0, mixed_bytes = 0, mixed_off32 = 0;

@@ -54,9 +54,11 @@ size_t table_smem_bytes(const TableSrc& ts);
 LaunchShape pick_shape(int64_t n, int max_block, int num_sms);
 
 cudaError_t launch_startup(const TableSrc& ts, const PropArgs& a, int num_sms, cudaStream_t s);
-// objs_per_thread: 1 or 2 (0 = chosen from n and the SM count)
+// How a GJ8 thread walks the gravity triangle: one object, two objects in lockstep, or one object
+// with two cursors (0 = default).
+enum WalkMode : int { kWalkOneObject = 1, kWalkTwoObjects = 2, kWalkTwoCursors = 3 };
 cudaError_t launch_gj8(const TableSrc& ts, const PropArgs& a, int num_sms, cudaStream_t s,
-    int block_override = 0, int objs_per_thread = 0);
+    int block_override = 0, int walk = 0);
 cudaError_t launch_gravity(const TableSrc& ts, int64_t n, const double* r, const double* m9,
     double* a, unsigned* err, int num_sms, cudaStream_t s);
 cudaError_t launch_corrector_unit(int kind, double h, int op, double* r27, double* v27, double* a27,

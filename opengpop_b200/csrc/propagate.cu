@@ -23,11 +23,14 @@ template <bool MIXED> struct ForceGravity {
     {
         gravity_gcrs1<MIXED>(g, prop_m + (size_t)idx * 9, r, a);
     }
-    template <int K>
+    template <int K, int C>
     __device__ __forceinline__ void prop_k(const double (&r)[K][3], const double (&)[K][3], int idx,
         double (&a)[K][3]) const
     {
-        gravity_gcrs<MIXED, K>(g, prop_m + (size_t)idx * 9, r, a);
+        if constexpr (C == 2)
+            gravity_gcrs_c2<MIXED>(g, prop_m + (size_t)idx * 9, r, a);
+        else
+            gravity_gcrs<MIXED, K>(g, prop_m + (size_t)idx * 9, r, a);
     }
     // ForceModel::ComputeGenerationAcceleration (force_model.cu:59-89): table (s'+4)*10 + k
     __device__ __forceinline__ void gen(const double* r, const double*, int step, int k, double* a) const
@@ -79,7 +82,7 @@ struct ForceAnalytic {
     {
         eval(r, v, (double)(idx - 4) * h, a);
     }
-    template <int K>
+    template <int K, int C>
     __device__ __forceinline__ void prop_k(const double (&r)[K][3], const double (&v)[K][3], int idx,
         double (&a)[K][3]) const
     {
@@ -288,8 +291,9 @@ __global__ void __launch_bounds__(256) startup_kernel(F f, TableSrc ts, PropArgs
 
 // ---- GJ8 step (prediction.cu:49-74 + gpu_propagator.cu:86-119) ----
 // K objects per thread: object k of thread g is g + k * (threads in the grid); every gravity
-// evaluation of a step runs the K objects in lockstep on the same table entries.
-template <class F, int K>
+// evaluation of a step runs the K objects in lockstep on the same table entries. C = 2 walks the
+// coefficient triangle of one object with two cursors (K = 1).
+template <class F, int K, int C>
 __global__ void __launch_bounds__(K == 1 ? 512 : 256, 1) gj8_kernel(F f, TableSrc ts, PropArgs a)
 {
     extern __shared__ __align__(128) uint8_t smem[];
@@ -373,12 +377,12 @@ __global__ void __launch_bounds__(K == 1 ? 512 : 256, 1) gj8_kernel(F f, TableSr
                 }
             }
             const int idx = step + 4;
-            f.template prop_k<K>(r, v, idx, a8);
+            f.template prop_k<K, C>(r, v, idx, a8);
             // Corrector: the first pass reuses the predictor's evaluation at the unchanged
             // position (bit-identical to the reference's repeated call).
             for (int it = 0; it < a.ncorr; ++it) {
                 if (it > 0)
-                    f.template prop_k<K>(r, v, idx, a8);
+                    f.template prop_k<K, C>(r, v, idx, a8);
 #pragma unroll
                 for (int k = 0; k < K; ++k)
 #pragma unroll
@@ -568,7 +572,7 @@ cudaError_t launch_startup(const TableSrc& ts, const PropArgs& a, int num_sms, c
     return cudaGetLastError();
 }
 
-template <class F, int K>
+template <class F, int K, int C>
 static cudaError_t launch_gj8_k(F f, const TableSrc& ts, const PropArgs& a, int num_sms,
     cudaStream_t s, int block_override)
 {
@@ -581,44 +585,46 @@ static cudaError_t launch_gj8_k(F f, const TableSrc& ts, const PropArgs& a, int 
     size_t smem = 0;
     if constexpr (F::kTable) {
         smem = table_smem_bytes(ts);
-        cudaError_t e = set_smem(gj8_kernel<F, K>, smem);
+        cudaError_t e = set_smem(gj8_kernel<F, K, C>, smem);
         if (e != cudaSuccess)
             return e;
     }
-    gj8_kernel<F, K><<<ls.grid, ls.block, smem, s>>>(f, ts, a);
+    gj8_kernel<F, K, C><<<ls.grid, ls.block, smem, s>>>(f, ts, a);
     return cudaGetLastError();
 }
 
 template <class F>
 static cudaError_t launch_gj8_f(F f, const TableSrc& ts, const PropArgs& a, int num_sms,
-    cudaStream_t s, int block_override, int objs_per_thread)
+    cudaStream_t s, int block_override, int walk)
 {
-    if (objs_per_thread == 2)
-        return launch_gj8_k<F, 2>(f, ts, a, num_sms, s, block_override);
-    return launch_gj8_k<F, 1>(f, ts, a, num_sms, s, block_override);
+    if (walk == kWalkTwoObjects)
+        return launch_gj8_k<F, 2, 1>(f, ts, a, num_sms, s, block_override);
+    if (walk == kWalkTwoCursors)
+        return launch_gj8_k<F, 1, 2>(f, ts, a, num_sms, s, block_override);
+    return launch_gj8_k<F, 1, 1>(f, ts, a, num_sms, s, block_override);
 }
 
 cudaError_t launch_gj8(const TableSrc& ts, const PropArgs& a, int num_sms, cudaStream_t s,
-    int block_override, int objs_per_thread)
+    int block_override, int walk)
 {
     if (a.n <= 0 || a.step_end <= a.step_begin)
         return cudaSuccess;
-    if (objs_per_thread <= 0) // default: two objects per thread once every SM gets 64 threads
-        objs_per_thread = a.n >= (int64_t)num_sms * 128 ? 2 : 1;
+    if (walk <= 0)
+        walk = kWalkTwoCursors;
     if (a.kind == 0) {
         if (ts.mixed) {
             ForceGravity<true> f {};
             f.gen_m = a.gen_m;
             f.prop_m = a.prop_m;
-            return launch_gj8_f(f, ts, a, num_sms, s, block_override, objs_per_thread);
+            return launch_gj8_f(f, ts, a, num_sms, s, block_override, walk);
         }
         ForceGravity<false> f {};
         f.gen_m = a.gen_m;
         f.prop_m = a.prop_m;
-        return launch_gj8_f(f, ts, a, num_sms, s, block_override, objs_per_thread);
+        return launch_gj8_f(f, ts, a, num_sms, s, block_override, walk);
     }
     ForceAnalytic f { a.kind, a.h };
-    return launch_gj8_f(f, ts, a, num_sms, s, block_override, objs_per_thread);
+    return launch_gj8_f(f, ts, a, num_sms, s, block_override, walk);
 }
 
 cudaError_t launch_gravity(const TableSrc& ts, int64_t n, const double* r, const double* m9,
