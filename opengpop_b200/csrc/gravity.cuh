@@ -55,18 +55,30 @@ template <int K> struct ColSums64 {
 };
 
 // Walks column entries e[first..last] in FP64, continuing the recursion from Q1 = Q(n-1),
-// Q2 = Q(n-2) of each object.
+// Q2 = Q(n-2) of each object. The product c(n+1) w Q(n-1) of the next term is formed while the
+// current term accumulates, so one FMA separates consecutive Q values on the dependency chain.
+// (The entry after the last one of column m < L is the first entry of column m+1, in bounds.)
 template <int K>
 __device__ __forceinline__ void column64(const GravEntry64* __restrict__ e, int first, int last,
     const double (&u)[K], const double (&w)[K], double (&Q1)[K], double (&Q2)[K], ColSums64<K>& s)
 {
-#pragma unroll 2
+    if (first > last)
+        return;
+    double t2[K];
+    {
+        const double c = reinterpret_cast<const double2*>(e + first)[0].x;
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+            t2[k] = (c * w[k]) * Q2[k];
+    }
+#pragma unroll 4
     for (int i = first; i <= last; ++i) {
-        const double c = reinterpret_cast<const double2*>(e + i)[0].x;
+        const double cn = reinterpret_cast<const double2*>(e + i + 1)[0].x;
         double Q[K];
 #pragma unroll
         for (int k = 0; k < K; ++k) {
-            Q[k] = fma(u[k], Q1[k], -(c * w[k]) * Q2[k]);
+            Q[k] = fma(u[k], Q1[k], -t2[k]);
+            t2[k] = (cn * w[k]) * Q1[k];
             Q2[k] = Q1[k];
             Q1[k] = Q[k];
         }
@@ -88,11 +100,16 @@ template <int K> struct ColSums32 {
 __device__ __forceinline__ void column32(const GravEntry32* __restrict__ e, int first, int last,
     float u, float w, float& Q1, float& Q2, ColSums32<1>& s)
 {
-#pragma unroll 2
+    if (first > last)
+        return;
+    float t2 = (reinterpret_cast<const float4*>(e + first)[0].x * w) * Q2;
+#pragma unroll 4
     for (int i = first; i <= last; ++i) {
         const float4* p = reinterpret_cast<const float4*>(e + i);
         const float4 a = p[0], b = p[1];
-        const float Q = fmaf(u, Q1, (a.x * w) * Q2);
+        const float cn = reinterpret_cast<const float4*>(e + i + 1)[0].x;
+        const float Q = fmaf(u, Q1, t2);
+        t2 = (cn * w) * Q1;
         const float2 QQ = make_float2(Q, Q);
         s.g[0] = __ffma2_rn(QQ, make_float2(a.z, a.w), s.g[0]);
         s.j[0] = __ffma2_rn(QQ, make_float2(b.x, b.y), s.j[0]);
@@ -106,12 +123,17 @@ __device__ __forceinline__ void column32(const GravEntry32* __restrict__ e, int 
 __device__ __forceinline__ void column32x2(const GravEntry32* __restrict__ e, int first, int last,
     float2 u, float2 w, float2& Q1, float2& Q2, ColSums32<2>& s)
 {
-#pragma unroll 2
+    if (first > last)
+        return;
+    const float4 a0 = reinterpret_cast<const float4*>(e + first)[0];
+    float2 t2 = __fmul2_rn(__fmul2_rn(make_float2(a0.x, a0.y), w), Q2);
+#pragma unroll 4
     for (int i = first; i <= last; ++i) {
         const float4* p = reinterpret_cast<const float4*>(e + i);
         const float4 a = p[0], b = p[1];
-        const float2 t = __fmul2_rn(make_float2(a.x, a.y), w);
-        const float2 Q = __ffma2_rn(u, Q1, __fmul2_rn(t, Q2));
+        const float4 an = reinterpret_cast<const float4*>(e + i + 1)[0];
+        const float2 Q = __ffma2_rn(u, Q1, t2);
+        t2 = __fmul2_rn(__fmul2_rn(make_float2(an.x, an.y), w), Q1);
         const float2 QA = make_float2(Q.x, Q.x), QB = make_float2(Q.y, Q.y);
         const float2 cg = make_float2(a.z, a.w), cj = make_float2(b.x, b.y), ch = make_float2(b.z, b.w);
         s.g[0] = __ffma2_rn(QA, cg, s.g[0]);
