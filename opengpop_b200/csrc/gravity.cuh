@@ -275,345 +275,6 @@ __device__ __forceinline__ void gravity_itrs(const GravSmem& gs, const double (&
     }
 }
 
-// ---- one object, two cursors ----
-// The triangle is split at column kSplit(L) into two contiguous groups of columns with about the
-// same number of terms; one thread walks both groups in lockstep (two independent recursion and
-// accumulation chains), so the FP pipes see twice the independent work per warp without more
-// threads per object. All lanes of a warp hold different objects but walk the same entries, so
-// control flow stays uniform.
-__host__ __device__ __forceinline__ int cursor_split(int L)
-{
-    const int E = (L + 1) * (L + 2) / 2;
-    int m = 0;
-    while (m < L && grav_col_offset(m + 1, L) <= E / 2)
-        ++m;
-    return m + 1; // first column of the second group
-}
-
-struct Col64 {
-    double Q1, Q2, g1, g2, j1, j2, h1, h2;
-    double Cm, Sm, Cp, Sp, qm;
-    int m, i, last; // current column, next entry in it, last column of the group
-};
-
-__device__ __forceinline__ void col64_step(Col64& c, const GravEntry64* __restrict__ e, double u, double w)
-{
-    const double2* p = reinterpret_cast<const double2*>(e);
-    const double cc = p[0].x;
-    const double2 g = p[1], j = p[2], h = p[3];
-    const double Q = fma(u, c.Q1, -(cc * w) * c.Q2);
-    c.g1 = fma(g.x, Q, c.g1);
-    c.g2 = fma(g.y, Q, c.g2);
-    c.j1 = fma(j.x, Q, c.j1);
-    c.j2 = fma(j.y, Q, c.j2);
-    c.h1 = fma(h.x, Q, c.h1);
-    c.h2 = fma(h.y, Q, c.h2);
-    c.Q2 = c.Q1;
-    c.Q1 = Q;
-}
-
-struct ObjTotals {
-    double G, H, J, K;
-};
-
-// eq. 4-11 column combination, then the eq. 3-18 step to the next column.
-__device__ __forceinline__ void col64_finish(Col64& c, ObjTotals& t, double C1, double S1, double q)
-{
-    const double dm = (double)c.m;
-    t.G += c.Cm * c.g1 + c.Sm * c.g2;
-    t.J += dm * (c.Cp * c.j1 + c.Sp * c.j2);
-    t.K -= dm * (c.Sp * c.j1 - c.Cp * c.j2);
-    t.H += c.Cp * c.h1 + c.Sp * c.h2;
-    c.Cp = c.Cm;
-    c.Sp = c.Sm;
-    const double Cn = C1 * c.Cm - S1 * c.Sm;
-    const double Sn = S1 * c.Cm + C1 * c.Sm;
-    c.Cm = Cn;
-    c.Sm = Sn;
-    c.qm *= q;
-    c.m += 1;
-}
-
-// Opens column c.m: n = m term with Q = q^m.
-__device__ __forceinline__ void col64_open(Col64& c, const GravEntry64* __restrict__ tab, int L)
-{
-    const GravEntry64* e = tab + grav_col_offset(c.m, L);
-    const double2* p = reinterpret_cast<const double2*>(e);
-    const double2 g = p[1], j = p[2], h = p[3];
-    c.Q1 = c.qm;
-    c.Q2 = 0.0;
-    c.g1 = g.x * c.Q1;
-    c.g2 = g.y * c.Q1;
-    c.j1 = j.x * c.Q1;
-    c.j2 = j.y * c.Q1;
-    c.h1 = h.x * c.Q1;
-    c.h2 = h.y * c.Q1;
-    c.i = 1;
-}
-
-__device__ __forceinline__ void cursor_seed(Col64& c, int m0, int last, double C1, double S1, double q)
-{
-    c.Cm = 1.0;
-    c.Sm = 0.0;
-    c.Cp = 0.0;
-    c.Sp = 0.0;
-    c.qm = 1.0;
-    for (int m = 0; m < m0; ++m) { // the same recursion as walking the columns one by one
-        c.Cp = c.Cm;
-        c.Sp = c.Sm;
-        const double Cn = C1 * c.Cm - S1 * c.Sm;
-        const double Sn = S1 * c.Cm + C1 * c.Sm;
-        c.Cm = Cn;
-        c.Sm = Sn;
-        c.qm *= q;
-    }
-    c.m = m0;
-    c.last = last;
-}
-
-__device__ __forceinline__ void gravity_itrs_fp64_c2(const GravSmem& gs, double x, double y,
-    double z, double& ax, double& ay, double& az)
-{
-    const int L = gs.L;
-    const double r = sqrt(x * x + y * y + z * z);
-    const double eps = z / r;
-    const double q = gs.radius / r;
-    const double u = q * eps, w = q * q;
-    const double C1 = x / r, S1 = y / r;
-    ObjTotals t { 0.0, 0.0, 0.0, 0.0 };
-    const int split = cursor_split(L);
-    Col64 A, B;
-    cursor_seed(A, 0, split - 1, C1, S1, q);
-    cursor_seed(B, split, L, C1, S1, q);
-    col64_open(A, gs.t64, L);
-    col64_open(B, gs.t64, L);
-    bool a_on = true, b_on = split <= L;
-    while (a_on || b_on) {
-        if (a_on && b_on) {
-            const int ra = (L - A.m) - A.i + 1, rb = (L - B.m) - B.i + 1;
-            const int k = ra < rb ? ra : rb;
-            const GravEntry64* ea = gs.t64 + grav_col_offset(A.m, L) + A.i;
-            const GravEntry64* eb = gs.t64 + grav_col_offset(B.m, L) + B.i;
-#pragma unroll 2
-            for (int s = 0; s < k; ++s) {
-                col64_step(A, ea + s, u, w);
-                col64_step(B, eb + s, u, w);
-            }
-            A.i += k;
-            B.i += k;
-        } else if (a_on) {
-            const GravEntry64* ea = gs.t64 + grav_col_offset(A.m, L);
-#pragma unroll 2
-            for (int s = A.i; s <= L - A.m; ++s)
-                col64_step(A, ea + s, u, w);
-            A.i = L - A.m + 1;
-        } else {
-            const GravEntry64* eb = gs.t64 + grav_col_offset(B.m, L);
-#pragma unroll 2
-            for (int s = B.i; s <= L - B.m; ++s)
-                col64_step(B, eb + s, u, w);
-            B.i = L - B.m + 1;
-        }
-        if (a_on && A.i > L - A.m) {
-            const bool more = A.m < A.last;
-            col64_finish(A, t, C1, S1, q);
-            if (more)
-                col64_open(A, gs.t64, L);
-            else
-                a_on = false;
-        }
-        if (b_on && B.i > L - B.m) {
-            const bool more = B.m < B.last;
-            col64_finish(B, t, C1, S1, q);
-            if (more)
-                col64_open(B, gs.t64, L);
-            else
-                b_on = false;
-        }
-    }
-    const double G = t.G + 1.0; // eq. 4-13
-    const double Lambda = G + z * t.H / r;
-    const double c = -gs.gm / (r * r);
-    ax = c * (Lambda * x / r - t.J);
-    ay = c * (Lambda * y / r - t.K);
-    az = c * (Lambda * z / r - t.H);
-}
-
-// Mixed precision with two cursors: FP32 lockstep walk over the n > 8 entries; the FP64 head
-// (n <= 8) of a column m <= 8 runs when the cursor opens that column.
-struct Col32 {
-    float Q1, Q2;
-    float2 g, j, h;
-    double Cm, Sm, Cp, Sp, qm;
-    int m, i, last;
-};
-
-__device__ __forceinline__ void col32_step(Col32& c, const GravEntry32* __restrict__ e, float u, float w)
-{
-    const float4* p = reinterpret_cast<const float4*>(e);
-    const float4 a = p[0], b = p[1];
-    const float Q = fmaf(u, c.Q1, (a.x * w) * c.Q2);
-    const float2 QQ = make_float2(Q, Q);
-    c.g = __ffma2_rn(QQ, make_float2(a.z, a.w), c.g);
-    c.j = __ffma2_rn(QQ, make_float2(b.x, b.y), c.j);
-    c.h = __ffma2_rn(QQ, make_float2(b.z, b.w), c.h);
-    c.Q2 = c.Q1;
-    c.Q1 = Q;
-}
-
-__device__ __forceinline__ void col32_finish(Col32& c, ObjTotals& t, double C1, double S1, double q)
-{
-    const double dm = (double)c.m;
-    const double g1 = c.g.x, g2 = c.g.y, j1 = c.j.x, j2 = c.j.y, h1 = c.h.x, h2 = c.h.y;
-    t.G += c.Cm * g1 + c.Sm * g2;
-    t.J += dm * (c.Cp * j1 + c.Sp * j2);
-    t.K -= dm * (c.Sp * j1 - c.Cp * j2);
-    t.H += c.Cp * h1 + c.Sp * h2;
-    c.Cp = c.Cm;
-    c.Sp = c.Sm;
-    const double Cn = C1 * c.Cm - S1 * c.Sm;
-    const double Sn = S1 * c.Cm + C1 * c.Sm;
-    c.Cm = Cn;
-    c.Sm = Sn;
-    c.qm *= q;
-    c.m += 1;
-}
-
-// Opens column c.m in mixed mode; returns with c.i = first FP32 entry of the column.
-__device__ __forceinline__ void col32_open(Col32& c, const GravSmem& gs, ObjTotals& t, double u,
-    double w)
-{
-    const int L = gs.L;
-    const GravEntry32* e32 = gs.t32 + grav_col_offset(c.m, L);
-    c.g = c.j = c.h = make_float2(0.f, 0.f);
-    if (c.m <= kMixedSplit) {
-        // FP64 head n = m..min(8, L), combined into the totals right away
-        const int top = L < kMixedSplit ? L : kMixedSplit;
-        const GravEntry64* e = gs.t64 + grav_col_offset(c.m, kMixedSplit);
-        double Q1[1] = { c.qm }, Q2[1] = { 0.0 };
-        ColSums64<1> s;
-        s.zero();
-        s.add(e, Q1);
-        const double uu[1] = { u }, ww[1] = { w };
-        column64<1>(e, 1, top - c.m, uu, ww, Q1, Q2, s);
-        const double dm = (double)c.m;
-        t.G += c.Cm * s.g1[0] + c.Sm * s.g2[0];
-        t.J += dm * (c.Cp * s.j1[0] + c.Sp * s.j2[0]);
-        t.K -= dm * (c.Sp * s.j1[0] - c.Cp * s.j2[0]);
-        t.H += c.Cp * s.h1[0] + c.Sp * s.h2[0];
-        c.Q1 = (float)Q1[0];
-        c.Q2 = (float)Q2[0];
-        c.i = kMixedSplit + 1 - c.m;
-    } else {
-        const float4* p = reinterpret_cast<const float4*>(e32);
-        const float4 a = p[0], b = p[1];
-        const float Qm = (float)c.qm;
-        const float2 QQ = make_float2(Qm, Qm);
-        c.g = __fmul2_rn(QQ, make_float2(a.z, a.w));
-        c.j = __fmul2_rn(QQ, make_float2(b.x, b.y));
-        c.h = __fmul2_rn(QQ, make_float2(b.z, b.w));
-        c.Q1 = Qm;
-        c.Q2 = 0.f;
-        c.i = 1;
-    }
-}
-
-__device__ __forceinline__ void gravity_itrs_mixed_c2(const GravSmem& gs, double x, double y,
-    double z, double& ax, double& ay, double& az)
-{
-    const int L = gs.L;
-    const double r = sqrt(x * x + y * y + z * z);
-    const double eps = z / r;
-    const double q = gs.radius / r;
-    const double u = q * eps, w = q * q;
-    const float uf = (float)u, wf = (float)w;
-    const double C1 = x / r, S1 = y / r;
-    ObjTotals t { 0.0, 0.0, 0.0, 0.0 };
-    const int split = cursor_split(L);
-    Col32 A, B;
-    {
-        Col64 tmp;
-        cursor_seed(tmp, 0, split - 1, C1, S1, q);
-        A.Cm = tmp.Cm; A.Sm = tmp.Sm; A.Cp = tmp.Cp; A.Sp = tmp.Sp; A.qm = tmp.qm; A.m = tmp.m; A.last = tmp.last;
-        cursor_seed(tmp, split, L, C1, S1, q);
-        B.Cm = tmp.Cm; B.Sm = tmp.Sm; B.Cp = tmp.Cp; B.Sp = tmp.Sp; B.qm = tmp.qm; B.m = tmp.m; B.last = tmp.last;
-    }
-    col32_open(A, gs, t, u, w);
-    bool a_on = true, b_on = split <= L;
-    if (b_on)
-        col32_open(B, gs, t, u, w);
-    while (a_on || b_on) {
-        if (a_on && b_on) {
-            const int ra = (L - A.m) - A.i + 1, rb = (L - B.m) - B.i + 1;
-            const int k = ra < rb ? ra : rb;
-            const GravEntry32* ea = gs.t32 + grav_col_offset(A.m, L) + A.i;
-            const GravEntry32* eb = gs.t32 + grav_col_offset(B.m, L) + B.i;
-#pragma unroll 2
-            for (int s = 0; s < k; ++s) {
-                col32_step(A, ea + s, uf, wf);
-                col32_step(B, eb + s, uf, wf);
-            }
-            A.i += k;
-            B.i += k;
-        } else if (a_on) {
-            const GravEntry32* ea = gs.t32 + grav_col_offset(A.m, L);
-#pragma unroll 2
-            for (int s = A.i; s <= L - A.m; ++s)
-                col32_step(A, ea + s, uf, wf);
-            A.i = L - A.m + 1;
-        } else {
-            const GravEntry32* eb = gs.t32 + grav_col_offset(B.m, L);
-#pragma unroll 2
-            for (int s = B.i; s <= L - B.m; ++s)
-                col32_step(B, eb + s, uf, wf);
-            B.i = L - B.m + 1;
-        }
-        if (a_on && A.i > L - A.m) {
-            const bool more = A.m < A.last;
-            col32_finish(A, t, C1, S1, q);
-            if (more)
-                col32_open(A, gs, t, u, w);
-            else
-                a_on = false;
-        }
-        if (b_on && B.i > L - B.m) {
-            const bool more = B.m < B.last;
-            col32_finish(B, t, C1, S1, q);
-            if (more)
-                col32_open(B, gs, t, u, w);
-            else
-                b_on = false;
-        }
-    }
-    const double G = t.G + 1.0; // eq. 4-13
-    const double Lambda = G + z * t.H / r;
-    const double c = -gs.gm / (r * r);
-    ax = c * (Lambda * x / r - t.J);
-    ay = c * (Lambda * y / r - t.K);
-    az = c * (Lambda * z / r - t.H);
-}
-
-template <bool MIXED>
-__device__ __forceinline__ void gravity_gcrs_c2(const GravSmem& gs, const double* __restrict__ M,
-    const double (&r)[1][3], double (&a)[1][3])
-{
-    double m[9];
-#pragma unroll
-    for (int i = 0; i < 9; ++i)
-        m[i] = __ldg(M + i);
-    const double px = m[0] * r[0][0] + m[1] * r[0][1] + m[2] * r[0][2];
-    const double py = m[3] * r[0][0] + m[4] * r[0][1] + m[5] * r[0][2];
-    const double pz = m[6] * r[0][0] + m[7] * r[0][1] + m[8] * r[0][2];
-    double ax, ay, az;
-    if constexpr (MIXED)
-        gravity_itrs_mixed_c2(gs, px, py, pz, ax, ay, az);
-    else
-        gravity_itrs_fp64_c2(gs, px, py, pz, ax, ay, az);
-    a[0][0] = m[0] * ax + m[3] * ay + m[6] * az;
-    a[0][1] = m[1] * ax + m[4] * ay + m[7] * az;
-    a[0][2] = m[2] * ax + m[5] * ay + m[8] * az;
-}
-
 // GCRS accelerations of K objects at GCRS positions r[k] with the ITRS->GCRS matrix M
 // (column-major): r_itrs = M^T r, a = M a_itrs (the two cublasDgemvStridedBatched of
 // gravity_source.cu:176-210).

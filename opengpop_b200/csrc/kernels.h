@@ -54,9 +54,8 @@ size_t table_smem_bytes(const TableSrc& ts);
 LaunchShape pick_shape(int64_t n, int max_block, int num_sms);
 
 cudaError_t launch_startup(const TableSrc& ts, const PropArgs& a, int num_sms, cudaStream_t s);
-// How a GJ8 thread walks the gravity triangle: one object, two objects in lockstep, or one object
-// with two cursors (0 = default).
-enum WalkMode : int { kWalkOneObject = 1, kWalkTwoObjects = 2, kWalkTwoCursors = 3 };
+// How many objects a GJ8 thread carries through the gravity triangle walk (0 = by problem size).
+enum WalkMode : int { kWalkOneObject = 1, kWalkTwoObjects = 2 };
 cudaError_t launch_gj8(const TableSrc& ts, const PropArgs& a, int num_sms, cudaStream_t s,
     int block_override = 0, int walk = 0);
 cudaError_t launch_gravity(const TableSrc& ts, int64_t n, const double* r, const double* m9,

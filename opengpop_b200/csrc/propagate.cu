@@ -23,14 +23,11 @@ template <bool MIXED> struct ForceGravity {
     {
         gravity_gcrs1<MIXED>(g, prop_m + (size_t)idx * 9, r, a);
     }
-    template <int K, int C>
+    template <int K>
     __device__ __forceinline__ void prop_k(const double (&r)[K][3], const double (&)[K][3], int idx,
         double (&a)[K][3]) const
     {
-        if constexpr (C == 2)
-            gravity_gcrs_c2<MIXED>(g, prop_m + (size_t)idx * 9, r, a);
-        else
-            gravity_gcrs<MIXED, K>(g, prop_m + (size_t)idx * 9, r, a);
+        gravity_gcrs<MIXED, K>(g, prop_m + (size_t)idx * 9, r, a);
     }
     // ForceModel::ComputeGenerationAcceleration (force_model.cu:59-89): table (s'+4)*10 + k
     __device__ __forceinline__ void gen(const double* r, const double*, int step, int k, double* a) const
@@ -82,7 +79,7 @@ struct ForceAnalytic {
     {
         eval(r, v, (double)(idx - 4) * h, a);
     }
-    template <int K, int C>
+    template <int K>
     __device__ __forceinline__ void prop_k(const double (&r)[K][3], const double (&v)[K][3], int idx,
         double (&a)[K][3]) const
     {
@@ -291,9 +288,8 @@ __global__ void __launch_bounds__(256) startup_kernel(F f, TableSrc ts, PropArgs
 
 // ---- GJ8 step (prediction.cu:49-74 + gpu_propagator.cu:86-119) ----
 // K objects per thread: object k of thread g is g + k * (threads in the grid); every gravity
-// evaluation of a step runs the K objects in lockstep on the same table entries. C = 2 walks the
-// coefficient triangle of one object with two cursors (K = 1).
-template <class F, int K, int C>
+// evaluation of a step runs the K objects in lockstep on the same table entries.
+template <class F, int K>
 __global__ void __launch_bounds__(K == 1 ? 512 : 256, 1) gj8_kernel(F f, TableSrc ts, PropArgs a)
 {
     extern __shared__ __align__(128) uint8_t smem[];
@@ -377,12 +373,12 @@ __global__ void __launch_bounds__(K == 1 ? 512 : 256, 1) gj8_kernel(F f, TableSr
                 }
             }
             const int idx = step + 4;
-            f.template prop_k<K, C>(r, v, idx, a8);
+            f.template prop_k<K>(r, v, idx, a8);
             // Corrector: the first pass reuses the predictor's evaluation at the unchanged
             // position (bit-identical to the reference's repeated call).
             for (int it = 0; it < a.ncorr; ++it) {
                 if (it > 0)
-                    f.template prop_k<K, C>(r, v, idx, a8);
+                    f.template prop_k<K>(r, v, idx, a8);
 #pragma unroll
                 for (int k = 0; k < K; ++k)
 #pragma unroll
@@ -572,7 +568,7 @@ cudaError_t launch_startup(const TableSrc& ts, const PropArgs& a, int num_sms, c
     return cudaGetLastError();
 }
 
-template <class F, int K, int C>
+template <class F, int K>
 static cudaError_t launch_gj8_k(F f, const TableSrc& ts, const PropArgs& a, int num_sms,
     cudaStream_t s, int block_override)
 {
@@ -585,11 +581,11 @@ static cudaError_t launch_gj8_k(F f, const TableSrc& ts, const PropArgs& a, int 
     size_t smem = 0;
     if constexpr (F::kTable) {
         smem = table_smem_bytes(ts);
-        cudaError_t e = set_smem(gj8_kernel<F, K, C>, smem);
+        cudaError_t e = set_smem(gj8_kernel<F, K>, smem);
         if (e != cudaSuccess)
             return e;
     }
-    gj8_kernel<F, K, C><<<ls.grid, ls.block, smem, s>>>(f, ts, a);
+    gj8_kernel<F, K><<<ls.grid, ls.block, smem, s>>>(f, ts, a);
     return cudaGetLastError();
 }
 
@@ -598,10 +594,8 @@ static cudaError_t launch_gj8_f(F f, const TableSrc& ts, const PropArgs& a, int 
     cudaStream_t s, int block_override, int walk)
 {
     if (walk == kWalkTwoObjects)
-        return launch_gj8_k<F, 2, 1>(f, ts, a, num_sms, s, block_override);
-    if (walk == kWalkTwoCursors)
-        return launch_gj8_k<F, 1, 2>(f, ts, a, num_sms, s, block_override);
-    return launch_gj8_k<F, 1, 1>(f, ts, a, num_sms, s, block_override);
+        return launch_gj8_k<F, 2>(f, ts, a, num_sms, s, block_override);
+    return launch_gj8_k<F, 1>(f, ts, a, num_sms, s, block_override);
 }
 
 cudaError_t launch_gj8(const TableSrc& ts, const PropArgs& a, int num_sms, cudaStream_t s,
@@ -609,8 +603,8 @@ cudaError_t launch_gj8(const TableSrc& ts, const PropArgs& a, int num_sms, cudaS
 {
     if (a.n <= 0 || a.step_end <= a.step_begin)
         return cudaSuccess;
-    if (walk <= 0)
-        walk = kWalkTwoCursors;
+    if (walk <= 0) // two objects per thread once every SM gets 64 threads, else one
+        walk = a.n >= (int64_t)num_sms * 128 ? kWalkTwoObjects : kWalkOneObject;
     if (a.kind == 0) {
         if (ts.mixed) {
             ForceGravity<true> f {};
