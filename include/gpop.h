@@ -127,6 +127,35 @@ gpop_status gpop_propagate_analytic(gpop_ctx* ctx, int32_t kind, double h, int32
     int32_t n_corrections, int64_t n, double* r_dev, double* v_dev, double* traj_r, double* traj_v,
     double* traj_a, void* stream);
 
+/* ---- batched propagation ---- */
+/* One propagation request of a batch: the arguments of exec propagate (exec/runner.cu:11-70)
+ * for one input, with its own step size, step count and gravity degree. Host buffers [n][3]. */
+typedef struct {
+    gpop_time start;
+    double h;
+    int32_t steps;
+    int32_t degree; /* <= 0 or > the context's degree: the context's degree */
+    int64_t n;
+    const double* r_in;
+    const double* v_in;
+    double* r_out;
+    double* v_out;
+} gpop_request;
+
+/* Propagates many independent requests (uneven object counts, durations, step sizes, degrees) in
+ * one persistent launch: the reference runs one GpuPropagator per request (gpu_propagator.cu:
+ * 121-136), i.e. one exec propagate call each. Results equal those of gpop_propagate per request
+ * to rounding. The launch sequence is captured in a CUDA graph and replayed when the next batch
+ * has the same shape. */
+gpop_status gpop_propagate_batch(gpop_ctx* ctx, const gpop_request* reqs, int32_t n_req);
+/* The batch plan: lanes per object chosen for each request and the estimated makespan (s). */
+gpop_status gpop_batch_plan(gpop_ctx* ctx, const gpop_request* reqs, int32_t n_req,
+    int32_t* lanes_per_object, double* est_seconds);
+/* Autotuner: measures the throughput of the batched GJ8 kernel for each gravity degree in
+ * {8, 20, 36, 70} (up to the context's) and 1..32 lanes per object, which the batch planner then
+ * uses. cache_path (may be NULL) is read if it exists and written otherwise. */
+gpop_status gpop_tune(gpop_ctx* ctx, const char* cache_path);
+
 /* ---- startup and integrator pieces (device buffers, one object each) ---- */
 /* GpuStartup::Startup (gpu_startup.cu:55-68). Outputs 9 columns x 3 (column 4 = epoch):
  * r27, v27, a27, s27, S27 (device). n_corrections = 0 returns the RK8 guess only. */

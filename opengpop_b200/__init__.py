@@ -29,7 +29,8 @@ EXPORTS = (
     "gpop_config_default", "gpop_create", "gpop_destroy", "gpop_last_error", "gpop_status_string",
     "gpop_gravity_degree", "gpop_kernel_launches", "gpop_propagate", "gpop_propagate_device",
     "gpop_propagate_device_noalloc", "gpop_propagate_trajectory", "gpop_propagator_create", "gpop_propagator_step",
-    "gpop_propagator_steps_done", "gpop_propagator_destroy", "gpop_propagate_analytic", "gpop_startup", "gpop_corrector_unit",
+    "gpop_propagator_steps_done", "gpop_propagator_destroy", "gpop_propagate_analytic",
+    "gpop_propagate_batch", "gpop_batch_plan", "gpop_tune", "gpop_startup", "gpop_corrector_unit",
     "gpop_predict_unit", "gpop_finalize_correction_unit", "gpop_gravity", "gpop_frame_matrices",
     "gpop_ca_create", "gpop_ca_create_analytic", "gpop_ca_propagate", "gpop_ca_find", "gpop_ca_pairs", "gpop_ca_num_pairs",
     "gpop_ca_trajectory", "gpop_ca_destroy",
@@ -51,6 +52,12 @@ class Time(C.Structure):
 class Config(C.Structure):
     _fields_ = [("data_dir", C.c_char_p), ("device", C.c_int32), ("gravity_degree", C.c_int32),
                 ("n_corrections", C.c_int32), ("precision", C.c_int32), ("flags", C.c_uint32)]
+
+
+class Request(C.Structure):
+    _fields_ = [("start", Time), ("h", C.c_double), ("steps", C.c_int32), ("degree", C.c_int32),
+                ("n", C.c_int64), ("r_in", C.c_void_p), ("v_in", C.c_void_p),
+                ("r_out", C.c_void_p), ("v_out", C.c_void_p)]
 
 
 class CaRecord(C.Structure):
@@ -92,6 +99,9 @@ def load_library(path=LIB_PATH):
         "gpop_propagator_steps_done": (i32, [_VP]),
         "gpop_propagator_destroy": (None, [_VP]),
         "gpop_propagate_analytic": (i32, [_VP, i32, f64, i32, i32, i64] + [_VP] * 6),
+        "gpop_propagate_batch": (i32, [_VP, _VP, i32]),
+        "gpop_batch_plan": (i32, [_VP, _VP, i32, _VP, C.POINTER(f64)]),
+        "gpop_tune": (i32, [_VP, C.c_char_p]),
         "gpop_startup": (i32, [_VP, i32, C.POINTER(Time), f64, i32] + [_VP] * 8),
         "gpop_corrector_unit": (i32, [_VP, i32, f64, i32] + [_VP] * 6),
         "gpop_predict_unit": (i32, [_VP, i32, f64, i32] + [_VP] * 6),
@@ -253,6 +263,47 @@ class Context:
         self._check(load_library().gpop_finalize_correction_unit(
             self._h, float(h), _dptr(r3), _dptr(v3), _dptr(a27), _dptr(s3), _dptr(S3),
             _stream_ptr(None)))
+
+    # ---- batched propagation ----
+    def _requests(self, reqs):
+        """reqs: list of dicts (start, h, steps, degree, r, v); returns the ctypes array and the
+        output arrays (kept alive with the inputs)."""
+        arr = (Request * len(reqs))()
+        keep = []
+        for i, q in enumerate(reqs):
+            r = _host(q["r"]).reshape(-1, 3)
+            v = _host(q["v"]).reshape(-1, 3)
+            ro = np.empty_like(r)
+            vo = np.empty_like(v)
+            keep.append((r, v, ro, vo))
+            arr[i].start = as_time(q["start"])
+            arr[i].h = float(q["h"])
+            arr[i].steps = int(q["steps"])
+            arr[i].degree = int(q.get("degree", 0))
+            arr[i].n = r.shape[0]
+            arr[i].r_in = r.ctypes.data
+            arr[i].v_in = v.ctypes.data
+            arr[i].r_out = ro.ctypes.data
+            arr[i].v_out = vo.ctypes.data
+        return arr, keep
+
+    def propagate_batch(self, reqs):
+        """Returns [(r_end, v_end)] per request."""
+        arr, keep = self._requests(reqs)
+        self._check(load_library().gpop_propagate_batch(self._h, arr, len(reqs)))
+        return [(k[2], k[3]) for k in keep]
+
+    def batch_plan(self, reqs):
+        arr, keep = self._requests(reqs)
+        lpo = np.zeros(len(reqs), np.int32)
+        est = C.c_double()
+        self._check(load_library().gpop_batch_plan(self._h, arr, len(reqs),
+                                                   lpo.ctypes.data_as(_VP), C.byref(est)))
+        return lpo, est.value
+
+    def tune(self, cache_path=None):
+        self._check(load_library().gpop_tune(
+            self._h, None if cache_path is None else cache_path.encode()))
 
     # ---- force model ----
     def gravity(self, r, a, frame9=None, precision=None, stream=None):

@@ -310,6 +310,7 @@ void gpop_destroy(gpop_ctx* ctx)
 {
     if (!ctx)
         return;
+    destroy_batch_cache(ctx);
     for (DevBuf* b : { &ctx->t64, &ctx->mixed, &ctx->nut, &ctx->eop, &ctx->leap, &ctx->err_word,
              &ctx->state, &ctx->gen_m, &ctx->prop_m, &ctx->gen_sec, &ctx->prop_sec, &ctx->io_r,
              &ctx->io_v })

@@ -1,0 +1,553 @@
+// batch_api.cu -- batched propagation entry points: planner, autotuner and the captured launch.
+#include "batch.cuh"
+#include "common.cuh"
+#include "context.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <fstream>
+#include <map>
+#include <new>
+#include <numeric>
+#include <tuple>
+
+using namespace gpop;
+
+namespace {
+
+constexpr int kWarpsPerSm = 16; // persistent grid: one 512-thread block per SM
+constexpr int kDegrees[4] = { 8, 20, 36, 70 };
+const double kNodesH[10] = { 0.0, 4.0 / 27.0, 2.0 / 9.0, 1.0 / 3.0, 1.0 / 2.0, 2.0 / 3.0, 1.0 / 6.0, 1.0, 5.0 / 6.0, 1.0 };
+
+int terms(int L) { return (L + 1) * (L + 2) / 2 - 3; }
+
+// Object-steps per second per SM of the batched kernel at degree L with P lanes per object.
+// Measured by gpop_tune; before tuning a model is used: cost proportional to the terms walked,
+// with a per-lane overhead for the column split and the shuffles.
+double eta(const gpop_ctx* ctx, int L, int P)
+{
+    int lp = 0;
+    while ((1 << lp) < P)
+        ++lp;
+    if (ctx->tuned) {
+        // interpolate in the number of terms between the tuned degrees
+        int i = 0;
+        while (i < 3 && kDegrees[i + 1] <= L)
+            ++i;
+        const int j = std::min(i + 1, 3);
+        const double t0 = terms(kDegrees[i]), t1 = terms(kDegrees[j]), t = terms(std::max(L, 2));
+        const double c0 = 1.0 / ctx->eta[i][lp], c1 = 1.0 / ctx->eta[j][lp];
+        const double f = (t1 > t0) ? std::min(1.0, std::max(0.0, (t - t0) / (t1 - t0))) : 0.0;
+        return 1.0 / (c0 + f * (c1 - c0));
+    }
+    const bool mixed = ctx->cfg.precision == GPOP_MIXED;
+    const double base70 = mixed ? 6.5e5 : 4.5e5; // object-steps/s per SM at 70x70, one lane
+    const double cost = (terms(std::max(L, 2)) + 60.0) / (terms(70) + 60.0);
+    return base70 / cost / (1.0 + 0.12 * lp);
+}
+
+// Lanes per object: small requests fill their warp with lanes (the warp is theirs either way);
+// then every request whose group time exceeds the makespan bound -- the larger of the average
+// warp load and the shortest possible group time of the longest request -- doubles its lanes
+// while that shortens the group, so long requests stop setting the critical path.
+template <class ItemTime>
+void choose_lanes(const std::vector<int64_t>& n, const std::vector<int>& steps, double warps,
+    const ItemTime& item_time, std::vector<int>& lpo)
+{
+    const size_t R = n.size();
+    for (size_t r = 0; r < R; ++r) {
+        int P = 1;
+        while (P < 32 && n[r] * (int64_t)(2 * P) <= 32)
+            P *= 2;
+        lpo[r] = P;
+    }
+    double crit = 0.0;
+    for (size_t r = 0; r < R; ++r)
+        if (steps[r] > 0)
+            crit = std::max(crit, item_time(r, 32));
+    for (int iter = 0; iter < 8; ++iter) {
+        double total = 0.0;
+        for (size_t r = 0; r < R; ++r)
+            if (steps[r] > 0)
+                total += (double)((n[r] + 32 / lpo[r] - 1) / (32 / lpo[r])) * item_time(r, lpo[r]);
+        const double bound = std::max(total / warps, crit);
+        bool changed = false;
+        for (size_t r = 0; r < R; ++r)
+            while (steps[r] > 0 && lpo[r] < 32 && item_time(r, lpo[r]) > bound
+                && item_time(r, 2 * lpo[r]) < item_time(r, lpo[r])) {
+                lpo[r] *= 2;
+                changed = true;
+            }
+        if (!changed)
+            break;
+    }
+}
+
+struct Plan {
+    std::vector<int> lpo;
+    std::vector<BatchItem> items;
+    double est = 0.0;
+};
+
+Plan make_plan(const gpop_ctx* ctx, const std::vector<int64_t>& n, const std::vector<int>& steps,
+    const std::vector<int>& L)
+{
+    const size_t R = n.size();
+    Plan p;
+    p.lpo.assign(R, 1);
+    const double warps = (double)ctx->num_sms * kWarpsPerSm;
+    auto item_time = [&](size_t r, int P) { // seconds for one warp to run its group through all steps
+        return (double)steps[r] * kWarpsPerSm * (32.0 / P) / eta(ctx, L[r], P);
+    };
+    if (ctx->force_lpo > 0) // autotuner: fixed lanes per object
+        p.lpo.assign(R, ctx->force_lpo);
+    else
+        choose_lanes(n, steps, warps, item_time, p.lpo);
+    std::vector<std::pair<double, BatchItem>> items;
+    double total = 0.0, longest = 0.0;
+    for (size_t r = 0; r < R; ++r) {
+        if (steps[r] <= 0)
+            continue;
+        const int per = 32 / p.lpo[r];
+        const double t = item_time(r, p.lpo[r]);
+        for (int64_t f = 0; f < n[r]; f += per) {
+            items.push_back({ t, BatchItem { (int)r, (int)f, (int)std::min<int64_t>(per, n[r] - f) } });
+            total += t;
+        }
+        longest = std::max(longest, t);
+    }
+    std::stable_sort(items.begin(), items.end(),
+        [](const std::pair<double, BatchItem>& a, const std::pair<double, BatchItem>& b) { return a.first > b.first; });
+    for (auto& it : items)
+        p.items.push_back(it.second);
+    p.est = std::max(total / warps, longest);
+    return p;
+}
+
+struct TableKey {
+    int y, mo, d, hh, mi;
+    double sec, h;
+    bool operator<(const TableKey& o) const
+    {
+        return std::tie(y, mo, d, hh, mi, sec, h) < std::tie(o.y, o.mo, o.d, o.hh, o.mi, o.sec, o.h);
+    }
+};
+
+gpop_status validate(gpop_ctx* ctx, const gpop_request* reqs, int32_t n_req)
+{
+    if (!reqs || n_req <= 0)
+        return fail(ctx, GPOP_ERR_INVALID_ARG, "empty batch");
+    for (int32_t i = 0; i < n_req; ++i) {
+        const gpop_request& q = reqs[i];
+        const gpop_time& t = q.start;
+        if (q.n <= 0 || !q.r_in || !q.v_in || !q.r_out || !q.v_out || q.steps < 0 || !(q.h > 0.0)
+            || !std::isfinite(q.h) || t.month < 1 || t.month > 12 || t.day < 1 || t.day > 31 || !std::isfinite(t.sec))
+            return fail(ctx, GPOP_ERR_INVALID_ARG, "invalid request " + std::to_string(i));
+        if (q.n > (int64_t)1 << 24)
+            return fail(ctx, GPOP_ERR_INVALID_ARG, "request " + std::to_string(i) + " has too many objects");
+    }
+    return GPOP_OK;
+}
+
+} // namespace
+
+// Buffers and captured graph of the last batch (replayed when the next batch has the same shape).
+struct BatchCache {
+    std::vector<int64_t> sig;
+    cudaGraphExec_t exec = nullptr;
+    DevBuf reqs, items, obj_req, state, io, tables, sec, cal, epoch_req, queue;
+    std::vector<double> host_io;
+    ~BatchCache()
+    {
+        if (exec)
+            cudaGraphExecDestroy(exec);
+        for (DevBuf* b : { &reqs, &items, &obj_req, &state, &io, &tables, &sec, &cal, &epoch_req, &queue })
+            b->release();
+    }
+};
+
+namespace gpop {
+void destroy_batch_cache(gpop_ctx* ctx)
+{
+    delete ctx->batch;
+    ctx->batch = nullptr;
+    if (ctx->batch_stream)
+        cudaStreamDestroy(ctx->batch_stream);
+    ctx->batch_stream = nullptr;
+    if (ctx->batch_host)
+        cudaFreeHost(ctx->batch_host);
+    ctx->batch_host = nullptr;
+    ctx->batch_host_cap = 0;
+}
+} // namespace gpop
+
+extern "C" {
+
+gpop_status gpop_batch_plan(gpop_ctx* ctx, const gpop_request* reqs, int32_t n_req,
+    int32_t* lanes_per_object, double* est_seconds)
+{
+    if (!ctx)
+        return GPOP_ERR_INVALID_ARG;
+    gpop_status st = validate(ctx, reqs, n_req);
+    if (st != GPOP_OK)
+        return st;
+    std::vector<int64_t> n(n_req);
+    std::vector<int> steps(n_req), L(n_req);
+    for (int i = 0; i < n_req; ++i) {
+        n[i] = reqs[i].n;
+        steps[i] = reqs[i].steps;
+        L[i] = (reqs[i].degree > 0 && reqs[i].degree < ctx->md.degree) ? reqs[i].degree : ctx->md.degree;
+    }
+    Plan p = make_plan(ctx, n, steps, L);
+    if (lanes_per_object)
+        std::copy(p.lpo.begin(), p.lpo.end(), lanes_per_object);
+    if (est_seconds)
+        *est_seconds = p.est;
+    return GPOP_OK;
+}
+
+gpop_status gpop_propagate_batch(gpop_ctx* ctx, const gpop_request* reqs, int32_t n_req)
+{
+    if (!ctx)
+        return GPOP_ERR_INVALID_ARG;
+    gpop_status st = validate(ctx, reqs, n_req);
+    if (st != GPOP_OK)
+        return st;
+    cudaError_t e = cudaSetDevice(ctx->cfg.device);
+    if (e != cudaSuccess)
+        return cuda_fail(ctx, e, "cudaSetDevice");
+    // ---- layout: objects of the requests that take steps, one epoch table per (start, h) ----
+    std::vector<int64_t> n(n_req);
+    std::vector<int> steps(n_req), L(n_req);
+    std::vector<int64_t> obj0(n_req, -1);
+    int64_t N = 0;
+    std::map<TableKey, int> table_of;
+    std::vector<TableKey> tables;
+    std::vector<int> table_len; // propagation entries of each table
+    std::vector<int> req_table(n_req, -1);
+    for (int i = 0; i < n_req; ++i) {
+        const gpop_request& q = reqs[i];
+        n[i] = q.n;
+        steps[i] = q.steps;
+        L[i] = (q.degree > 0 && q.degree < ctx->md.degree) ? q.degree : ctx->md.degree;
+        if (q.steps == 0)
+            continue;
+        obj0[i] = N;
+        N += q.n;
+        TableKey k { q.start.year, q.start.month, q.start.day, q.start.hour, q.start.min, q.start.sec, q.h };
+        auto it = table_of.find(k);
+        int t;
+        if (it == table_of.end()) {
+            t = (int)tables.size();
+            table_of[k] = t;
+            tables.push_back(k);
+            table_len.push_back(0);
+        } else {
+            t = it->second;
+        }
+        table_len[t] = std::max(table_len[t], 4 + std::max(q.steps, 4) + 1);
+        req_table[i] = t;
+    }
+    for (int i = 0; i < n_req; ++i) // zero-step requests return their input (exec/runner.cu:48-51)
+        if (reqs[i].steps == 0) {
+            std::copy(reqs[i].r_in, reqs[i].r_in + 3 * reqs[i].n, reqs[i].r_out);
+            std::copy(reqs[i].v_in, reqs[i].v_in + 3 * reqs[i].n, reqs[i].v_out);
+        }
+    if (N == 0)
+        return GPOP_OK;
+    Plan plan = make_plan(ctx, n, steps, L);
+    // epoch table offsets (in matrices): [gen 80 | prop len] per table
+    std::vector<int64_t> t_off(tables.size());
+    int64_t E = 0;
+    for (size_t t = 0; t < tables.size(); ++t) {
+        t_off[t] = E;
+        E += 80 + table_len[t];
+    }
+    // shape signature: the graph is replayed only for an identical plan and layout
+    std::vector<int64_t> sig { (int64_t)ctx->cfg.precision, (int64_t)ctx->cfg.flags, N, E, (int64_t)n_req };
+    for (int i = 0; i < n_req; ++i) {
+        sig.push_back(n[i]);
+        sig.push_back(steps[i]);
+        sig.push_back(L[i]);
+        sig.push_back(plan.lpo[i]);
+        int64_t hb;
+        std::memcpy(&hb, &reqs[i].h, 8);
+        sig.push_back(hb);
+        int64_t sb;
+        std::memcpy(&sb, &reqs[i].start.sec, 8);
+        sig.push_back(sb);
+        sig.push_back(((int64_t)reqs[i].start.year << 32) | (reqs[i].start.month << 24) | (reqs[i].start.day << 16)
+            | (reqs[i].start.hour << 8) | reqs[i].start.min);
+    }
+    if (!ctx->batch)
+        ctx->batch = new (std::nothrow) BatchCache();
+    BatchCache* bc = ctx->batch;
+    if (!bc)
+        return fail(ctx, GPOP_ERR_NOMEM, "batch cache");
+    const bool replay = bc->exec && bc->sig == sig;
+    cudaStream_t s = ctx->batch_stream;
+    if (!s && (e = cudaStreamCreateWithFlags(&ctx->batch_stream, cudaStreamNonBlocking)) != cudaSuccess)
+        return cuda_fail(ctx, e, "batch stream");
+    s = ctx->batch_stream;
+    // ---- inputs: one pinned staging buffer [r0 | v0 | r_out | v_out] ----
+    const size_t io_bytes = (size_t)N * 3 * 4 * sizeof(double);
+    if ((e = bc->io.ensure(io_bytes)) != cudaSuccess)
+        return fail(ctx, GPOP_ERR_NOMEM, "batch state buffers");
+    if (ctx->batch_host_cap < io_bytes) {
+        if (ctx->batch_host)
+            cudaFreeHost(ctx->batch_host);
+        ctx->batch_host = nullptr;
+        ctx->batch_host_cap = 0;
+        if ((e = cudaMallocHost(&ctx->batch_host, io_bytes)) != cudaSuccess)
+            return fail(ctx, GPOP_ERR_NOMEM, "pinned staging buffer");
+        ctx->batch_host_cap = io_bytes;
+    }
+    double* host = static_cast<double*>(ctx->batch_host);
+    for (int i = 0; i < n_req; ++i) {
+        if (obj0[i] < 0)
+            continue;
+        std::copy(reqs[i].r_in, reqs[i].r_in + 3 * n[i], host + 3 * obj0[i]);
+        std::copy(reqs[i].v_in, reqs[i].v_in + 3 * n[i], host + 3 * N + 3 * obj0[i]);
+    }
+    double* dio = bc->io.as<double>();
+    if ((e = cudaMemcpyAsync(dio, host, (size_t)N * 6 * sizeof(double), cudaMemcpyHostToDevice, s)) != cudaSuccess)
+        return cuda_fail(ctx, e, "batch upload");
+    if (!replay) {
+        if (bc->exec) {
+            cudaGraphExecDestroy(bc->exec);
+            bc->exec = nullptr;
+        }
+        // request descriptors, items, epoch arguments
+        std::vector<BatchReq> rq(n_req);
+        std::vector<int> obj_req(N);
+        std::vector<double> sec(E);
+        std::vector<int> epoch_req(E), cal(5 * tables.size());
+        if ((e = bc->tables.ensure((size_t)E * 9 * sizeof(double))) != cudaSuccess
+            || (e = bc->sec.ensure((size_t)E * sizeof(double))) != cudaSuccess
+            || (e = bc->epoch_req.ensure((size_t)E * sizeof(int))) != cudaSuccess
+            || (e = bc->cal.ensure(cal.size() * sizeof(int) + 4)) != cudaSuccess
+            || (e = bc->reqs.ensure(n_req * sizeof(BatchReq))) != cudaSuccess
+            || (e = bc->items.ensure(std::max<size_t>(1, plan.items.size()) * sizeof(BatchItem))) != cudaSuccess
+            || (e = bc->obj_req.ensure((size_t)N * sizeof(int))) != cudaSuccess
+            || (e = bc->state.ensure((size_t)kStateArrays * N * sizeof(double))) != cudaSuccess
+            || (e = bc->queue.ensure(sizeof(int))) != cudaSuccess)
+            return fail(ctx, GPOP_ERR_NOMEM, std::string("batch buffers: ") + cudaGetErrorString(e));
+        for (size_t t = 0; t < tables.size(); ++t) {
+            const TableKey& k = tables[t];
+            cal[5 * t] = k.y;
+            cal[5 * t + 1] = k.mo;
+            cal[5 * t + 2] = k.d;
+            cal[5 * t + 3] = k.hh;
+            cal[5 * t + 4] = k.mi;
+            const double base = k.sec - 4.0 * k.h; // (sec - before h) + time from table start
+            for (int idx = 0; idx < 80; ++idx) {
+                const int sp = idx / 10 - 4;
+                double from = ((double)(idx / 10) + kNodesH[idx % 10]) * k.h;
+                if ((ctx->cfg.flags & GPOP_FIX_BACKWARD_RK8_EPOCH) && sp < 0)
+                    from = ((double)(sp + 1) - kNodesH[idx % 10]) * k.h + 4.0 * k.h;
+                sec[t_off[t] + idx] = base + from;
+                epoch_req[t_off[t] + idx] = (int)t;
+            }
+            for (int i = 0; i < table_len[t]; ++i) {
+                sec[t_off[t] + 80 + i] = base + (double)i * k.h;
+                epoch_req[t_off[t] + 80 + i] = (int)t;
+            }
+        }
+        double* dtab = bc->tables.as<double>();
+        for (int i = 0; i < n_req; ++i) {
+            rq[i].obj0 = std::max<int64_t>(0, obj0[i]);
+            rq[i].n = (int)n[i];
+            rq[i].steps = steps[i];
+            rq[i].L = L[i];
+            rq[i].lpo = plan.lpo[i];
+            rq[i].h = reqs[i].h;
+            if (req_table[i] >= 0) {
+                rq[i].gen_m = dtab + t_off[req_table[i]] * 9;
+                rq[i].prop_m = dtab + (t_off[req_table[i]] + 80) * 9;
+                for (int64_t o = 0; o < n[i]; ++o)
+                    obj_req[obj0[i] + o] = i;
+            }
+        }
+        if ((e = cudaMemcpyAsync(bc->sec.p, sec.data(), E * sizeof(double), cudaMemcpyHostToDevice, s)) != cudaSuccess
+            || (e = cudaMemcpyAsync(bc->epoch_req.p, epoch_req.data(), E * sizeof(int), cudaMemcpyHostToDevice, s))
+                != cudaSuccess
+            || (e = cudaMemcpyAsync(bc->cal.p, cal.data(), cal.size() * sizeof(int), cudaMemcpyHostToDevice, s))
+                != cudaSuccess
+            || (e = cudaMemcpyAsync(bc->reqs.p, rq.data(), n_req * sizeof(BatchReq), cudaMemcpyHostToDevice, s))
+                != cudaSuccess
+            || (e = cudaMemcpyAsync(bc->items.p, plan.items.data(), plan.items.size() * sizeof(BatchItem),
+                    cudaMemcpyHostToDevice, s))
+                != cudaSuccess
+            || (e = cudaMemcpyAsync(bc->obj_req.p, obj_req.data(), N * sizeof(int), cudaMemcpyHostToDevice, s))
+                != cudaSuccess
+            || (e = cudaStreamSynchronize(s)) != cudaSuccess) // the host vectors go out of scope
+            return cuda_fail(ctx, e, "batch plan upload");
+        // ---- capture: frames, startup, queue reset, persistent GJ8 ----
+        const bool mixed = ctx->cfg.precision == GPOP_MIXED;
+        TableSrc ts = ctx->table(mixed);
+        BatchArgs a;
+        a.reqs = bc->reqs.as<BatchReq>();
+        a.n_req = n_req;
+        a.items = bc->items.as<BatchItem>();
+        a.n_items = (int)plan.items.size();
+        a.next_item = bc->queue.as<int>();
+        a.obj_req = bc->obj_req.as<int>();
+        a.n_obj = N;
+        a.ncorr = ctx->cfg.n_corrections;
+        a.flags = ctx->cfg.flags;
+        a.state = bc->state.as<double>();
+        a.r0 = dio;
+        a.v0 = dio + 3 * N;
+        a.r_out = dio + 6 * N;
+        a.v_out = dio + 9 * N;
+        a.err = ctx->err_word.as<unsigned>();
+        a.Ltab = ctx->md.degree;
+        cudaGraph_t graph = nullptr;
+        if ((e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
+            return cuda_fail(ctx, e, "graph capture");
+        cudaError_t le = launch_frames_batch(ctx->frames, bc->cal.as<int>(), bc->epoch_req.as<int>(),
+            bc->sec.as<double>(), (int)E, dtab, s);
+        if (le == cudaSuccess)
+            le = launch_batch_startup(ts, a, ctx->num_sms, s);
+        if (le == cudaSuccess)
+            le = cudaMemsetAsync(bc->queue.p, 0, sizeof(int), s);
+        if (le == cudaSuccess)
+            le = launch_batch_gj8(ts, a, ctx->num_sms, 32 * kWarpsPerSm, s);
+        e = cudaStreamEndCapture(s, &graph);
+        if (le != cudaSuccess || e != cudaSuccess) {
+            if (graph)
+                cudaGraphDestroy(graph);
+            return cuda_fail(ctx, le != cudaSuccess ? le : e, "capturing the batch launch");
+        }
+        e = cudaGraphInstantiate(&bc->exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) {
+            bc->exec = nullptr;
+            return cuda_fail(ctx, e, "instantiating the batch graph");
+        }
+        bc->sig = sig;
+    }
+    if ((e = cudaGraphLaunch(bc->exec, s)) != cudaSuccess)
+        return cuda_fail(ctx, e, "batch graph launch");
+    ctx->launches += 3;
+    if ((e = cudaMemcpyAsync(host + 6 * N, dio + 6 * N, (size_t)N * 6 * sizeof(double), cudaMemcpyDeviceToHost, s))
+        != cudaSuccess)
+        return cuda_fail(ctx, e, "batch download");
+    st = check_device_errors(ctx, s);
+    if (st != GPOP_OK)
+        return st;
+    for (int i = 0; i < n_req; ++i) {
+        if (obj0[i] < 0)
+            continue;
+        std::copy(host + 6 * N + 3 * obj0[i], host + 6 * N + 3 * (obj0[i] + n[i]), reqs[i].r_out);
+        std::copy(host + 9 * N + 3 * obj0[i], host + 9 * N + 3 * (obj0[i] + n[i]), reqs[i].v_out);
+    }
+    return GPOP_OK;
+}
+
+gpop_status gpop_tune(gpop_ctx* ctx, const char* cache_path)
+{
+    if (!ctx)
+        return GPOP_ERR_INVALID_ARG;
+    const bool mixed = ctx->cfg.precision == GPOP_MIXED;
+    if (cache_path) { // "<precision> <L> <P> <eta>" lines
+        std::ifstream f(cache_path);
+        if (f.is_open()) {
+            int prec, Lc, P;
+            double val;
+            int found = 0;
+            while (f >> prec >> Lc >> P >> val)
+                for (int i = 0; i < 4; ++i)
+                    for (int lp = 0; lp < 6; ++lp)
+                        if (prec == (int)mixed && Lc == kDegrees[i] && P == (1 << lp) && val > 0) {
+                            ctx->eta[i][lp] = val;
+                            ++found;
+                        }
+            if (found == 24) {
+                ctx->tuned = true;
+                return GPOP_OK;
+            }
+        }
+    }
+    // Calibration: one request per (degree, lanes) that fills every warp of the persistent grid,
+    // on near-circular orbits. The captured graph is replayed at two durations; the difference
+    // (16 GJ8 steps) removes the frames, startup and launch overheads.
+    const gpop_time t0 { 2024, 1, 1, 0, 0, 0.0 };
+    const bool saved = ctx->tuned;
+    double measured[4][6];
+    auto replay_ms = [&](gpop_request& q, int steps, float& ms) -> gpop_status {
+        q.steps = steps;
+        ctx->tuned = false;
+        gpop_status st = gpop_propagate_batch(ctx, &q, 1); // builds the plan and the graph
+        if (st != GPOP_OK)
+            return st;
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        cudaError_t e = cudaEventCreate(&e0);
+        if (e == cudaSuccess)
+            e = cudaEventCreate(&e1);
+        if (e == cudaSuccess)
+            e = cudaEventRecord(e0, ctx->batch_stream);
+        if (e == cudaSuccess)
+            e = cudaGraphLaunch(ctx->batch->exec, ctx->batch_stream);
+        if (e == cudaSuccess)
+            e = cudaEventRecord(e1, ctx->batch_stream);
+        if (e == cudaSuccess)
+            e = cudaEventSynchronize(e1);
+        if (e == cudaSuccess)
+            e = cudaEventElapsedTime(&ms, e0, e1);
+        if (e0)
+            cudaEventDestroy(e0);
+        if (e1)
+            cudaEventDestroy(e1);
+        if (e != cudaSuccess)
+            return cuda_fail(ctx, e, "timing the batch graph");
+        ctx->launches += 3;
+        return check_device_errors(ctx, ctx->batch_stream);
+    };
+    for (int i = 0; i < 4; ++i) {
+        const int Lc = std::min(kDegrees[i], ctx->md.degree);
+        for (int lp = 0; lp < 6; ++lp) {
+            const int P = 1 << lp;
+            const int64_t nobj = (int64_t)ctx->num_sms * kWarpsPerSm * (32 / P);
+            std::vector<double> r(3 * nobj), v(3 * nobj), ro(3 * nobj), vo(3 * nobj);
+            for (int64_t o = 0; o < nobj; ++o) {
+                const double ang = 0.001 * (double)o, a = 7.0e6 + 10.0 * (double)(o % 97);
+                const double sp = std::sqrt(ctx->md.gm / a), inc = 0.3 + 1e-4 * (double)(o % 31);
+                r[3 * o] = a * std::cos(ang);
+                r[3 * o + 1] = a * std::sin(ang) * std::cos(inc);
+                r[3 * o + 2] = a * std::sin(ang) * std::sin(inc);
+                v[3 * o] = -sp * std::sin(ang);
+                v[3 * o + 1] = sp * std::cos(ang) * std::cos(inc);
+                v[3 * o + 2] = sp * std::cos(ang) * std::sin(inc);
+            }
+            gpop_request q { t0, 30.0, 0, Lc, nobj, r.data(), v.data(), ro.data(), vo.data() };
+            // pin the lanes: the planner keeps P for a request that fills the grid exactly
+            float ms_short = 0.f, ms_long = 0.f;
+            ctx->force_lpo = P;
+            gpop_status st = replay_ms(q, 8, ms_short);
+            if (st == GPOP_OK)
+                st = replay_ms(q, 24, ms_long);
+            ctx->force_lpo = 0;
+            if (st != GPOP_OK) {
+                ctx->tuned = saved;
+                return st;
+            }
+            const double dt = std::max(1e-6, (double)(ms_long - ms_short) * 1e-3);
+            measured[i][lp] = (double)nobj * 16.0 / dt / ctx->num_sms;
+        }
+    }
+    for (int i = 0; i < 4; ++i)
+        for (int lp = 0; lp < 6; ++lp)
+            ctx->eta[i][lp] = measured[i][lp];
+    ctx->tuned = true;
+    if (cache_path) {
+        std::ofstream f(cache_path);
+        for (int i = 0; i < 4; ++i)
+            for (int lp = 0; lp < 6; ++lp)
+                f << (int)mixed << " " << kDegrees[i] << " " << (1 << lp) << " " << ctx->eta[i][lp] << "\n";
+    }
+    return GPOP_OK;
+}
+
+} // extern "C"

@@ -39,6 +39,8 @@ struct DevBuf {
 
 } // namespace gpop
 
+struct BatchCache; // buffers and captured graph of the last batch (batch_api.cu)
+
 struct gpop_ctx {
     gpop_config cfg {};
     std::string data_dir;
@@ -55,6 +57,15 @@ struct gpop_ctx {
     int64_t launches = 0;
     // scratch
     gpop::DevBuf state, gen_m, prop_m, gen_sec, prop_sec, io_r, io_v;
+    // batched propagation: cached plan and graph, its stream and pinned staging buffer
+    BatchCache* batch = nullptr;
+    cudaStream_t batch_stream = nullptr;
+    void* batch_host = nullptr;
+    size_t batch_host_cap = 0;
+    // batched-kernel throughput (object-steps/s per SM) for degrees {8, 20, 36, 70} x lanes 1..32
+    bool tuned = false;
+    double eta[4][6] = {};
+    int force_lpo = 0; // lanes per object fixed by the autotuner while it measures (0 = planner)
 
     gpop::TableSrc table(bool mixed_mode) const
     {
@@ -114,4 +125,6 @@ gpop_status propagator_step(gpop_propagator* p, int steps, double* traj_r, doubl
     double* traj_a, cudaStream_t s);
 // Reads and clears the device error word (synchronises the stream).
 gpop_status check_device_errors(gpop_ctx* ctx, cudaStream_t s);
+// Frees the batch cache, stream and staging buffer of a context.
+void destroy_batch_cache(gpop_ctx* ctx);
 } // namespace gpop

@@ -26,7 +26,8 @@ constexpr int kMixedSplit = 8; // highest degree kept in FP64 in the mixed mode
 struct GravSmem {
     const GravEntry64* t64; // FP64 mode: full table; mixed mode: head table (n <= 8)
     const GravEntry32* t32; // mixed mode: full FP32 table (recursion constant stored negated, twice)
-    int L;
+    int L; // degree summed (<= Lt)
+    int Lt; // degree of the table layout (columns of Lt - m + 1 entries)
     double radius, gm;
 };
 
@@ -202,13 +203,13 @@ __device__ __forceinline__ void gravity_itrs(const GravSmem& gs, const double (&
             Q2[k] = 0.0;
         }
         if constexpr (!MIXED) {
-            const GravEntry64* e = gs.t64 + grav_col_offset(m, L);
+            const GravEntry64* e = gs.t64 + grav_col_offset(m, gs.Lt);
             s.add(e, Q1); // n = m
             column64<K>(e, 1, L - m, u, w, Q1, Q2, s);
         } else {
             ColSums32<K> f;
             f.zero();
-            const GravEntry32* e32 = gs.t32 + grav_col_offset(m, L);
+            const GravEntry32* e32 = gs.t32 + grav_col_offset(m, gs.Lt);
             float Q1f[K], Q2f[K];
             if (m <= kMixedSplit) {
                 const int top = L < kMixedSplit ? L : kMixedSplit;

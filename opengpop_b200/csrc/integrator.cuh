@@ -1,0 +1,134 @@
+// integrator.cuh -- RK8 startup and mid-corrector device code (lib/gpu_startup/src/gpu_startup.cu),
+// shared by the single-request and batched kernels. A force model F provides
+//   gen(r, v, step, k, a)  -- acceleration at RK8 stage k of startup step `step` (+-1..4)
+//   prop(r, v, idx, a)     -- acceleration at propagation epoch index idx (t = (idx - 4) h)
+#pragma once
+#include "gj8_tables.cuh"
+
+namespace gpop {
+
+// ---- RK8 startup and mid-corrector (lib/gpu_startup/src/gpu_startup.cu:55-318) ----
+struct StartupMats {
+    double r[9][3], v[9][3], a[9][3], s[9][3], S[9][3];
+};
+
+// RK8::step (gpu_startup.cu:108-144): stage state = base + h sum a_ki K_i; new column = base +
+// h sum b_k K_k, for both position (K = stage velocity) and velocity (K = acceleration).
+template <class F>
+__device__ void rk8_step(const F& f, double h, int step, StartupMats& m)
+{
+    const double hh = step > 0 ? h : -h;
+    const int base = 4 + step + (step > 0 ? -1 : 1);
+    double Kx[10][3], Kv[10][3];
+    double tx[3], tv[3];
+    for (int j = 0; j < 3; ++j) {
+        tx[j] = m.r[base][j];
+        tv[j] = m.v[base][j];
+        Kx[0][j] = tv[j];
+    }
+    f.gen(tx, tv, step, 0, Kv[0]);
+    for (int k = 1; k <= 9; ++k) {
+        for (int j = 0; j < 3; ++j) {
+            double sx = 0.0, sv = 0.0;
+            for (int i = 0; i < k; ++i) {
+                sx = fma(c_RKA[k - 1][i], Kx[i][j], sx);
+                sv = fma(c_RKA[k - 1][i], Kv[i][j], sv);
+            }
+            tx[j] = fma(hh, sx, m.r[base][j]);
+            tv[j] = fma(hh, sv, m.v[base][j]);
+        }
+        f.gen(tx, tv, step, k, Kv[k]);
+        for (int j = 0; j < 3; ++j)
+            Kx[k][j] = tv[j];
+    }
+    const int col = 4 + step;
+    for (int j = 0; j < 3; ++j) {
+        double sx = 0.0, sv = 0.0;
+        for (int k = 0; k < 10; ++k) {
+            sx = fma(Kx[k][j], c_RKB[k], sx);
+            sv = fma(Kv[k][j], c_RKB[k], sv);
+        }
+        m.v[col][j] = fma(hh, sv, m.v[base][j]);
+        m.r[col][j] = fma(hh, sx, m.r[base][j]);
+    }
+}
+
+// StartupCorrector::CalculateAccelerationMatrix (gpu_startup.cu:196-224)
+template <class F> __device__ void corrector_accel(const F& f, StartupMats& m, bool epoch)
+{
+    for (int i = 0; i < 9; ++i)
+        if (i != 4 || epoch)
+            f.prop(m.r[i], m.v[i], i, m.a[i]);
+}
+
+// StartupCorrector::CalculateS0 (gpu_startup.cu:170-195), Berry & Healy eqs. 73, 75, 86
+__device__ inline void corrector_s0(double h, StartupMats& m)
+{
+    const double hinv = 1 / h, h2inv = 1 / (h * h);
+    for (int j = 0; j < 3; ++j) {
+        double sb = 0.0, sa = 0.0;
+        for (int k = 0; k < 9; ++k) {
+            sb = fma(c_SA[4][k], m.a[k][j], sb);
+            sa = fma(c_GJ[4][k], m.a[k][j], sa);
+        }
+        m.s[4][j] = fma(hinv, m.v[4][j], -sb);
+        m.S[4][j] = fma(h2inv, m.r[4][j], -sa);
+    }
+}
+
+// CalculateAllSKernel (gpu_startup/src/device/calculate_all_s.cu:19-47)
+__device__ inline void corrector_all_s(StartupMats& m)
+{
+    for (int i = 1; i <= 4; ++i)
+        for (int j = 0; j < 3; ++j) {
+            m.s[4 + i][j] = m.s[4 + i - 1][j] + (m.a[4 + i - 1][j] + m.a[4 + i][j]) / 2;
+            m.s[4 - i][j] = m.s[4 - i + 1][j] - (m.a[4 - i + 1][j] + m.a[4 - i][j]) / 2;
+            m.S[4 + i][j] = m.s[4 + i - 1][j] + m.S[4 + i - 1][j] + m.a[4 + i - 1][j] / 2;
+            m.S[4 - i][j] = -m.s[4 - i + 1][j] + m.S[4 - i + 1][j] + m.a[4 - i + 1][j] / 2;
+        }
+}
+
+// StartupCorrector::Correct (gpu_startup.cu:247-294)
+template <class F> __device__ void corrector_correct(const F& f, double h, StartupMats& m)
+{
+    corrector_s0(h, m);
+    corrector_all_s(m);
+    const double h2 = h * h;
+    for (int c = 0; c < 9; ++c) {
+        if (c == 4)
+            continue; // the epoch column is restored
+        for (int j = 0; j < 3; ++j) {
+            double sv = 0.0, sr = 0.0;
+            for (int k = 0; k < 9; ++k) {
+                sv = fma(m.a[k][j], c_SA[c][k], sv);
+                sr = fma(m.a[k][j], c_GJ[c][k], sr);
+            }
+            m.v[c][j] = h * (sv + m.s[c][j]);
+            m.r[c][j] = h2 * (sr + m.S[c][j]);
+        }
+    }
+    corrector_accel(f, m, false);
+}
+
+template <class F>
+__device__ void run_startup(const F& f, double h, int ncorr, const double* r0, const double* v0, StartupMats& m)
+{
+    for (int c = 0; c < 9; ++c)
+        for (int j = 0; j < 3; ++j)
+            m.r[c][j] = m.v[c][j] = m.a[c][j] = m.s[c][j] = m.S[c][j] = 0.0;
+    for (int j = 0; j < 3; ++j) {
+        m.r[4][j] = r0[j];
+        m.v[4][j] = v0[j];
+    }
+    for (int i = 1; i <= 4; ++i) { // StartupPredictor::Predict (gpu_startup.cu:162-165)
+        rk8_step(f, h, i, m);
+        rk8_step(f, h, -i, m);
+    }
+    if (ncorr <= 0)
+        return;
+    corrector_accel(f, m, true);
+    for (int i = 0; i < ncorr; ++i)
+        corrector_correct(f, h, m);
+}
+
+} // namespace gpop
