@@ -156,6 +156,33 @@ gpop_status gpop_batch_plan(gpop_ctx* ctx, const gpop_request* reqs, int32_t n_r
  * uses. cache_path (may be NULL) is read if it exists and written otherwise. */
 gpop_status gpop_tune(gpop_ctx* ctx, const char* cache_path);
 
+/* ---- variational equations and adjoint (FP64; the reference has no counterpart) ----
+ * Derivatives of the discrete propagation map of gpop_propagate in FP64 (RK8 startup + GJ8 with
+ * the context's corrector passes, gravity at every iterate), with respect to the initial GCRS
+ * state x0 = (r0, v0). Host buffers. */
+/* Gravity acceleration (a_dev may be NULL) and its Jacobian jac_dev [n][3][3] = d a_i / d r_j at
+ * GCRS positions r_dev [n][3] with frame matrix frame9_dev (as gpop_gravity; NULL = identity).
+ * FP64, device buffers. */
+gpop_status gpop_gravity_jacobian(gpop_ctx* ctx, int64_t n, const double* r_dev,
+    const double* frame9_dev, double* a_dev, double* jac_dev, void* stream);
+/* 6x6 state transition matrices by the forward variational equations: stm_out [n][6][6],
+ * stm[i][j] = d x_N,i / d x0_j with x = (r, v); r_out, v_out (may be NULL) = the final state. */
+gpop_status gpop_stm(gpop_ctx* ctx, const gpop_time* start, double h, int32_t steps, int64_t n,
+    const double* r_in, const double* v_in, double* r_out, double* v_out, double* stm_out);
+/* Vector-Jacobian product by the adjoint (reverse) sweep, GJ8 state checkpointed every 64
+ * steps: grad_r0, grad_v0 [n][3] = d(sum r_bar . r_N + v_bar . v_N) / d(r0, v0). r_bar or v_bar
+ * may be NULL (zero). */
+gpop_status gpop_propagate_vjp(gpop_ctx* ctx, const gpop_time* start, double h, int32_t steps,
+    int64_t n, const double* r_in, const double* v_in, const double* r_bar, const double* v_bar,
+    double* grad_r0, double* grad_v0);
+/* Closest approach of listed pairs (pairs [n_pairs][2] object indices, a != b) over `steps` steps
+ * with the reference's running minimum, Hermite interpolation and secant TCA
+ * (closest_approach/src/device.cu:56-173), and the adjoint gradient of each miss distance:
+ * tca, miss [n_pairs]; grad [n_pairs][12] = d miss / d(r0_a, v0_a, r0_b, v0_b). */
+gpop_status gpop_miss_gradient(gpop_ctx* ctx, const gpop_time* start, double h, int32_t steps,
+    int64_t n, const double* r_in, const double* v_in, int64_t n_pairs, const int32_t* pairs,
+    double* tca, double* miss, double* grad);
+
 /* ---- startup and integrator pieces (device buffers, one object each) ---- */
 /* GpuStartup::Startup (gpu_startup.cu:55-68). Outputs 9 columns x 3 (column 4 = epoch):
  * r27, v27, a27, s27, S27 (device). n_corrections = 0 returns the RK8 guess only. */

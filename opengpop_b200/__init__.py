@@ -30,7 +30,8 @@ EXPORTS = (
     "gpop_gravity_degree", "gpop_kernel_launches", "gpop_propagate", "gpop_propagate_device",
     "gpop_propagate_device_noalloc", "gpop_propagate_trajectory", "gpop_propagator_create", "gpop_propagator_step",
     "gpop_propagator_steps_done", "gpop_propagator_destroy", "gpop_propagate_analytic",
-    "gpop_propagate_batch", "gpop_batch_plan", "gpop_tune", "gpop_startup", "gpop_corrector_unit",
+    "gpop_propagate_batch", "gpop_batch_plan", "gpop_tune", "gpop_gravity_jacobian", "gpop_stm", "gpop_propagate_vjp",
+    "gpop_miss_gradient", "gpop_startup", "gpop_corrector_unit",
     "gpop_predict_unit", "gpop_finalize_correction_unit", "gpop_gravity", "gpop_frame_matrices",
     "gpop_ca_create", "gpop_ca_create_analytic", "gpop_ca_propagate", "gpop_ca_find", "gpop_ca_pairs", "gpop_ca_num_pairs",
     "gpop_ca_trajectory", "gpop_ca_destroy",
@@ -102,6 +103,11 @@ def load_library(path=LIB_PATH):
         "gpop_propagate_batch": (i32, [_VP, _VP, i32]),
         "gpop_batch_plan": (i32, [_VP, _VP, i32, _VP, C.POINTER(f64)]),
         "gpop_tune": (i32, [_VP, C.c_char_p]),
+        "gpop_gravity_jacobian": (i32, [_VP, i64, _VP, _VP, _VP, _VP, _VP]),
+        "gpop_stm": (i32, [_VP, C.POINTER(Time), f64, i32, i64] + [_VP] * 5),
+        "gpop_propagate_vjp": (i32, [_VP, C.POINTER(Time), f64, i32, i64] + [_VP] * 6),
+        "gpop_miss_gradient": (i32, [_VP, C.POINTER(Time), f64, i32, i64, _VP, _VP, i64]
+                               + [_VP] * 4),
         "gpop_startup": (i32, [_VP, i32, C.POINTER(Time), f64, i32] + [_VP] * 8),
         "gpop_corrector_unit": (i32, [_VP, i32, f64, i32] + [_VP] * 6),
         "gpop_predict_unit": (i32, [_VP, i32, f64, i32] + [_VP] * 6),
@@ -304,6 +310,52 @@ class Context:
     def tune(self, cache_path=None):
         self._check(load_library().gpop_tune(
             self._h, None if cache_path is None else cache_path.encode()))
+
+    # ---- variational equations and adjoint (FP64) ----
+    def gravity_jacobian(self, r, jac, frame9=None, acc=None, stream=None):
+        """FP64 acceleration Jacobian [n, 3, 3] (device tensors) at GCRS positions r [n, 3]."""
+        self._check(load_library().gpop_gravity_jacobian(
+            self._h, int(r.shape[0]), _dptr(r), None if frame9 is None else _dptr(frame9),
+            None if acc is None else _dptr(acc), _dptr(jac), _stream_ptr(stream)))
+
+    def stm(self, start, h, steps, r, v):
+        """Returns (r_end, v_end, stm [n, 6, 6]) with stm[i, j] = d x_N,i / d x0_j, x = (r, v)."""
+        r = _host(r).reshape(-1, 3)
+        v = _host(v).reshape(-1, 3)
+        ro, vo = np.empty_like(r), np.empty_like(v)
+        phi = np.empty((r.shape[0], 6, 6))
+        self._check(load_library().gpop_stm(
+            self._h, C.byref(as_time(start)), float(h), int(steps), r.shape[0], r.ctypes.data,
+            v.ctypes.data, ro.ctypes.data, vo.ctypes.data, phi.ctypes.data))
+        return ro, vo, phi
+
+    def propagate_vjp(self, start, h, steps, r, v, r_bar=None, v_bar=None):
+        """Adjoint: d(sum r_bar . r_N + v_bar . v_N) / d(r0, v0) as two [n, 3] arrays."""
+        r = _host(r).reshape(-1, 3)
+        v = _host(v).reshape(-1, 3)
+        rb = None if r_bar is None else _host(r_bar).reshape(-1, 3)
+        vb = None if v_bar is None else _host(v_bar).reshape(-1, 3)
+        gr, gv = np.empty_like(r), np.empty_like(v)
+        self._check(load_library().gpop_propagate_vjp(
+            self._h, C.byref(as_time(start)), float(h), int(steps), r.shape[0], r.ctypes.data,
+            v.ctypes.data, None if rb is None else rb.ctypes.data,
+            None if vb is None else vb.ctypes.data, gr.ctypes.data, gv.ctypes.data))
+        return gr, gv
+
+    def miss_gradient(self, start, h, steps, r, v, pairs):
+        """Closest approach of listed pairs and the adjoint gradient of each miss distance:
+        returns (tca [p], miss [p], grad [p, 12] = d miss / d(r0_a, v0_a, r0_b, v0_b))."""
+        r = _host(r).reshape(-1, 3)
+        v = _host(v).reshape(-1, 3)
+        pr = np.ascontiguousarray(pairs, dtype=np.int32).reshape(-1, 2)
+        tca = np.empty(pr.shape[0])
+        miss = np.empty(pr.shape[0])
+        grad = np.empty((pr.shape[0], 12))
+        self._check(load_library().gpop_miss_gradient(
+            self._h, C.byref(as_time(start)), float(h), int(steps), r.shape[0], r.ctypes.data,
+            v.ctypes.data, pr.shape[0], pr.ctypes.data, tca.ctypes.data, miss.ctypes.data,
+            grad.ctypes.data))
+        return tca, miss, grad
 
     # ---- force model ----
     def gravity(self, r, a, frame9=None, precision=None, stream=None):

@@ -11,148 +11,11 @@
 #include "frames.cuh"
 #include "gravity.cuh"
 #include "integrator.cuh"
+#include "lanes.cuh"
 
 #include <type_traits>
 
 namespace gpop {
-
-__device__ __forceinline__ void cmul(double ac, double as, double bc, double bs, double& rc, double& rs)
-{
-    const double c = ac * bc - as * bs;
-    const double s = as * bc + ac * bs;
-    rc = c;
-    rs = s;
-}
-
-// (C1 + i S1)^p by binary powering (p >= 0).
-__device__ __forceinline__ void cpow(double c1, double s1, int p, double& rc, double& rs)
-{
-    double xc = 1.0, xs = 0.0, bc = c1, bs = s1;
-    while (p > 0) {
-        if (p & 1)
-            cmul(xc, xs, bc, bs, xc, xs);
-        p >>= 1;
-        if (p)
-            cmul(bc, bs, bc, bs, bc, bs);
-    }
-    rc = xc;
-    rs = xs;
-}
-
-// Gravity in the Earth-fixed frame with the columns split over the P lanes of an object
-// (lane l takes columns l, l + P, ...); the per-object totals are added across the P lanes.
-template <bool MIXED>
-__device__ __forceinline__ void gravity_itrs_lanes(const GravSmem& gs, int l, int P, double x,
-    double y, double z, double& ax, double& ay, double& az)
-{
-    const int L = gs.L, Lt = gs.Lt;
-    const double r = sqrt(x * x + y * y + z * z);
-    const double eps = z / r;
-    const double q = gs.radius / r;
-    const double u = q * eps, w = q * q;
-    const float uf = (float)u, wf = (float)w;
-    const double C1 = x / r, S1 = y / r;
-    double CP, SP, Cm, Sm, Cp, Sp, CPm1, SPm1;
-    cpow(C1, S1, P, CP, SP); // step between this lane's columns
-    cpow(C1, S1, l, Cm, Sm);
-    if (l > 0)
-        cpow(C1, S1, l - 1, Cp, Sp);
-    else
-        Cp = Sp = 0.0; // column 0 has no J, K or H part
-    cpow(C1, S1, P - 1, CPm1, SPm1); // (C + iS)_{P-1}: the m-1 values of column P
-    double qm = 1.0, qP = 1.0;
-    for (int i = 0; i < l; ++i)
-        qm *= q;
-    for (int i = 0; i < P; ++i)
-        qP *= q;
-    double G = 0.0, H = 0.0, J = 0.0, KK = 0.0;
-    for (int m = l; m <= L; m += P) {
-        ColSums64<1> s;
-        s.zero();
-        double Q1[1] = { qm }, Q2[1] = { 0.0 };
-        const double uu[1] = { u }, ww[1] = { w };
-        if constexpr (!MIXED) {
-            const GravEntry64* e = gs.t64 + grav_col_offset(m, Lt);
-            s.add(e, Q1);
-            column64<1>(e, 1, L - m, uu, ww, Q1, Q2, s);
-        } else {
-            ColSums32<1> f;
-            f.zero();
-            const GravEntry32* e32 = gs.t32 + grav_col_offset(m, Lt);
-            float Q1f[1], Q2f[1];
-            const float ufa[1] = { uf }, wfa[1] = { wf };
-            if (m <= kMixedSplit) {
-                const int top = L < kMixedSplit ? L : kMixedSplit;
-                const GravEntry64* e = gs.t64 + grav_col_offset(m, kMixedSplit);
-                s.add(e, Q1);
-                column64<1>(e, 1, top - m, uu, ww, Q1, Q2, s);
-                Q1f[0] = (float)Q1[0];
-                Q2f[0] = (float)Q2[0];
-                column32k<1>(e32, kMixedSplit + 1 - m, L - m, ufa, wfa, Q1f, Q2f, f);
-            } else {
-                const float4* p = reinterpret_cast<const float4*>(e32);
-                const float4 a = p[0], b = p[1];
-                const float Qm = (float)qm;
-                const float2 QQ = make_float2(Qm, Qm);
-                f.g[0] = __fmul2_rn(QQ, make_float2(a.z, a.w));
-                f.j[0] = __fmul2_rn(QQ, make_float2(b.x, b.y));
-                f.h[0] = __fmul2_rn(QQ, make_float2(b.z, b.w));
-                Q1f[0] = Qm;
-                Q2f[0] = 0.f;
-                column32k<1>(e32, 1, L - m, ufa, wfa, Q1f, Q2f, f);
-            }
-            s.g1[0] += (double)f.g[0].x;
-            s.g2[0] += (double)f.g[0].y;
-            s.j1[0] += (double)f.j[0].x;
-            s.j2[0] += (double)f.j[0].y;
-            s.h1[0] += (double)f.h[0].x;
-            s.h2[0] += (double)f.h[0].y;
-        }
-        const double dm = (double)m; // eq. 4-11
-        G += Cm * s.g1[0] + Sm * s.g2[0];
-        J += dm * (Cp * s.j1[0] + Sp * s.j2[0]);
-        KK -= dm * (Sp * s.j1[0] - Cp * s.j2[0]);
-        H += Cp * s.h1[0] + Sp * s.h2[0];
-        if (m == 0) {
-            Cp = CPm1;
-            Sp = SPm1;
-        } else {
-            cmul(Cp, Sp, CP, SP, Cp, Sp);
-        }
-        cmul(Cm, Sm, CP, SP, Cm, Sm);
-        qm *= qP;
-    }
-    for (int o = P >> 1; o > 0; o >>= 1) {
-        G += __shfl_xor_sync(0xffffffffu, G, o);
-        H += __shfl_xor_sync(0xffffffffu, H, o);
-        J += __shfl_xor_sync(0xffffffffu, J, o);
-        KK += __shfl_xor_sync(0xffffffffu, KK, o);
-    }
-    const double Gt = G + 1.0; // eq. 4-13
-    const double Lambda = Gt + z * H / r;
-    const double c = -gs.gm / (r * r);
-    ax = c * (Lambda * x / r - J);
-    ay = c * (Lambda * y / r - KK);
-    az = c * (Lambda * z / r - H);
-}
-
-template <bool MIXED>
-__device__ __forceinline__ void gravity_gcrs_lanes(const GravSmem& gs, int l, int P,
-    const double* __restrict__ M, const double* r, double* a)
-{
-    double m[9];
-#pragma unroll
-    for (int i = 0; i < 9; ++i)
-        m[i] = __ldg(M + i);
-    const double px = m[0] * r[0] + m[1] * r[1] + m[2] * r[2];
-    const double py = m[3] * r[0] + m[4] * r[1] + m[5] * r[2];
-    const double pz = m[6] * r[0] + m[7] * r[1] + m[8] * r[2];
-    double ax, ay, az;
-    gravity_itrs_lanes<MIXED>(gs, l, P, px, py, pz, ax, ay, az);
-    a[0] = m[0] * ax + m[3] * ay + m[6] * az;
-    a[1] = m[1] * ax + m[4] * ay + m[7] * az;
-    a[2] = m[2] * ax + m[5] * ay + m[8] * az;
-}
 
 // Force model of one request (startup kernel, one lane per object).
 template <bool MIXED> struct ForceReq {

@@ -1,26 +1,30 @@
 // integrator.cuh -- RK8 startup and mid-corrector device code (lib/gpu_startup/src/gpu_startup.cu),
-// shared by the single-request and batched kernels. A force model F provides
+// shared by the single-request, batched and variational kernels. A force model F provides
 //   gen(r, v, step, k, a)  -- acceleration at RK8 stage k of startup step `step` (+-1..4)
 //   prop(r, v, idx, a)     -- acceleration at propagation epoch index idx (t = (idx - 4) h)
+// The state type T is double, or a value with a tangent (variational equations): the startup is
+// linear in the state apart from the force evaluations, so only + - and scaling by constants are
+// applied to T.
 #pragma once
 #include "gj8_tables.cuh"
 
 namespace gpop {
 
 // ---- RK8 startup and mid-corrector (lib/gpu_startup/src/gpu_startup.cu:55-318) ----
-struct StartupMats {
-    double r[9][3], v[9][3], a[9][3], s[9][3], S[9][3];
+template <class T> struct StartupMatsT {
+    T r[9][3], v[9][3], a[9][3], s[9][3], S[9][3];
 };
+using StartupMats = StartupMatsT<double>;
 
 // RK8::step (gpu_startup.cu:108-144): stage state = base + h sum a_ki K_i; new column = base +
 // h sum b_k K_k, for both position (K = stage velocity) and velocity (K = acceleration).
-template <class F>
-__device__ void rk8_step(const F& f, double h, int step, StartupMats& m)
+template <class F, class T>
+__device__ void rk8_step(const F& f, double h, int step, StartupMatsT<T>& m)
 {
     const double hh = step > 0 ? h : -h;
     const int base = 4 + step + (step > 0 ? -1 : 1);
-    double Kx[10][3], Kv[10][3];
-    double tx[3], tv[3];
+    T Kx[10][3], Kv[10][3];
+    T tx[3], tv[3];
     for (int j = 0; j < 3; ++j) {
         tx[j] = m.r[base][j];
         tv[j] = m.v[base][j];
@@ -29,7 +33,7 @@ __device__ void rk8_step(const F& f, double h, int step, StartupMats& m)
     f.gen(tx, tv, step, 0, Kv[0]);
     for (int k = 1; k <= 9; ++k) {
         for (int j = 0; j < 3; ++j) {
-            double sx = 0.0, sv = 0.0;
+            T sx = 0.0, sv = 0.0;
             for (int i = 0; i < k; ++i) {
                 sx = fma(c_RKA[k - 1][i], Kx[i][j], sx);
                 sv = fma(c_RKA[k - 1][i], Kv[i][j], sv);
@@ -43,7 +47,7 @@ __device__ void rk8_step(const F& f, double h, int step, StartupMats& m)
     }
     const int col = 4 + step;
     for (int j = 0; j < 3; ++j) {
-        double sx = 0.0, sv = 0.0;
+        T sx = 0.0, sv = 0.0;
         for (int k = 0; k < 10; ++k) {
             sx = fma(Kx[k][j], c_RKB[k], sx);
             sv = fma(Kv[k][j], c_RKB[k], sv);
@@ -54,7 +58,7 @@ __device__ void rk8_step(const F& f, double h, int step, StartupMats& m)
 }
 
 // StartupCorrector::CalculateAccelerationMatrix (gpu_startup.cu:196-224)
-template <class F> __device__ void corrector_accel(const F& f, StartupMats& m, bool epoch)
+template <class F, class T> __device__ void corrector_accel(const F& f, StartupMatsT<T>& m, bool epoch)
 {
     for (int i = 0; i < 9; ++i)
         if (i != 4 || epoch)
@@ -62,11 +66,11 @@ template <class F> __device__ void corrector_accel(const F& f, StartupMats& m, b
 }
 
 // StartupCorrector::CalculateS0 (gpu_startup.cu:170-195), Berry & Healy eqs. 73, 75, 86
-__device__ inline void corrector_s0(double h, StartupMats& m)
+template <class T> __device__ inline void corrector_s0(double h, StartupMatsT<T>& m)
 {
     const double hinv = 1 / h, h2inv = 1 / (h * h);
     for (int j = 0; j < 3; ++j) {
-        double sb = 0.0, sa = 0.0;
+        T sb = 0.0, sa = 0.0;
         for (int k = 0; k < 9; ++k) {
             sb = fma(c_SA[4][k], m.a[k][j], sb);
             sa = fma(c_GJ[4][k], m.a[k][j], sa);
@@ -77,7 +81,7 @@ __device__ inline void corrector_s0(double h, StartupMats& m)
 }
 
 // CalculateAllSKernel (gpu_startup/src/device/calculate_all_s.cu:19-47)
-__device__ inline void corrector_all_s(StartupMats& m)
+template <class T> __device__ inline void corrector_all_s(StartupMatsT<T>& m)
 {
     for (int i = 1; i <= 4; ++i)
         for (int j = 0; j < 3; ++j) {
@@ -89,7 +93,7 @@ __device__ inline void corrector_all_s(StartupMats& m)
 }
 
 // StartupCorrector::Correct (gpu_startup.cu:247-294)
-template <class F> __device__ void corrector_correct(const F& f, double h, StartupMats& m)
+template <class F, class T> __device__ void corrector_correct(const F& f, double h, StartupMatsT<T>& m)
 {
     corrector_s0(h, m);
     corrector_all_s(m);
@@ -98,7 +102,7 @@ template <class F> __device__ void corrector_correct(const F& f, double h, Start
         if (c == 4)
             continue; // the epoch column is restored
         for (int j = 0; j < 3; ++j) {
-            double sv = 0.0, sr = 0.0;
+            T sv = 0.0, sr = 0.0;
             for (int k = 0; k < 9; ++k) {
                 sv = fma(m.a[k][j], c_SA[c][k], sv);
                 sr = fma(m.a[k][j], c_GJ[c][k], sr);
@@ -110,8 +114,8 @@ template <class F> __device__ void corrector_correct(const F& f, double h, Start
     corrector_accel(f, m, false);
 }
 
-template <class F>
-__device__ void run_startup(const F& f, double h, int ncorr, const double* r0, const double* v0, StartupMats& m)
+template <class F, class T>
+__device__ void run_startup(const F& f, double h, int ncorr, const T* r0, const T* v0, StartupMatsT<T>& m)
 {
     for (int c = 0; c < 9; ++c)
         for (int j = 0; j < 3; ++j)

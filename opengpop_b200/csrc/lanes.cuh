@@ -1,0 +1,341 @@
+// lanes.cuh -- gravity with the columns of the triangle split over the P lanes of an object
+// (lane l of P takes m = l, l + P, ...); the per-object sums are added with warp shuffles among
+// the lanes named by `mask` (the whole warp, or the object's aligned group of P lanes), so every
+// lane of the object ends with the same result. Used where one object per thread leaves
+// the GPU idle: long single requests of a batch and the variational/adjoint kernels.
+#pragma once
+#include "gravity.cuh"
+
+namespace gpop {
+
+__device__ __forceinline__ void cmul(double ac, double as, double bc, double bs, double& rc, double& rs)
+{
+    const double c = ac * bc - as * bs;
+    const double s = as * bc + ac * bs;
+    rc = c;
+    rs = s;
+}
+
+// (C1 + i S1)^p by binary powering (p >= 0).
+__device__ __forceinline__ void cpow(double c1, double s1, int p, double& rc, double& rs)
+{
+    double xc = 1.0, xs = 0.0, bc = c1, bs = s1;
+    while (p > 0) {
+        if (p & 1)
+            cmul(xc, xs, bc, bs, xc, xs);
+        p >>= 1;
+        if (p)
+            cmul(bc, bs, bc, bs, bc, bs);
+    }
+    rc = xc;
+    rs = xs;
+}
+
+// Gravity in the Earth-fixed frame with the columns split over the P lanes of an object
+// (lane l takes columns l, l + P, ...); the per-object totals are added across the P lanes.
+template <bool MIXED>
+__device__ __forceinline__ void gravity_itrs_lanes(const GravSmem& gs, int l, int P, double x,
+    double y, double z, double& ax, double& ay, double& az, unsigned mask = 0xffffffffu)
+{
+    const int L = gs.L, Lt = gs.Lt;
+    const double r = sqrt(x * x + y * y + z * z);
+    const double eps = z / r;
+    const double q = gs.radius / r;
+    const double u = q * eps, w = q * q;
+    const float uf = (float)u, wf = (float)w;
+    const double C1 = x / r, S1 = y / r;
+    double CP, SP, Cm, Sm, Cp, Sp, CPm1, SPm1;
+    cpow(C1, S1, P, CP, SP); // step between this lane's columns
+    cpow(C1, S1, l, Cm, Sm);
+    if (l > 0)
+        cpow(C1, S1, l - 1, Cp, Sp);
+    else
+        Cp = Sp = 0.0; // column 0 has no J, K or H part
+    cpow(C1, S1, P - 1, CPm1, SPm1); // (C + iS)_{P-1}: the m-1 values of column P
+    double qm = 1.0, qP = 1.0;
+    for (int i = 0; i < l; ++i)
+        qm *= q;
+    for (int i = 0; i < P; ++i)
+        qP *= q;
+    double G = 0.0, H = 0.0, J = 0.0, KK = 0.0;
+    for (int m = l; m <= L; m += P) {
+        ColSums64<1> s;
+        s.zero();
+        double Q1[1] = { qm }, Q2[1] = { 0.0 };
+        const double uu[1] = { u }, ww[1] = { w };
+        if constexpr (!MIXED) {
+            const GravEntry64* e = gs.t64 + grav_col_offset(m, Lt);
+            s.add(e, Q1);
+            column64<1>(e, 1, L - m, uu, ww, Q1, Q2, s);
+        } else {
+            ColSums32<1> f;
+            f.zero();
+            const GravEntry32* e32 = gs.t32 + grav_col_offset(m, Lt);
+            float Q1f[1], Q2f[1];
+            const float ufa[1] = { uf }, wfa[1] = { wf };
+            if (m <= kMixedSplit) {
+                const int top = L < kMixedSplit ? L : kMixedSplit;
+                const GravEntry64* e = gs.t64 + grav_col_offset(m, kMixedSplit);
+                s.add(e, Q1);
+                column64<1>(e, 1, top - m, uu, ww, Q1, Q2, s);
+                Q1f[0] = (float)Q1[0];
+                Q2f[0] = (float)Q2[0];
+                column32k<1>(e32, kMixedSplit + 1 - m, L - m, ufa, wfa, Q1f, Q2f, f);
+            } else {
+                const float4* p = reinterpret_cast<const float4*>(e32);
+                const float4 a = p[0], b = p[1];
+                const float Qm = (float)qm;
+                const float2 QQ = make_float2(Qm, Qm);
+                f.g[0] = __fmul2_rn(QQ, make_float2(a.z, a.w));
+                f.j[0] = __fmul2_rn(QQ, make_float2(b.x, b.y));
+                f.h[0] = __fmul2_rn(QQ, make_float2(b.z, b.w));
+                Q1f[0] = Qm;
+                Q2f[0] = 0.f;
+                column32k<1>(e32, 1, L - m, ufa, wfa, Q1f, Q2f, f);
+            }
+            s.g1[0] += (double)f.g[0].x;
+            s.g2[0] += (double)f.g[0].y;
+            s.j1[0] += (double)f.j[0].x;
+            s.j2[0] += (double)f.j[0].y;
+            s.h1[0] += (double)f.h[0].x;
+            s.h2[0] += (double)f.h[0].y;
+        }
+        const double dm = (double)m; // eq. 4-11
+        G += Cm * s.g1[0] + Sm * s.g2[0];
+        J += dm * (Cp * s.j1[0] + Sp * s.j2[0]);
+        KK -= dm * (Sp * s.j1[0] - Cp * s.j2[0]);
+        H += Cp * s.h1[0] + Sp * s.h2[0];
+        if (m == 0) {
+            Cp = CPm1;
+            Sp = SPm1;
+        } else {
+            cmul(Cp, Sp, CP, SP, Cp, Sp);
+        }
+        cmul(Cm, Sm, CP, SP, Cm, Sm);
+        qm *= qP;
+    }
+    for (int o = P >> 1; o > 0; o >>= 1) {
+        G += __shfl_xor_sync(mask, G, o);
+        H += __shfl_xor_sync(mask, H, o);
+        J += __shfl_xor_sync(mask, J, o);
+        KK += __shfl_xor_sync(mask, KK, o);
+    }
+    const double Gt = G + 1.0; // eq. 4-13
+    const double Lambda = Gt + z * H / r;
+    const double c = -gs.gm / (r * r);
+    ax = c * (Lambda * x / r - J);
+    ay = c * (Lambda * y / r - KK);
+    az = c * (Lambda * z / r - H);
+}
+
+template <bool MIXED>
+__device__ __forceinline__ void gravity_gcrs_lanes(const GravSmem& gs, int l, int P,
+    const double* __restrict__ M, const double* r, double* a, unsigned mask = 0xffffffffu)
+{
+    double m[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i)
+        m[i] = __ldg(M + i);
+    const double px = m[0] * r[0] + m[1] * r[1] + m[2] * r[2];
+    const double py = m[3] * r[0] + m[4] * r[1] + m[5] * r[2];
+    const double pz = m[6] * r[0] + m[7] * r[1] + m[8] * r[2];
+    double ax, ay, az;
+    gravity_itrs_lanes<MIXED>(gs, l, P, px, py, pz, ax, ay, az, mask);
+    a[0] = m[0] * ax + m[3] * ay + m[6] * az;
+    a[1] = m[1] * ax + m[4] * ay + m[7] * az;
+    a[2] = m[2] * ax + m[5] * ay + m[8] * az;
+}
+
+// ---- gravity Jacobian (FP64) ----
+// The column sums are functions of q = R/r and eps = z/r only, and Q(n,m) = q^n P(n,m)(eps) is
+// homogeneous of degree n in q, so dQ/dq = n Q / q and dQ/deps follows the recursion
+//   E(n) = q Q(n-1) + u E(n-1) - c w E(n-2),  E(m) = 0   (from Q(n) = u Q(n-1) - c w Q(n-2)).
+// Three sums per table entry (of Q, n Q and E) give each column's value and both partials; the
+// longitude dependence enters through (C1 + i S1)^m, whose partials are m (C1 + i S1)^(m-1) and
+// i m (C1 + i S1)^(m-1). G, J, K, H and their partials in (q, eps, C1, S1) are then chained to
+// the Earth-fixed position. Cost per (n, m) term: about 3 times one acceleration evaluation.
+struct JacF {
+    double v, q, e, c, s; // value and partials in q, eps, C1, S1
+};
+
+__device__ __forceinline__ void jac_warp_sum(double& x, int P, unsigned mask)
+{
+    for (int o = P >> 1; o > 0; o >>= 1)
+        x += __shfl_xor_sync(mask, x, o);
+}
+
+// Acceleration a and Jacobian Jm[i][j] = d a_i / d p_j in the Earth-fixed frame.
+// mask: the lanes of the object's group (the shuffles stay inside it).
+__device__ __forceinline__ void gravity_jac_itrs_lanes(const GravSmem& gs, int l, int P, double x,
+    double y, double z, double* a, double (*Jm)[3], unsigned mask)
+{
+    const int L = gs.L, Lt = gs.Lt;
+    const double r = sqrt(x * x + y * y + z * z);
+    const double invr = 1.0 / r;
+    const double eps = z / r;
+    const double q = gs.radius / r;
+    const double u = q * eps, w = q * q;
+    const double C1 = x / r, S1 = y / r;
+    JacF G { 0, 0, 0, 0, 0 }, J { 0, 0, 0, 0, 0 }, K { 0, 0, 0, 0, 0 }, H { 0, 0, 0, 0, 0 };
+    double CP, SP, qP = 1.0, qm = 1.0;
+    cpow(C1, S1, P, CP, SP);
+    for (int i = 0; i < P; ++i)
+        qP *= q;
+    for (int i = 0; i < l; ++i)
+        qm *= q;
+    double Cm = 0, Sm = 0, Cp = 0, Sp = 0, Cq = 0, Sq = 0; // z^m, z^(m-1), z^(m-2)
+    for (int m = l; m <= L; m += P) {
+        if (m == l || m - P < 2) { // first column of the lane, or a zero power to restart
+            cpow(C1, S1, m, Cm, Sm);
+            if (m >= 1)
+                cpow(C1, S1, m - 1, Cp, Sp);
+            else
+                Cp = Sp = 0.0;
+            if (m >= 2)
+                cpow(C1, S1, m - 2, Cq, Sq);
+            else
+                Cq = Sq = 0.0;
+        } else {
+            cmul(Cm, Sm, CP, SP, Cm, Sm);
+            cmul(Cp, Sp, CP, SP, Cp, Sp);
+            cmul(Cq, Sq, CP, SP, Cq, Sq);
+        }
+        const GravEntry64* e = gs.t64 + grav_col_offset(m, Lt);
+        // sums of Q, n Q and E times (g1, g2, j1, j2, h1, h2)
+        double s0[6], s1[6], s2[6];
+        {
+            const double2* p = reinterpret_cast<const double2*>(e);
+            const double2 g = p[1], j = p[2], h = p[3];
+            const double t[6] = { g.x, g.y, j.x, j.y, h.x, h.y };
+            const double nq = (double)m * qm;
+#pragma unroll
+            for (int k = 0; k < 6; ++k) {
+                s0[k] = t[k] * qm;
+                s1[k] = t[k] * nq;
+                s2[k] = 0.0;
+            }
+        }
+        double Q1 = qm, Q2 = 0.0, E1 = 0.0, E2 = 0.0, dn = (double)m;
+        for (int i = 1; i <= L - m; ++i) {
+            const double2* p = reinterpret_cast<const double2*>(e + i);
+            const double cw = p[0].x * w;
+            const double Q = fma(u, Q1, -cw * Q2);
+            const double E = fma(q, Q1, fma(u, E1, -cw * E2));
+            dn += 1.0;
+            const double nQ = dn * Q;
+            const double2 g = p[1], j = p[2], h = p[3];
+            const double t[6] = { g.x, g.y, j.x, j.y, h.x, h.y };
+#pragma unroll
+            for (int k = 0; k < 6; ++k) {
+                s0[k] = fma(t[k], Q, s0[k]);
+                s1[k] = fma(t[k], nQ, s1[k]);
+                s2[k] = fma(t[k], E, s2[k]);
+            }
+            Q2 = Q1;
+            Q1 = Q;
+            E2 = E1;
+            E1 = E;
+        }
+        const double dm = (double)m, dm1 = dm - 1.0;
+        // G = sum Re(z^m) g1 + Im(z^m) g2
+        G.v += Cm * s0[0] + Sm * s0[1];
+        G.q += Cm * s1[0] + Sm * s1[1];
+        G.e += Cm * s2[0] + Sm * s2[1];
+        G.c += dm * (Cp * s0[0] + Sp * s0[1]);
+        G.s += dm * (-Sp * s0[0] + Cp * s0[1]);
+        // J = sum m (Re(z^(m-1)) j1 + Im(z^(m-1)) j2)
+        J.v += dm * (Cp * s0[2] + Sp * s0[3]);
+        J.q += dm * (Cp * s1[2] + Sp * s1[3]);
+        J.e += dm * (Cp * s2[2] + Sp * s2[3]);
+        J.c += dm * dm1 * (Cq * s0[2] + Sq * s0[3]);
+        J.s += dm * dm1 * (-Sq * s0[2] + Cq * s0[3]);
+        // K = -sum m (Im(z^(m-1)) j1 - Re(z^(m-1)) j2)
+        K.v -= dm * (Sp * s0[2] - Cp * s0[3]);
+        K.q -= dm * (Sp * s1[2] - Cp * s1[3]);
+        K.e -= dm * (Sp * s2[2] - Cp * s2[3]);
+        K.c -= dm * dm1 * (Sq * s0[2] - Cq * s0[3]);
+        K.s -= dm * dm1 * (Cq * s0[2] + Sq * s0[3]);
+        // H = sum Re(z^(m-1)) h1 + Im(z^(m-1)) h2
+        H.v += Cp * s0[4] + Sp * s0[5];
+        H.q += Cp * s1[4] + Sp * s1[5];
+        H.e += Cp * s2[4] + Sp * s2[5];
+        H.c += dm1 * (Cq * s0[4] + Sq * s0[5]);
+        H.s += dm1 * (-Sq * s0[4] + Cq * s0[5]);
+        qm *= qP;
+    }
+    JacF* F[4] = { &G, &J, &K, &H };
+#pragma unroll
+    for (int f = 0; f < 4; ++f) {
+        jac_warp_sum(F[f]->v, P, mask);
+        jac_warp_sum(F[f]->q, P, mask);
+        jac_warp_sum(F[f]->e, P, mask);
+        jac_warp_sum(F[f]->c, P, mask);
+        jac_warp_sum(F[f]->s, P, mask);
+        F[f]->q /= q; // sums of n Q: q dQ/dq
+    }
+    const double ph[3] = { C1, S1, eps };
+    double gq[3], ge[3], gc[3], gsn[3]; // gradients of q, eps, C1, S1
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        gq[j] = -q * invr * ph[j];
+        ge[j] = ((j == 2 ? 1.0 : 0.0) - eps * ph[j]) * invr;
+        gc[j] = ((j == 0 ? 1.0 : 0.0) - C1 * ph[j]) * invr;
+        gsn[j] = ((j == 1 ? 1.0 : 0.0) - S1 * ph[j]) * invr;
+    }
+    double dF[4][3];
+#pragma unroll
+    for (int f = 0; f < 4; ++f)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+            dF[f][j] = F[f]->q * gq[j] + F[f]->e * ge[j] + F[f]->c * gc[j] + F[f]->s * gsn[j];
+    // a = c (Lambda p^ - P), P = (J, K, H), Lambda = 1 + G + eps H, c = -GM / r^2
+    const double Lambda = G.v + 1.0 + z * H.v / r;
+    const double c = -gs.gm / (r * r);
+    const double Pv[3] = { J.v, K.v, H.v };
+    const double* dP[3] = { dF[1], dF[2], dF[3] };
+    double dL[3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+        dL[j] = dF[0][j] + eps * dF[3][j] + H.v * ge[j];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const double base = Lambda * ph[i] - Pv[i];
+        a[i] = c * base;
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+            Jm[i][j] = -2.0 * c * ph[j] * invr * base
+                + c * (dL[j] * ph[i] + Lambda * ((i == j ? 1.0 : 0.0) - ph[i] * ph[j]) * invr - dP[i][j]);
+    }
+}
+
+// GCRS acceleration and Jacobian for the ITRS<-GCRS matrix M of gravity_gcrs: p = A r with
+// A[i][k] = M[3 i + k], a = A^T a_itrs, J = A^T J_itrs A.
+__device__ __forceinline__ void gravity_jac_gcrs_lanes(const GravSmem& gs, int l, int P,
+    const double* __restrict__ M, const double* r, double* a, double (*Jg)[3], unsigned mask)
+{
+    double A[3][3];
+#pragma unroll
+    for (int i = 0; i < 9; ++i)
+        A[i / 3][i % 3] = __ldg(M + i);
+    double p[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+        p[i] = A[i][0] * r[0] + A[i][1] * r[1] + A[i][2] * r[2];
+    double ai[3], Ji[3][3];
+    gravity_jac_itrs_lanes(gs, l, P, p[0], p[1], p[2], ai, Ji, mask);
+    double T[3][3]; // J_itrs A
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+            T[i][k] = Ji[i][0] * A[0][k] + Ji[i][1] * A[1][k] + Ji[i][2] * A[2][k];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        a[k] = A[0][k] * ai[0] + A[1][k] * ai[1] + A[2][k] * ai[2];
+#pragma unroll
+        for (int l2 = 0; l2 < 3; ++l2)
+            Jg[k][l2] = A[0][k] * T[0][l2] + A[1][k] * T[1][l2] + A[2][k] * T[2][l2];
+    }
+}
+
+} // namespace gpop
