@@ -11,7 +11,14 @@ import oracle_api as O
 pytestmark = pytest.mark.gpu
 
 START = (2024, 1, 1, 0, 0, 0.0)
-H_R, H_V = 1e-3, 1e-6  # finite-difference steps (m, m/s)
+# Central-difference steps (m, m/s). At the differentiation configuration's steps (1e-3 m,
+# 1e-6 m/s) the difference quotient of an FP64 propagation is limited by its rounding noise: about
+# 1e-4 relative after 24 h of LEO (the two perturbed runs round differently; measured 1.8e-4).
+# The resolved steps (1 m, 1e-3 m/s) keep the truncation error below 1e-7 and the noise below
+# 1e-8, so the 1e-5 bound is asserted against them; the configuration's steps are checked at
+# their noise level.
+H_R, H_V = 1.0, 1e-3
+H_R_CFG, H_V_CFG = 1e-3, 1e-6
 
 
 @pytest.fixture(scope="module")
@@ -84,11 +91,11 @@ def test_jacobian_matches_fd_of_oracle(ctx, oracle_data):
     assert res.max() < 1e-4
 
 
-def _fd_stm(ctx, steps, r, v, h=30.0):
+def _fd_stm(ctx, steps, r, v, h=30.0, hr=H_R, hv=H_V):
     n = r.shape[0]
     out = np.zeros((n, 6, 6))
     for j in range(6):
-        step = H_R if j < 3 else H_V
+        step = hr if j < 3 else hv
         dr = np.zeros((n, 3))
         dv = np.zeros((n, 3))
         (dr if j < 3 else dv)[:, j % 3] = step
@@ -107,9 +114,22 @@ def test_stm_matches_finite_differences(ctx, steps):
     r_ref, v_ref = ctx.propagate(START, 30.0, steps, r, v)
     assert np.abs(ro - r_ref).max() < 1e-6 and np.abs(vo - v_ref).max() < 1e-9
     fd = _fd_stm(ctx, steps, r, v)
-    for j in range(6):  # per column: 1e-5 relative
-        err = np.linalg.norm(phi[:, :, j] - fd[:, :, j], axis=1) / np.linalg.norm(fd[:, :, j], axis=1)
-        assert err.max() < 1e-5, (j, err.max())
+    err = np.linalg.norm(phi - fd, axis=1) / np.linalg.norm(fd, axis=1)  # per column
+    assert err.max() < 1e-5, err.max()
+
+
+def test_stm_one_day_leo(ctx):
+    # the differentiation configuration's duration (24 h at 30 s)
+    from opengpop_b200 import orbits
+    r, v = orbits.leo(4, seed=30)
+    steps = 2880
+    _, _, phi = ctx.stm(START, 30.0, steps, r, v)
+    fd = _fd_stm(ctx, steps, r, v)
+    err = np.linalg.norm(phi - fd, axis=1) / np.linalg.norm(fd, axis=1)
+    assert err.max() < 1e-5, err.max()
+    fd = _fd_stm(ctx, steps, r, v, hr=H_R_CFG, hv=H_V_CFG)
+    err = np.linalg.norm(phi - fd, axis=1) / np.linalg.norm(fd, axis=1)
+    assert err.max() < 1e-3, err.max()  # rounding-limited difference quotient
 
 
 def test_stm_zero_steps_is_identity(ctx):
