@@ -193,7 +193,10 @@ __device__ __forceinline__ void gravity_itrs(const GravSmem& gs, const double (&
         uf[k] = (float)u[k];
         wf[k] = (float)w[k];
     }
-    for (int m = 0; m <= L; ++m) {
+    // Mixed mode: columns m <= 8 are combined in FP64 below; the columns m > 8 (every term of
+    // degree > 8) are walked, combined and summed in FP32 after this loop.
+    const int Lhead = (MIXED && L > kMixedSplit) ? kMixedSplit : L;
+    for (int m = 0; m <= Lhead; ++m) {
         ColSums64<K> s;
         s.zero();
         double Q1[K], Q2[K];
@@ -263,6 +266,67 @@ __device__ __forceinline__ void gravity_itrs(const GravSmem& gs, const double (&
             Cm[k] = Cn;
             Sm[k] = Sn;
             qm[k] *= q[k];
+        }
+    }
+    if constexpr (MIXED) {
+        if (L > kMixedSplit) {
+            // the n = m term (Q = q^m) and the rest of each column in FP32; the column sums are
+            // combined with FP32 cos/sin(m lambda) and (R/r)^m recursions into FP32 partial G, J,
+            // K, H, added to the FP64 totals once
+            float cf[K], sf[K], cpf[K], spf[K], qmf[K], c1f[K], s1f[K], qf[K];
+            float Gf[K], Hf[K], Jf[K], Kf[K];
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                cf[k] = (float)Cm[k];
+                sf[k] = (float)Sm[k];
+                cpf[k] = (float)Cp[k];
+                spf[k] = (float)Sp[k];
+                qmf[k] = (float)qm[k];
+                c1f[k] = (float)C1[k];
+                s1f[k] = (float)S1[k];
+                qf[k] = (float)q[k];
+                Gf[k] = Hf[k] = Jf[k] = Kf[k] = 0.f;
+            }
+            for (int m = kMixedSplit + 1; m <= L; ++m) {
+                ColSums32<K> f;
+                f.zero();
+                const GravEntry32* e32 = gs.t32 + grav_col_offset(m, gs.Lt);
+                const float4* p = reinterpret_cast<const float4*>(e32);
+                const float4 a = p[0], b = p[1];
+                float Q1f[K], Q2f[K];
+#pragma unroll
+                for (int k = 0; k < K; ++k) {
+                    const float2 QQ = make_float2(qmf[k], qmf[k]);
+                    f.g[k] = __fmul2_rn(QQ, make_float2(a.z, a.w));
+                    f.j[k] = __fmul2_rn(QQ, make_float2(b.x, b.y));
+                    f.h[k] = __fmul2_rn(QQ, make_float2(b.z, b.w));
+                    Q1f[k] = qmf[k];
+                    Q2f[k] = 0.f;
+                }
+                column32k<K>(e32, 1, L - m, uf, wf, Q1f, Q2f, f);
+                const float dm = (float)m;
+#pragma unroll
+                for (int k = 0; k < K; ++k) {
+                    Gf[k] += cf[k] * f.g[k].x + sf[k] * f.g[k].y;
+                    Jf[k] += dm * (cpf[k] * f.j[k].x + spf[k] * f.j[k].y);
+                    Kf[k] -= dm * (spf[k] * f.j[k].x - cpf[k] * f.j[k].y);
+                    Hf[k] += cpf[k] * f.h[k].x + spf[k] * f.h[k].y;
+                    cpf[k] = cf[k];
+                    spf[k] = sf[k];
+                    const float cn = c1f[k] * cf[k] - s1f[k] * sf[k];
+                    const float sn = s1f[k] * cf[k] + c1f[k] * sf[k];
+                    cf[k] = cn;
+                    sf[k] = sn;
+                    qmf[k] *= qf[k];
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                G[k] += (double)Gf[k];
+                H[k] += (double)Hf[k];
+                J[k] += (double)Jf[k];
+                KK[k] += (double)Kf[k];
+            }
         }
     }
 #pragma unroll
