@@ -199,19 +199,228 @@ def probe_peak(torch, fp64, dev):
     return best
 
 
+# ---- auxiliary workloads (one GPU; each prints its own JSON line) ----
+def w_jac(L):
+    """FP64 flops of one gravity evaluation with its 3x3 Jacobian at degree L: per (n, m) term
+    the Q and dQ/deps recursions (7) and 18 sums (36) plus n Q (1); per column about 100."""
+    return 44 * terms(L) + 100 * (L + 1) + 200
+
+
+def _peaks(torch, dev):
+    return probe_peak(torch, True, dev), probe_peak(torch, False, dev)
+
+
+def _common(args, metric, value, unit, dtype, config, extra):
+    line = {"metric": metric, "value": value, "unit": unit, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": dtype, "data": "synthetic", "config": config}
+    line.update(extra)
+    print(json.dumps(line), flush=True)
+
+
+def run_batch(args, torch, G, dev):
+    """Batched uneven requests: 4,096 requests in one persistent launch under a captured graph."""
+    from opengpop_b200 import orbits
+    reqs = orbits.batch_requests(4096, SEED)
+    osteps = sum(q["r"].shape[0] * q["steps"] for q in reqs)
+    f_total = sum(q["r"].shape[0] * q["steps"] * flops_per_object_step(q["degree"]) for q in reqs)
+    f32 = sum(q["r"].shape[0] * q["steps"] * fp32_flops_per_object_step(q["degree"])
+              for q in reqs if q["degree"] > 8)
+    ctx = G.Context(precision=G.MIXED)
+    t0 = time.perf_counter()
+    ctx.tune()
+    tune_s = time.perf_counter() - t0
+    lpo, est = ctx.batch_plan(reqs)
+    sampler = ClockSampler(torch.cuda.current_device())
+    for _ in range(args.warmup):
+        ctx.propagate_batch(reqs)
+    sampler.start()
+    dev_t, wall_t = [], []
+    launches0 = ctx.kernel_launches
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        ctx.propagate_batch(reqs)
+        wall_t.append(time.perf_counter() - t0)
+        dev_t.append(ctx.batch_device_seconds)
+    clocks = sampler.stop()
+    launches = ctx.kernel_launches - launches0
+    ctx.close()
+    t = sum(dev_t) / len(dev_t)
+    peak64, peak32 = _peaks(torch, dev)
+    achieved = f_total / t / 1e12
+    t_min = (f_total - f32) / (peak64 * 1e12) + f32 / (peak32 * 1e12) if peak64 and peak32 else None
+    io = sum(q["r"].shape[0] for q in reqs) * 6 * 8
+    _common(args, "object-steps/s, batched uneven requests (mixed precision)", osteps / t,
+            "object-steps/s", "f64+f32",
+            {"workload": "4,096 requests (objects log-uniform 1-512, 1 h-7 d, h in {10,30,60,120} s, "
+                         "degree in {8,20,36,70}, seed %d), one persistent launch per batch" % SEED,
+             "object_steps_per_batch": osteps, "l2": "inputs (and state) larger than L2",
+             "lanes_per_object_histogram": np.bincount(lpo, minlength=33)[[1, 2, 4, 8, 16, 32]].tolist(),
+             "planner_estimate_s": est, "tune_s": tune_s},
+            {"ms_per_step": 1e3 * t,
+             "requests_per_s": len(reqs) / t,
+             "e2e": {"value": osteps / (sum(wall_t) / len(wall_t)), "unit": "object-steps/s",
+                     "h2d_bytes_per_step": io, "d2h_bytes_per_step": io,
+                     "call": "gpop_propagate_batch (host buffers, packing, copies)"},
+             "roofline": {"bound": "fp64+fp32", "achieved": achieved,
+                          "peak": f_total / t_min / 1e12 if t_min else None, "unit": "TFLOP/s",
+                          "frac": achieved / (f_total / t_min / 1e12) if t_min else None,
+                          "traffic": None},
+             "cpu_baseline": None, "clocks": clocks, "gpu_launches": launches})
+    return 0
+
+
+def run_screen(args, torch, G, dev):
+    """Closest approach: 20,000 LEO objects, 2,000 seed-chosen objects against all (2,000
+    singleton sets plus one set of 18,000: 37,999,000 pairs), 70x70, 30 s, 3 days, 5 km."""
+    from opengpop_b200 import orbits
+    n, n_sel, steps, thr = 20000, 2000, 8640, 5000.0
+    r, v = orbits.leo(n, SEED)
+    sel = np.random.default_rng(SEED).choice(n, n_sel, replace=False)
+    order = np.concatenate([sel, np.setdiff1d(np.arange(n), sel)])
+    r, v = r[order], v[order]
+    set_ids = np.concatenate([np.arange(n_sel), np.full(n - n_sel, n_sel)]).astype(np.uint32)
+    ctx = G.Context(precision=G.FP64)
+    sampler = ClockSampler(torch.cuda.current_device())
+    res = []
+    for i in range(args.warmup + args.steps):
+        if i == args.warmup:
+            sampler.start()
+        t0 = time.perf_counter()
+        ca = ctx.closest_approach(START, H, r, v, set_ids)
+        ca.propagate(steps)
+        recs = ca.find(thr)
+        wall = time.perf_counter() - t0
+        dt = ca.device_seconds()
+        pairs = ca.num_pairs
+        ca.close()
+        if i >= args.warmup:
+            res.append((wall, dt))
+    clocks = sampler.stop()
+    ctx.close()
+    wall = float(np.mean([x[0] for x in res]))
+    t_prop, t_screen, t_refine = (float(np.mean([x[1][k] for x in res])) for k in range(3))
+    pair_steps = pairs * steps
+    peak64 = probe_peak(torch, True, dev)
+    achieved = 9.0 * pair_steps / t_screen / 1e12
+    _common(args, "conjunction pair-steps/s of the screen (FP64)", pair_steps / t_screen,
+            "pair-steps/s", "f64",
+            {"workload": "20,000 LEO objects (seed %d), 2,000 vs all = %d pairs, 70x70, 30 s, "
+                         "%d steps (3 days), threshold 5 km" % (SEED, pairs, steps),
+             "pairs": pairs, "steps": steps, "l2": "trajectory store 12 GB > L2"},
+            {"ms_per_step": 1e3 * wall,
+             "device_seconds": {"propagation": t_prop, "screen": t_screen, "refinement": t_refine},
+             "pairs_per_s_whole_job": pairs / wall,
+             "found_below_threshold": len(recs),
+             "e2e": {"value": pair_steps / wall, "unit": "pair-steps/s",
+                     "h2d_bytes_per_step": n * 6 * 8 + n * 4, "d2h_bytes_per_step": len(recs) * 64,
+                     "call": "gpop_ca_create + gpop_ca_propagate + gpop_ca_find"},
+             "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak64, "unit": "TFLOP/s",
+                          "frac": achieved / peak64 if peak64 else None, "traffic": None,
+                          "per_unit": "9 FP64 flops per pair-step"},
+             "cpu_baseline": None, "clocks": clocks})
+    return 0
+
+
+def run_adjoint(args, torch, G, dev):
+    """Differentiation: 10,000 pairs (24 h, 30 s, 70x70, FP64), adjoint gradient of each miss
+    distance; and 8,192 state transition matrices by the forward variational equations."""
+    from opengpop_b200 import orbits
+    n_pairs, steps, n_stm = 10000, 2880, 8192
+    r, v, pairs = orbits.conjunction_pairs(n_pairs, SEED)
+    ctx = G.Context(precision=G.FP64)
+    sampler = ClockSampler(torch.cuda.current_device())
+    t_miss, t_stm = [], []
+    for i in range(args.warmup + args.steps):
+        if i == args.warmup:
+            sampler.start()
+        t0 = time.perf_counter()
+        ctx.miss_gradient(START, H, steps, r, v, pairs)
+        t1 = time.perf_counter()
+        ctx.stm(START, H, steps, r[:n_stm], v[:n_stm])
+        t2 = time.perf_counter()
+        if i >= args.warmup:
+            t_miss.append(t1 - t0)
+            t_stm.append(t2 - t1)
+    clocks = sampler.stop()
+    ctx.close()
+    tm, ts = float(np.mean(t_miss)), float(np.mean(t_stm))
+    # work of the miss-gradient call: forward propagation of 2 n_pairs objects, then per unit
+    # (pair side) a recomputed forward pass (7 W per step), the reverse pass (7 Jacobian
+    # evaluations per step) and the tangent startup (145 Jacobian evaluations)
+    W = 24 * terms(DEGREE) + 15 * DEGREE + 60
+    units = 2 * n_pairs
+    f_miss = units * steps * (2 * flops_per_object_step() + 7 * w_jac(DEGREE)) + units * 145 * w_jac(DEGREE)
+    f_stm = n_stm * steps * (7 * w_jac(DEGREE) + 6 * 500) + n_stm * 145 * w_jac(DEGREE)
+    peak64 = probe_peak(torch, True, dev)
+    ach = f_miss / tm / 1e12
+    _common(args, "miss-distance gradients/s (adjoint, FP64)", n_pairs / tm, "pairs/s", "f64",
+            {"workload": "%d LEO pairs (seed %d), 70x70, 30 s, %d steps (24 h), checkpoint every 64 "
+                         "steps; %d STMs over the same span" % (n_pairs, SEED, steps, n_stm)},
+            {"ms_per_step": 1e3 * tm,
+             "stm": {"value": n_stm * steps / ts, "unit": "object-steps/s (with 6x6 STM)",
+                     "seconds": ts, "roofline_frac": (f_stm / ts / 1e12) / peak64 if peak64 else None},
+             "e2e": {"value": n_pairs / tm, "unit": "pairs/s", "h2d_bytes_per_step": units * 48,
+                     "d2h_bytes_per_step": n_pairs * 14 * 8, "call": "gpop_miss_gradient"},
+             "roofline": {"bound": "fp64", "achieved": ach, "peak": peak64, "unit": "TFLOP/s",
+                          "frac": ach / peak64 if peak64 else None, "traffic": None,
+                          "per_unit": "per unit-step 2 (7 W + 500) + 7 W_J, W(70) = %d, "
+                                      "W_J(70) = %d flops" % (W, w_jac(DEGREE))},
+             "cpu_baseline": None, "clocks": clocks})
+    return 0
+
+
+def accuracy_7d(G, n_sample):
+    """Mixed vs FP64 position error after 7 days (20,160 steps) on n_sample objects spread over
+    the population."""
+    from opengpop_b200 import orbits
+    r, v = orbits.mixed_population(N_OBJECTS, SEED)
+    idx = np.linspace(0, N_OBJECTS - 1, n_sample).astype(int)
+    out = {}
+    for name, prec in (("fp64", G.FP64), ("mixed", G.MIXED)):
+        c = G.Context(precision=prec)
+        out[name] = c.propagate(START, H, 20160, r[idx], v[idx])
+        c.close()
+    err = np.linalg.norm(out["mixed"][0] - out["fp64"][0], axis=1)
+    return {"objects": int(n_sample), "days": 7, "steps": 20160, "max_m": float(err.max()),
+            "p99_m": float(np.percentile(err, 99)), "median_m": float(np.median(err)),
+            "bound_m": 1.0}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
-    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=None,
+                    help="timed steps (default 10; batch 2, screen and adjoint 1)")
+    ap.add_argument("--warmup", type=int, default=None,
+                    help="warm-up steps (default 3; batch, screen and adjoint 1)")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--prop-steps", type=int, default=64, help="GJ8 steps per bench step")
     ap.add_argument("--objects", type=int, default=N_OBJECTS)
     ap.add_argument("--e2e-steps", type=int, default=960, help="GJ8 steps per e2e call")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="propagate",
+                    choices=["propagate", "batch", "screen", "adjoint"],
+                    help="propagate: the headline line; the others print their own line (1 GPU)")
+    ap.add_argument("--accuracy-objects", type=int, default=8192,
+                    help="objects of the 7-day mixed-vs-FP64 error sample (0 = skip)")
     args = ap.parse_args()
+    short = args.workload != "propagate"  # whole-job workloads of several seconds per step
+    if args.steps is None:
+        args.steps = {"batch": 2, "screen": 1, "adjoint": 1}.get(args.workload, 10)
+    if args.warmup is None:
+        args.warmup = 1 if short else 3
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload != "propagate":
+        if env_int("RANK", 0) != 0:
+            return 0
+        import torch
+        import opengpop_b200 as G
+        dev = torch.device("cuda", env_int("LOCAL_RANK", 0))
+        torch.cuda.set_device(dev)
+        return {"batch": run_batch, "screen": run_screen, "adjoint": run_adjoint}[args.workload](
+            args, torch, G, dev)
 
     import torch
     import torch.distributed as dist
@@ -321,6 +530,8 @@ def main():
     fp64_launch_t = sum(times_fp64) / max(1, launches_fp64)
     fp64_achieved = flops_per_object_step() * n * steps_per_launch / fp64_launch_t / 1e12
 
+    accuracy = accuracy_7d(G, args.accuracy_objects) if args.accuracy_objects > 0 and rank == 0 else None
+
     if rank == 0:
         cpu = None
         if not args.no_cpu_baseline:
@@ -345,6 +556,7 @@ def main():
                                   "unit": "TFLOP/s",
                                   "frac": fp64_achieved / peak64 if peak64 else None}},
             "mixed_vs_fp64": value / value_fp64,
+            "accuracy_7d": accuracy,
             "e2e": {"value": e2e_value, "unit": "object-steps/s",
                     "h2d_bytes_per_step": 2 * n * 3 * 8, "d2h_bytes_per_step": 2 * n * 3 * 8,
                     "call": "gpop_propagate, %d GJ8 steps per call incl. startup" % e2e_steps},

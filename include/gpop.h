@@ -151,6 +151,9 @@ gpop_status gpop_propagate_batch(gpop_ctx* ctx, const gpop_request* reqs, int32_
 /* The batch plan: lanes per object chosen for each request and the estimated makespan (s). */
 gpop_status gpop_batch_plan(gpop_ctx* ctx, const gpop_request* reqs, int32_t n_req,
     int32_t* lanes_per_object, double* est_seconds);
+/* Device time (s, CUDA events) of the last gpop_propagate_batch launch: frames, startup and the
+ * persistent GJ8 kernel, without the host copies. */
+double gpop_batch_device_seconds(const gpop_ctx* ctx);
 /* Autotuner: measures the throughput of the batched GJ8 kernel for each gravity degree in
  * {8, 20, 36, 70} (up to the context's) and 1..32 lanes per object, which the batch planner then
  * uses. cache_path (may be NULL) is read if it exists and written otherwise. */
@@ -244,6 +247,9 @@ int64_t gpop_ca_num_pairs(const gpop_ca* ca);
 /* Device trajectory of the propagated phases ([steps][3][n] SoA), for inspection and tests. */
 gpop_status gpop_ca_trajectory(gpop_ca* ca, double* r_host, double* v_host, double* a_host,
     int32_t* steps_out);
+/* Cumulative device time (s, CUDA events) of this object's propagation, screen and TCA refinement:
+ * out3 = {propagation, screen, refinement}. No counterpart in the reference. */
+gpop_status gpop_ca_device_seconds(const gpop_ca* ca, double* out3);
 void gpop_ca_destroy(gpop_ca* ca);
 
 #if defined(__GNUC__)

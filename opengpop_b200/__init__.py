@@ -30,11 +30,11 @@ EXPORTS = (
     "gpop_gravity_degree", "gpop_kernel_launches", "gpop_propagate", "gpop_propagate_device",
     "gpop_propagate_device_noalloc", "gpop_propagate_trajectory", "gpop_propagator_create", "gpop_propagator_step",
     "gpop_propagator_steps_done", "gpop_propagator_destroy", "gpop_propagate_analytic",
-    "gpop_propagate_batch", "gpop_batch_plan", "gpop_tune", "gpop_gravity_jacobian", "gpop_stm", "gpop_propagate_vjp",
+    "gpop_propagate_batch", "gpop_batch_plan", "gpop_tune", "gpop_batch_device_seconds", "gpop_gravity_jacobian", "gpop_stm", "gpop_propagate_vjp",
     "gpop_miss_gradient", "gpop_startup", "gpop_corrector_unit",
     "gpop_predict_unit", "gpop_finalize_correction_unit", "gpop_gravity", "gpop_frame_matrices",
     "gpop_ca_create", "gpop_ca_create_analytic", "gpop_ca_propagate", "gpop_ca_find", "gpop_ca_pairs", "gpop_ca_num_pairs",
-    "gpop_ca_trajectory", "gpop_ca_destroy",
+    "gpop_ca_trajectory", "gpop_ca_device_seconds", "gpop_ca_destroy",
 )
 
 
@@ -103,6 +103,7 @@ def load_library(path=LIB_PATH):
         "gpop_propagate_batch": (i32, [_VP, _VP, i32]),
         "gpop_batch_plan": (i32, [_VP, _VP, i32, _VP, C.POINTER(f64)]),
         "gpop_tune": (i32, [_VP, C.c_char_p]),
+        "gpop_batch_device_seconds": (f64, [_VP]),
         "gpop_gravity_jacobian": (i32, [_VP, i64, _VP, _VP, _VP, _VP, _VP]),
         "gpop_stm": (i32, [_VP, C.POINTER(Time), f64, i32, i64] + [_VP] * 5),
         "gpop_propagate_vjp": (i32, [_VP, C.POINTER(Time), f64, i32, i64] + [_VP] * 6),
@@ -121,6 +122,7 @@ def load_library(path=LIB_PATH):
         "gpop_ca_pairs": (i32, [_VP] * 6),
         "gpop_ca_num_pairs": (i64, [_VP]),
         "gpop_ca_trajectory": (i32, [_VP] * 4 + [C.POINTER(i32)]),
+        "gpop_ca_device_seconds": (i32, [_VP, _VP]),
         "gpop_ca_destroy": (None, [_VP]),
     }
     for name, (res, args) in sig.items():
@@ -307,6 +309,11 @@ class Context:
                                                    lpo.ctypes.data_as(_VP), C.byref(est)))
         return lpo, est.value
 
+    @property
+    def batch_device_seconds(self):
+        """Device time of the last propagate_batch launch (without host copies)."""
+        return load_library().gpop_batch_device_seconds(self._h)
+
     def tune(self, cache_path=None):
         self._check(load_library().gpop_tune(
             self._h, None if cache_path is None else cache_path.encode()))
@@ -469,6 +476,12 @@ class ClosestApproach:
             self._h, d.ctypes.data_as(_VP), t.ctypes.data_as(_VP), pa.ctypes.data_as(_VP),
             pb.ctypes.data_as(_VP), cs.ctypes.data_as(_VP)))
         return dict(distance=d, time=t, posA=pa, posB=pb, closest_step=cs)
+
+    def device_seconds(self):
+        """Cumulative device seconds (propagation, screen, refinement)."""
+        out = np.zeros(3)
+        self.ctx._check(load_library().gpop_ca_device_seconds(self._h, out.ctypes.data_as(_VP)))
+        return out
 
     def trajectory(self):
         lib = load_library()

@@ -428,15 +428,19 @@ gpop_status gpop_propagate_batch(gpop_ctx* ctx, const gpop_request* reqs, int32_
         }
         bc->sig = sig;
     }
+    DeviceTimer timer;
+    timer.mark(s);
     if ((e = cudaGraphLaunch(bc->exec, s)) != cudaSuccess)
         return cuda_fail(ctx, e, "batch graph launch");
     ctx->launches += 3;
+    timer.mark(s);
     if ((e = cudaMemcpyAsync(host + 6 * N, dio + 6 * N, (size_t)N * 6 * sizeof(double), cudaMemcpyDeviceToHost, s))
         != cudaSuccess)
         return cuda_fail(ctx, e, "batch download");
     st = check_device_errors(ctx, s);
     if (st != GPOP_OK)
         return st;
+    ctx->batch_seconds = timer.seconds(0, 1);
     for (int i = 0; i < n_req; ++i) {
         if (obj0[i] < 0)
             continue;
@@ -445,6 +449,8 @@ gpop_status gpop_propagate_batch(gpop_ctx* ctx, const gpop_request* reqs, int32_
     }
     return GPOP_OK;
 }
+
+double gpop_batch_device_seconds(const gpop_ctx* ctx) { return ctx ? ctx->batch_seconds : -1.0; }
 
 gpop_status gpop_tune(gpop_ctx* ctx, const char* cache_path)
 {

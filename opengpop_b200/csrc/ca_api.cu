@@ -33,6 +33,8 @@ struct gpop_ca {
     bool refined = false;
     // propagation scratch
     DevBuf state, gen_m, prop_m;
+    // cumulative device time (s) of propagation, screen and refinement (CUDA events)
+    double t_prop = 0, t_screen = 0, t_refine = 0;
 
     ~gpop_ca()
     {
@@ -98,11 +100,15 @@ gpop_status refine(gpop_ca* ca, cudaStream_t s)
     a.time = ca->time.as<double>();
     a.pos_a = ca->pos_a.as<double>();
     a.pos_b = ca->pos_b.as<double>();
+    DeviceTimer timer;
+    timer.mark(s);
     if ((e = launch_refine(a, s)) != cudaSuccess)
         return cuda_fail(ctx, e, "refine kernel");
     ctx->launches++;
+    timer.mark(s);
     if ((e = cudaStreamSynchronize(s)) != cudaSuccess)
         return cuda_fail(ctx, e, "refine kernel");
+    ca->t_refine += timer.seconds(0, 1);
     ca->refined = true;
     return GPOP_OK;
 }
@@ -283,12 +289,15 @@ gpop_status gpop_ca_propagate(gpop_ca* ca, int32_t steps)
     p.gen_m = &ca->gen_m;
     p.prop_m = &ca->prop_m;
     const size_t off = (size_t)ca->total_steps * 3 * ca->n;
+    DeviceTimer timer;
+    timer.mark(s);
     gpop_status st = propagator_init(&p, s);
     if (st == GPOP_OK)
         st = propagator_step(&p, steps, ca->traj_r.as<double>() + off, ca->traj_v.as<double>() + off,
             ca->traj_a.as<double>() + off, s);
     if (st != GPOP_OK)
         return st;
+    timer.mark(s);
     ScreenArgs a;
     a.n = ca->n;
     a.traj_r = ca->traj_r.as<double>();
@@ -304,8 +313,11 @@ gpop_status gpop_ca_propagate(gpop_ca* ca, int32_t steps)
     if ((e = launch_screen(a, ca->num_tiles, s)) != cudaSuccess)
         return cuda_fail(ctx, e, "screen kernel");
     ctx->launches++;
+    timer.mark(s);
     if ((e = cudaStreamSynchronize(s)) != cudaSuccess)
         return cuda_fail(ctx, e, "screen kernel");
+    ca->t_prop += timer.seconds(0, 1);
+    ca->t_screen += timer.seconds(1, 2);
     ca->total_steps = need;
     ca->refined = false;
     return GPOP_OK;
@@ -438,6 +450,16 @@ gpop_status gpop_ca_trajectory(gpop_ca* ca, double* r_host, double* v_host, doub
     if (a_host && e == cudaSuccess)
         e = cudaMemcpy(a_host, ca->traj_a.p, bytes, cudaMemcpyDeviceToHost);
     return e == cudaSuccess ? GPOP_OK : cuda_fail(ca->ctx, e, "copying the trajectory");
+}
+
+gpop_status gpop_ca_device_seconds(const gpop_ca* ca, double* out3)
+{
+    if (!ca || !out3)
+        return GPOP_ERR_INVALID_ARG;
+    out3[0] = ca->t_prop;
+    out3[1] = ca->t_screen;
+    out3[2] = ca->t_refine;
+    return GPOP_OK;
 }
 
 void gpop_ca_destroy(gpop_ca* ca) { delete ca; }

@@ -37,6 +37,35 @@ struct DevBuf {
     template <class T> T* as() const { return static_cast<T*>(p); }
 };
 
+// Up to four CUDA events on one stream; seconds(a, b) after the stream has passed mark b.
+struct DeviceTimer {
+    cudaEvent_t ev[4] = {};
+    int n = 0;
+    void mark(cudaStream_t s)
+    {
+        if (n >= 4)
+            return;
+        if (cudaEventCreate(&ev[n]) == cudaSuccess)
+            cudaEventRecord(ev[n], s);
+        else
+            ev[n] = nullptr;
+        ++n;
+    }
+    double seconds(int a, int b) const
+    {
+        float ms = 0.f;
+        if (a < n && b < n && ev[a] && ev[b] && cudaEventElapsedTime(&ms, ev[a], ev[b]) == cudaSuccess)
+            return ms * 1e-3;
+        return 0.0;
+    }
+    ~DeviceTimer()
+    {
+        for (int i = 0; i < n; ++i)
+            if (ev[i])
+                cudaEventDestroy(ev[i]);
+    }
+};
+
 } // namespace gpop
 
 struct BatchCache; // buffers and captured graph of the last batch (batch_api.cu)
@@ -66,6 +95,7 @@ struct gpop_ctx {
     bool tuned = false;
     double eta[4][6] = {};
     int force_lpo = 0; // lanes per object fixed by the autotuner while it measures (0 = planner)
+    double batch_seconds = 0; // device time of the last batch launch (CUDA events around the graph)
 
     gpop::TableSrc table(bool mixed_mode) const
     {

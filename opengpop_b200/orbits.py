@@ -62,3 +62,29 @@ def mixed_population(n, seed):
     inc = np.radians(g.uniform(0.0, 180.0, n))
     raan, argp, M = (np.radians(g.uniform(0.0, 360.0, n)) for _ in range(3))
     return kepler_to_cartesian(a, e, inc, raan, argp, M)
+
+
+def batch_requests(n_req, seed, start=EPOCH):
+    """Uneven propagation requests of the batched configuration: object counts log-uniform in
+    [1, 512], durations log-uniform in [1 h, 7 d], step sizes uniform in {10, 30, 60, 120} s, gravity
+    degrees uniform in {8, 20, 36, 70}; states from the mixed population. Returns dicts with keys
+    start, h, steps, degree, r, v (the argument of Context.propagate_batch)."""
+    g = np.random.default_rng(seed)
+    out = []
+    for _ in range(n_req):
+        n = int(round(np.exp(g.uniform(0.0, np.log(512.0)))))
+        dur = float(np.exp(g.uniform(np.log(3600.0), np.log(7 * 86400.0))))
+        h = float(g.choice([10.0, 30.0, 60.0, 120.0]))
+        degree = int(g.choice([8, 20, 36, 70]))
+        steps = max(1, int(round(dur / h)))
+        r, v = mixed_population(n, int(g.integers(1 << 30)))
+        out.append(dict(start=start, h=h, steps=steps, degree=degree, r=r, v=v))
+    return out
+
+
+def conjunction_pairs(n_pairs, seed):
+    """The differentiation configuration's pairs: 2 n_pairs LEO objects (distribution of the
+    1,024-object configuration) matched at random into disjoint pairs. Returns r, v, pairs [p, 2]."""
+    r, v = leo(2 * n_pairs, seed)
+    pairs = np.random.default_rng(seed + 1).permutation(2 * n_pairs).astype(np.int32).reshape(-1, 2)
+    return r, v, pairs
