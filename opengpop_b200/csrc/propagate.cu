@@ -7,6 +7,7 @@
 #include "gravity.cuh"
 #include "gj8_tables.cuh"
 #include "integrator.cuh"
+#include "lanes.cuh"
 #include "kernels.h"
 
 #include <type_traits>
@@ -309,6 +310,125 @@ __global__ void __launch_bounds__(K == 1 ? 512 : 256, 1) gj8_kernel(F f, TableSr
     }
 }
 
+// ---- GJ8 step with P lanes per object (few objects) ----
+// Same step as gj8_kernel; the P lanes of an object's aligned group split the gravity columns
+// (lanes.cuh) and hold identical state, and lane 0 of the group stores. Used when the objects
+// alone leave most warp slots of the GPU empty (a few tens of thousands of objects or fewer).
+template <bool MIXED>
+__global__ void __launch_bounds__(512, 1) gj8_lanes_kernel(TableSrc ts, PropArgs a, int P)
+{
+    extern __shared__ __align__(128) uint8_t smem[];
+    GravSmem g;
+    if (!bind_table<MIXED>(smem, ts, a.err, g))
+        return;
+    const int64_t o = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / P;
+    const int lane = (int)(threadIdx.x & 31);
+    const int l = lane & (P - 1);
+    if (o >= a.n)
+        return; // whole groups leave: shuffles name the group only
+    const unsigned mask = P == 32 ? 0xffffffffu : ((1u << P) - 1u) << (lane & ~(P - 1));
+    const bool lead = l == 0;
+    const int64_t n = a.n;
+    double* st = a.state;
+    const double h = a.h;
+    double r[3], v[3], s[3], S[3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        r[j] = st[(kR + j) * n + o];
+        v[j] = st[(kV + j) * n + o];
+        s[j] = st[(kSs + j) * n + o];
+        S[j] = st[(kSb + j) * n + o];
+    }
+    for (int step = a.step_begin; step < a.step_end; ++step) {
+        double ae[3];
+        if (step <= 4) {
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                r[j] = st[(kRep + (step - 1) * 6 + j) * n + o];
+                v[j] = st[(kRep + (step - 1) * 6 + 3 + j) * n + o];
+                ae[j] = st[(kRepA + (step - 1) * 3 + j) * n + o];
+            }
+        } else {
+            const int ring0 = (step - 5) % 9;
+            double s1[3], s2[3], prev[3], a7[3], a8[3];
+            {
+                double hist[9][3];
+#pragma unroll
+                for (int c = 0; c < 9; ++c) {
+                    int slot = ring0 + c;
+                    slot -= slot >= 9 ? 9 : 0;
+#pragma unroll
+                    for (int j = 0; j < 3; ++j)
+                        hist[c][j] = st[(kHist + slot * 3 + j) * n + o];
+                }
+#pragma unroll
+                for (int j = 0; j < 3; ++j) { // as gj8_kernel
+                    double vt = 0.0, rt = 0.0;
+#pragma unroll
+                    for (int c = 0; c < 9; ++c) {
+                        vt = fma(hist[c][j], c_SA[9][c], vt);
+                        rt = fma(hist[c][j], c_GJ[9][c], rt);
+                    }
+                    S[j] += s[j] + hist[8][j] / 2;
+                    v[j] = (vt + s[j] + hist[8][j] / 2) * h;
+                    r[j] = (rt + S[j]) * h * h;
+                    double c1 = 0.0, c2 = 0.0;
+#pragma unroll
+                    for (int c = 0; c < 8; ++c) {
+                        c1 = fma(hist[c + 1][j], c_SA[8][c], c1);
+                        c2 = fma(hist[c + 1][j], c_GJ[8][c], c2);
+                    }
+                    s1[j] = c1;
+                    s2[j] = c2;
+                    prev[j] = s[j];
+                    a7[j] = hist[8][j];
+                }
+            }
+            const double* M = a.prop_m + (size_t)(step + 4) * 9;
+            for (int it = 0; it < a.ncorr; ++it) {
+                gravity_gcrs_lanes<MIXED>(g, l, P, M, r, a8, mask);
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    s[j] = prev[j] + (a8[j] + a7[j]) / 2;
+                    v[j] = h * (s1[j] + a8[j] * c_SA[8][8] + s[j]);
+                    r[j] = h * h * (s2[j] + a8[j] * c_GJ[8][8] + S[j]);
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                if (lead)
+                    st[(kHist + ring0 * 3 + j) * n + o] = a8[j];
+                ae[j] = a8[j];
+            }
+        }
+        __syncwarp(mask); // the group's ring write precedes its next step's loads
+        if (lead) {
+            const int64_t t = step - a.traj_step0;
+            for (int j = 0; j < 3; ++j) {
+                if (a.traj_r)
+                    a.traj_r[(t * 3 + j) * n + o] = r[j];
+                if (a.traj_v)
+                    a.traj_v[(t * 3 + j) * n + o] = v[j];
+                if (a.traj_a)
+                    a.traj_a[(t * 3 + j) * n + o] = ae[j];
+            }
+        }
+    }
+    if (!lead)
+        return;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        st[(kR + j) * n + o] = r[j];
+        st[(kV + j) * n + o] = v[j];
+        st[(kSs + j) * n + o] = s[j];
+        st[(kSb + j) * n + o] = S[j];
+        if (a.out_r)
+            a.out_r[o * 3 + j] = r[j];
+        if (a.out_v)
+            a.out_v[o * 3 + j] = v[j];
+    }
+}
+
 template <bool MIXED>
 __global__ void __launch_bounds__(512, 1) gravity_kernel(TableSrc ts, int64_t n, const double* r,
     const double* m9, double* a, unsigned* err)
@@ -476,13 +596,41 @@ static cudaError_t launch_gj8_f(F f, const TableSrc& ts, const PropArgs& a, int 
     return launch_gj8_k<F, 1>(f, ts, a, num_sms, s, block_override);
 }
 
+int lanes_per_object(int64_t n, int num_sms)
+{
+    int P = 1; // the most lanes that keep every object in one wave of 512-thread blocks
+    while (P < 32 && n * 2 * P <= (int64_t)num_sms * 512)
+        P *= 2;
+    return P;
+}
+
 cudaError_t launch_gj8(const TableSrc& ts, const PropArgs& a, int num_sms, cudaStream_t s,
     int block_override, int walk)
 {
     if (a.n <= 0 || a.step_end <= a.step_begin)
         return cudaSuccess;
-    if (walk <= 0) // two objects per thread once every SM gets 64 threads, else one
+    if (walk <= 0) // two objects per thread once every SM gets 64 threads, else one; the lane
+                   // split (kWalkLanes) is taken only on request
         walk = a.n >= (int64_t)num_sms * 128 ? kWalkTwoObjects : kWalkOneObject;
+    if (walk == kWalkLanes && a.kind == 0) {
+        const int P = lanes_per_object(a.n, num_sms);
+        const int64_t threads = a.n * P;
+        const int block = (int)std::min<int64_t>(512, ((threads + 31) / 32) * 32);
+        const size_t smem = table_smem_bytes(ts);
+        cudaError_t e;
+        if (ts.mixed) {
+            if ((e = set_smem(gj8_lanes_kernel<true>, smem)) != cudaSuccess)
+                return e;
+            gj8_lanes_kernel<true><<<(unsigned)((threads + block - 1) / block), block, smem, s>>>(ts, a, P);
+        } else {
+            if ((e = set_smem(gj8_lanes_kernel<false>, smem)) != cudaSuccess)
+                return e;
+            gj8_lanes_kernel<false><<<(unsigned)((threads + block - 1) / block), block, smem, s>>>(ts, a, P);
+        }
+        return cudaGetLastError();
+    }
+    if (walk == kWalkLanes)
+        walk = kWalkOneObject;
     if (a.kind == 0) {
         if (ts.mixed) {
             ForceGravity<true> f {};
