@@ -221,14 +221,15 @@ def _common(args, metric, value, unit, dtype, config, extra):
 def run_batch(args, torch, G, dev):
     """Batched uneven requests: 4,096 requests in one persistent launch under a captured graph."""
     from opengpop_b200 import orbits
-    reqs = orbits.batch_requests(4096, SEED)
+    reqs = orbits.batch_requests(args.batch_requests, SEED, max_days=args.batch_max_days)
     osteps = sum(q["r"].shape[0] * q["steps"] for q in reqs)
     f_total = sum(q["r"].shape[0] * q["steps"] * flops_per_object_step(q["degree"]) for q in reqs)
     f32 = sum(q["r"].shape[0] * q["steps"] * fp32_flops_per_object_step(q["degree"])
               for q in reqs if q["degree"] > 8)
     ctx = G.Context(precision=G.MIXED)
     t0 = time.perf_counter()
-    ctx.tune()
+    if not args.no_tune:
+        ctx.tune()
     tune_s = time.perf_counter() - t0
     lpo, est = ctx.batch_plan(reqs)
     sampler = ClockSampler(torch.cuda.current_device())
@@ -252,8 +253,9 @@ def run_batch(args, torch, G, dev):
     io = sum(q["r"].shape[0] for q in reqs) * 6 * 8
     _common(args, "object-steps/s, batched uneven requests (mixed precision)", osteps / t,
             "object-steps/s", "f64+f32",
-            {"workload": "4,096 requests (objects log-uniform 1-512, 1 h-7 d, h in {10,30,60,120} s, "
-                         "degree in {8,20,36,70}, seed %d), one persistent launch per batch" % SEED,
+            {"workload": "%d requests (objects log-uniform 1-512, 1 h-7 d, h in {10,30,60,120} s, "
+                         "degree in {8,20,36,70}, seed %d), one persistent launch per batch"
+                         % (len(reqs), SEED),
              "object_steps_per_batch": osteps, "l2": "inputs (and state) larger than L2",
              "lanes_per_object_histogram": np.bincount(lpo, minlength=33)[[1, 2, 4, 8, 16, 32]].tolist(),
              "planner_estimate_s": est, "tune_s": tune_s},
@@ -274,7 +276,8 @@ def run_screen(args, torch, G, dev):
     """Closest approach: 20,000 LEO objects, 2,000 seed-chosen objects against all (2,000
     singleton sets plus one set of 18,000: 37,999,000 pairs), 70x70, 30 s, 3 days, 5 km."""
     from opengpop_b200 import orbits
-    n, n_sel, steps, thr = 20000, 2000, 8640, 5000.0
+    n, steps, thr = args.screen_objects, args.screen_steps, 5000.0
+    n_sel = n // 10
     r, v = orbits.leo(n, SEED)
     sel = np.random.default_rng(SEED).choice(n, n_sel, replace=False)
     order = np.concatenate([sel, np.setdiff1d(np.arange(n), sel)])
@@ -305,9 +308,10 @@ def run_screen(args, torch, G, dev):
     achieved = 9.0 * pair_steps / t_screen / 1e12
     _common(args, "conjunction pair-steps/s of the screen (FP64)", pair_steps / t_screen,
             "pair-steps/s", "f64",
-            {"workload": "20,000 LEO objects (seed %d), 2,000 vs all = %d pairs, 70x70, 30 s, "
-                         "%d steps (3 days), threshold 5 km" % (SEED, pairs, steps),
-             "pairs": pairs, "steps": steps, "l2": "trajectory store 12 GB > L2"},
+            {"workload": "%d LEO objects (seed %d), %d vs all = %d pairs, 70x70, 30 s, "
+                         "%d steps, threshold 5 km" % (n, SEED, n_sel, pairs, steps),
+             "pairs": pairs, "steps": steps,
+             "l2": "trajectory store %.1f GB" % (n * steps * 72 / 1e9)},
             {"ms_per_step": 1e3 * wall,
              "device_seconds": {"propagation": t_prop, "screen": t_screen, "refinement": t_refine},
              "pairs_per_s_whole_job": pairs / wall,
@@ -326,7 +330,7 @@ def run_adjoint(args, torch, G, dev):
     """Differentiation: 10,000 pairs (24 h, 30 s, 70x70, FP64), adjoint gradient of each miss
     distance; and 8,192 state transition matrices by the forward variational equations."""
     from opengpop_b200 import orbits
-    n_pairs, steps, n_stm = 10000, 2880, 8192
+    n_pairs, steps, n_stm = args.adjoint_pairs, args.adjoint_steps, args.stm_objects
     r, v, pairs = orbits.conjunction_pairs(n_pairs, SEED)
     ctx = G.Context(precision=G.FP64)
     sampler = ClockSampler(torch.cuda.current_device())
@@ -402,6 +406,14 @@ def main():
     ap.add_argument("--workload", default="propagate",
                     choices=["propagate", "batch", "screen", "adjoint"],
                     help="propagate: the headline line; the others print their own line (1 GPU)")
+    ap.add_argument("--batch-requests", type=int, default=4096)
+    ap.add_argument("--batch-max-days", type=float, default=7.0)
+    ap.add_argument("--no-tune", action="store_true", help="batch: plan with the untuned model")
+    ap.add_argument("--screen-objects", type=int, default=20000)
+    ap.add_argument("--screen-steps", type=int, default=8640)
+    ap.add_argument("--adjoint-pairs", type=int, default=10000)
+    ap.add_argument("--adjoint-steps", type=int, default=2880)
+    ap.add_argument("--stm-objects", type=int, default=8192)
     ap.add_argument("--accuracy-objects", type=int, default=8192,
                     help="objects of the 7-day mixed-vs-FP64 error sample (0 = skip)")
     args = ap.parse_args()

@@ -64,16 +64,18 @@ def mixed_population(n, seed):
     return kepler_to_cartesian(a, e, inc, raan, argp, M)
 
 
-def batch_requests(n_req, seed, start=EPOCH):
+def batch_requests(n_req, seed, start=EPOCH, max_days=7.0):
     """Uneven propagation requests of the batched configuration: object counts log-uniform in
     [1, 512], durations log-uniform in [1 h, 7 d], step sizes uniform in {10, 30, 60, 120} s, gravity
     degrees uniform in {8, 20, 36, 70}; states from the mixed population. Returns dicts with keys
-    start, h, steps, degree, r, v (the argument of Context.propagate_batch)."""
+    start, h, steps, degree, r, v (the argument of Context.propagate_batch). max_days < 7 scales
+    the durations down (small cases for profiling)."""
     g = np.random.default_rng(seed)
     out = []
+    scale = max_days / 7.0
     for _ in range(n_req):
         n = int(round(np.exp(g.uniform(0.0, np.log(512.0)))))
-        dur = float(np.exp(g.uniform(np.log(3600.0), np.log(7 * 86400.0))))
+        dur = scale * float(np.exp(g.uniform(np.log(3600.0), np.log(7 * 86400.0))))
         h = float(g.choice([10.0, 30.0, 60.0, 120.0]))
         degree = int(g.choice([8, 20, 36, 70]))
         steps = max(1, int(round(dur / h)))
