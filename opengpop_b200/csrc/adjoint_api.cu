@@ -126,7 +126,7 @@ gpop_status run_adjoint(gpop_ctx* ctx, gpop_propagator& p, int32_t steps, int64_
     a.scratch = scratch.as<double>();
     a.grad = grad;
     a.err = ctx->err_word.as<unsigned>();
-    if ((e = launch_adjoint(ctx->table(false), a, s)) != cudaSuccess)
+    if ((e = launch_adjoint(ctx->lane_table(false), a, s)) != cudaSuccess)
         return cuda_fail(ctx, e, "adjoint kernel");
     ctx->launches++;
     return check_device_errors(ctx, s);
@@ -147,7 +147,7 @@ gpop_status gpop_gravity_jacobian(gpop_ctx* ctx, int64_t n, const double* r_dev,
     if (e != cudaSuccess)
         return cuda_fail(ctx, e, "cudaSetDevice");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    if ((e = launch_jacobian(ctx->table(false), n, r_dev, frame9_dev, a_dev, jac_dev,
+    if ((e = launch_jacobian(ctx->lane_table(false), n, r_dev, frame9_dev, a_dev, jac_dev,
              ctx->err_word.as<unsigned>(), s))
         != cudaSuccess)
         return cuda_fail(ctx, e, "Jacobian kernel");
@@ -201,7 +201,7 @@ gpop_status gpop_stm(gpop_ctx* ctx, const gpop_time* start, double h, int32_t st
     a.v_out = dvo.as<double>();
     a.phi = dphi.as<double>();
     a.err = ctx->err_word.as<unsigned>();
-    if ((e = launch_stm(ctx->table(false), a, s)) != cudaSuccess)
+    if ((e = launch_stm(ctx->lane_table(false), a, s)) != cudaSuccess)
         return cuda_fail(ctx, e, "STM kernel");
     ctx->launches++;
     if ((e = cudaMemcpyAsync(stm_out, dphi.p, 36 * n * sizeof(double), cudaMemcpyDeviceToHost, s)) != cudaSuccess

@@ -134,7 +134,8 @@ gpop_status propagator_step(gpop_propagator* p, int steps, double* traj_r, doubl
     cudaError_t e = cudaSetDevice(ctx->cfg.device);
     if (e != cudaSuccess)
         return cuda_fail(ctx, e, "cudaSetDevice");
-    TableSrc ts = ctx->table(p->mixed);
+    TableSrc ts = ctx->walk_mode == kWalkLanes && p->kind == GPOP_FORCE_GRAVITY ? ctx->lane_table(p->mixed)
+                                                                                : ctx->table(p->mixed);
     PropArgs a;
     a.n = p->n;
     a.h = p->h;
@@ -148,7 +149,7 @@ gpop_status propagator_step(gpop_propagator* p, int steps, double* traj_r, doubl
     a.r0 = p->r;
     a.v0 = p->v;
     if (!p->started) {
-        if ((e = launch_startup(ts, a, ctx->num_sms, s)) != cudaSuccess)
+        if ((e = launch_startup(ctx->table(p->mixed), a, ctx->num_sms, s)) != cudaSuccess)
             return cuda_fail(ctx, e, "startup kernel");
         ctx->launches++;
         p->started = true;
@@ -241,7 +242,7 @@ gpop_status gpop_create(const gpop_config* cfg_in, gpop_ctx** out)
     if (const char* spl = std::getenv("GPOP_STEPS_PER_LAUNCH"))
         ctx->steps_per_launch = std::max(1, atoi(spl));
     if (const char* wm = std::getenv("GPOP_WALK_MODE"))
-        ctx->walk_mode = std::min(2, std::max(0, atoi(wm)));
+        ctx->walk_mode = std::min(3, std::max(0, atoi(wm)));
     cudaError_t e = cudaSetDevice(cfg.device);
     if (e != cudaSuccess)
         return cuda_fail(ctx, e, "cudaSetDevice");
@@ -261,6 +262,15 @@ gpop_status gpop_create(const gpop_config* cfg_in, gpop_ctx** out)
     ctx->mixed_bytes = ctx->mixed_off32 + (uint32_t)(t32.size() * sizeof(GravEntry32));
     if (table_smem_bytes(ctx->table(false)) > 227 * 1024)
         return fail(ctx, GPOP_ERR_UNSUPPORTED, "gravity degree too high for the shared-memory table");
+    std::vector<uint8_t> lane64, lane_mixed;
+    if (L > kLaneMaxDegree)
+        return fail(ctx, GPOP_ERR_UNSUPPORTED, "gravity degree too high for the lane-layout tables");
+    build_lane_blob(t64.data(), L, nullptr, 0, lane64, ctx->lane64_off32);
+    build_lane_blob(head.data(), 8, t32.data(), L, lane_mixed, ctx->lane_mixed_off32);
+    ctx->lane64_bytes = (uint32_t)lane64.size();
+    ctx->lane_mixed_bytes = (uint32_t)lane_mixed.size();
+    if (table_smem_bytes(ctx->lane_table(false)) > 227 * 1024)
+        return fail(ctx, GPOP_ERR_UNSUPPORTED, "gravity degree too high for the lane-layout table");
     // frame data
     std::vector<NutTerm> nut;
     nut.insert(nut.end(), ctx->md.lon0.begin(), ctx->md.lon0.end());
@@ -274,7 +284,9 @@ gpop_status gpop_create(const gpop_config* cfg_in, gpop_ctx** out)
         || (e = ctx->nut.ensure(nut.size() * sizeof(NutTerm))) != cudaSuccess
         || (e = ctx->eop.ensure(ctx->md.eop.size() * sizeof(EopRec))) != cudaSuccess
         || (e = ctx->leap.ensure(leap.size() * sizeof(double))) != cudaSuccess
-        || (e = ctx->err_word.ensure(sizeof(unsigned))) != cudaSuccess)
+        || (e = ctx->err_word.ensure(sizeof(unsigned))) != cudaSuccess
+        || (e = ctx->lane64.ensure(lane64.size())) != cudaSuccess
+        || (e = ctx->lane_mixed.ensure(lane_mixed.size())) != cudaSuccess)
         return cuda_fail(ctx, e, "allocating model data");
     uint8_t* mixed = ctx->mixed.as<uint8_t>();
     if ((e = cudaMemcpy(ctx->t64.p, t64.data(), ctx->t64_bytes, cudaMemcpyHostToDevice)) != cudaSuccess
@@ -289,7 +301,10 @@ gpop_status gpop_create(const gpop_config* cfg_in, gpop_ctx** out)
             != cudaSuccess
         || (e = cudaMemcpy(ctx->leap.p, leap.data(), leap.size() * sizeof(double), cudaMemcpyHostToDevice))
             != cudaSuccess
-        || (e = cudaMemset(ctx->err_word.p, 0, sizeof(unsigned))) != cudaSuccess)
+        || (e = cudaMemset(ctx->err_word.p, 0, sizeof(unsigned))) != cudaSuccess
+        || (e = cudaMemcpy(ctx->lane64.p, lane64.data(), lane64.size(), cudaMemcpyHostToDevice)) != cudaSuccess
+        || (e = cudaMemcpy(ctx->lane_mixed.p, lane_mixed.data(), lane_mixed.size(), cudaMemcpyHostToDevice))
+            != cudaSuccess)
         return cuda_fail(ctx, e, "uploading model data");
     FrameData& fd = ctx->frames;
     fd.nut = ctx->nut.as<NutTerm>();
@@ -311,7 +326,7 @@ void gpop_destroy(gpop_ctx* ctx)
     if (!ctx)
         return;
     destroy_batch_cache(ctx);
-    for (DevBuf* b : { &ctx->t64, &ctx->mixed, &ctx->nut, &ctx->eop, &ctx->leap, &ctx->err_word,
+    for (DevBuf* b : { &ctx->lane64, &ctx->lane_mixed, &ctx->t64, &ctx->mixed, &ctx->nut, &ctx->eop, &ctx->leap, &ctx->err_word,
              &ctx->state, &ctx->gen_m, &ctx->prop_m, &ctx->gen_sec, &ctx->prop_sec, &ctx->io_r,
              &ctx->io_v })
         b->release();

@@ -95,7 +95,7 @@ __global__ void __launch_bounds__(512, 1) batch_gj8_kernel(TableSrc ts, BatchArg
 {
     extern __shared__ __align__(128) uint8_t smem[];
     GravSmem g0;
-    if (!stage_batch_table<MIXED>(smem, ts, a.err, g0))
+    if (!bind_lane_table(smem, ts, a.err, g0))
         return;
     const int lane = threadIdx.x & 31;
     const int64_t n = a.n_obj;

@@ -47,7 +47,7 @@ struct BatchArgs {
 };
 
 cudaError_t launch_batch_startup(const TableSrc& ts, const BatchArgs& a, int num_sms, cudaStream_t s);
-// blocks: persistent grid size (0 = one block per SM); block: threads per block.
+// ts: the lane-layout table. blocks: persistent grid size; block: threads per block.
 cudaError_t launch_batch_gj8(const TableSrc& ts, const BatchArgs& a, int blocks, int block,
     cudaStream_t s);
 cudaError_t launch_frames_batch(const FrameData& fd, const int* cal, const int* epoch_req,

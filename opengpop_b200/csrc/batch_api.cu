@@ -413,7 +413,7 @@ gpop_status gpop_propagate_batch(gpop_ctx* ctx, const gpop_request* reqs, int32_
         if (le == cudaSuccess)
             le = cudaMemsetAsync(bc->queue.p, 0, sizeof(int), s);
         if (le == cudaSuccess)
-            le = launch_batch_gj8(ts, a, ctx->num_sms, 32 * kWarpsPerSm, s);
+            le = launch_batch_gj8(ctx->lane_table(mixed), a, ctx->num_sms, 32 * kWarpsPerSm, s);
         e = cudaStreamEndCapture(s, &graph);
         if (le != cudaSuccess || e != cudaSuccess) {
             if (graph)

@@ -82,6 +82,9 @@ struct gpop_ctx {
     // device-resident model data
     gpop::DevBuf t64, mixed, nut, eop, leap, err_word;
     uint32_t t64_bytes = 0, mixed_bytes = 0, mixed_off32 = 0;
+    // the same tables in the lane layout (lane-split kernels)
+    gpop::DevBuf lane64, lane_mixed;
+    uint32_t lane64_bytes = 0, lane64_off32 = 0, lane_mixed_bytes = 0, lane_mixed_off32 = 0;
     gpop::FrameData frames {};
     int64_t launches = 0;
     // scratch
@@ -96,6 +99,20 @@ struct gpop_ctx {
     double eta[4][6] = {};
     int force_lpo = 0; // lanes per object fixed by the autotuner while it measures (0 = planner)
     double batch_seconds = 0; // device time of the last batch launch (CUDA events around the graph)
+
+    gpop::TableSrc lane_table(bool mixed_mode) const
+    {
+        gpop::TableSrc ts;
+        ts.L = md.degree;
+        ts.radius = md.radius;
+        ts.gm = md.gm;
+        ts.mixed = mixed_mode;
+        ts.lanes = true;
+        ts.src = mixed_mode ? lane_mixed.p : lane64.p;
+        ts.bytes = mixed_mode ? lane_mixed_bytes : lane64_bytes;
+        ts.off32 = mixed_mode ? lane_mixed_off32 : lane64_off32;
+        return ts;
+    }
 
     gpop::TableSrc table(bool mixed_mode) const
     {

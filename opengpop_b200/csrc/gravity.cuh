@@ -40,6 +40,8 @@ struct GravSmem {
     int L; // degree summed (<= Lt)
     int Lt; // degree of the table layout (columns of Lt - m + 1 entries)
     double radius, gm;
+    const int* cb64 = nullptr; // lane layout: first 16-byte unit of each FP64 (or head) column
+    const int* cb32 = nullptr; // lane layout: the same for the FP32 table
 };
 
 template <int K> struct ColSums64 {

@@ -14,6 +14,7 @@ struct TableSrc {
     int L = 0;
     double radius = 0, gm = 0;
     bool mixed = false;
+    bool lanes = false; // lane layout (build_lane_blob): column bases, FP64 at kLaneOff64, FP32 at off32
 };
 
 // Per-object propagation state, SoA: array k (n doubles each) at state + k * n.

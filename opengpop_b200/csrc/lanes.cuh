@@ -2,11 +2,41 @@
 // (lane l of P takes m = l, l + P, ...); the per-object sums are added with warp shuffles among
 // the lanes named by `mask` (the whole warp, or the object's aligned group of P lanes), so every
 // lane of the object ends with the same result. Used where one object per thread leaves
-// the GPU idle: long single requests of a batch and the variational/adjoint kernels.
+// the GPU idle: long single requests of a batch and the variational/adjoint kernels. The tables
+// are in the lane layout (build_lane_blob), so the lanes' simultaneous reads of different columns
+// fall in different shared-memory banks.
 #pragma once
 #include "gravity.cuh"
+#include "kernels.h"
 
 namespace gpop {
+
+// Columns of the lane-layout tables (build_lane_blob).
+__device__ __forceinline__ const GravEntry64* lane_col64(const GravSmem& g, int m)
+{
+    return reinterpret_cast<const GravEntry64*>(reinterpret_cast<const uint4*>(g.t64) + g.cb64[m]);
+}
+__device__ __forceinline__ const GravEntry32* lane_col32(const GravSmem& g, int m)
+{
+    return reinterpret_cast<const GravEntry32*>(reinterpret_cast<const uint4*>(g.t32) + g.cb32[m]);
+}
+
+// Stages a lane-layout blob into shared memory (after a 128-byte mbarrier slot) and binds it.
+__device__ __forceinline__ bool bind_lane_table(uint8_t* smem, const TableSrc& ts, unsigned* err, GravSmem& g)
+{
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(smem);
+    uint8_t* tab = smem + 128;
+    const bool ok = stage_to_smem(tab, ts.src, ts.bytes, mbar, err);
+    g.L = ts.L;
+    g.Lt = ts.L;
+    g.radius = ts.radius;
+    g.gm = ts.gm;
+    g.cb64 = reinterpret_cast<const int*>(tab);
+    g.cb32 = reinterpret_cast<const int*>(tab + 512);
+    g.t64 = reinterpret_cast<const GravEntry64*>(tab + kLaneOff64);
+    g.t32 = reinterpret_cast<const GravEntry32*>(tab + ts.off32);
+    return ok;
+}
 
 __device__ __forceinline__ void cmul(double ac, double as, double bc, double bs, double& rc, double& rs)
 {
@@ -37,7 +67,7 @@ template <bool MIXED>
 __device__ __forceinline__ void gravity_itrs_lanes(const GravSmem& gs, int l, int P, double x,
     double y, double z, double& ax, double& ay, double& az, unsigned mask = 0xffffffffu)
 {
-    const int L = gs.L, Lt = gs.Lt;
+    const int L = gs.L;
     const double r = sqrt(x * x + y * y + z * z);
     const double eps = z / r;
     const double q = gs.radius / r;
@@ -64,18 +94,18 @@ __device__ __forceinline__ void gravity_itrs_lanes(const GravSmem& gs, int l, in
         double Q1[1] = { qm }, Q2[1] = { 0.0 };
         const double uu[1] = { u }, ww[1] = { w };
         if constexpr (!MIXED) {
-            const GravEntry64* e = gs.t64 + grav_col_offset(m, Lt);
+            const GravEntry64* e = lane_col64(gs, m);
             s.add(e, Q1);
             column64<1>(e, 1, L - m, uu, ww, Q1, Q2, s);
         } else {
             ColSums32<1> f;
             f.zero();
-            const GravEntry32* e32 = gs.t32 + grav_col_offset(m, Lt);
+            const GravEntry32* e32 = lane_col32(gs, m);
             float Q1f[1], Q2f[1];
             const float ufa[1] = { uf }, wfa[1] = { wf };
             if (m <= kMixedSplit) {
                 const int top = L < kMixedSplit ? L : kMixedSplit;
-                const GravEntry64* e = gs.t64 + grav_col_offset(m, kMixedSplit);
+                const GravEntry64* e = lane_col64(gs, m); // head table (n <= 8)
                 s.add(e, Q1);
                 column64<1>(e, 1, top - m, uu, ww, Q1, Q2, s);
                 Q1f[0] = (float)Q1[0];
@@ -169,7 +199,7 @@ __device__ __forceinline__ void jac_warp_sum(double& x, int P, unsigned mask)
 __device__ __forceinline__ void gravity_jac_itrs_lanes(const GravSmem& gs, int l, int P, double x,
     double y, double z, double* a, double (*Jm)[3], unsigned mask)
 {
-    const int L = gs.L, Lt = gs.Lt;
+    const int L = gs.L;
     const double r = sqrt(x * x + y * y + z * z);
     const double invr = 1.0 / r;
     const double eps = z / r;
@@ -200,7 +230,7 @@ __device__ __forceinline__ void gravity_jac_itrs_lanes(const GravSmem& gs, int l
             cmul(Cp, Sp, CP, SP, Cp, Sp);
             cmul(Cq, Sq, CP, SP, Cq, Sq);
         }
-        const GravEntry64* e = gs.t64 + grav_col_offset(m, Lt);
+        const GravEntry64* e = lane_col64(gs, m);
         // sums of Q, n Q and E times (g1, g2, j1, j2, h1, h2)
         double s0[6], s1[6], s2[6];
         {

@@ -1,6 +1,8 @@
 // model.cpp -- model data loaders and gravity-table builder (host side of the product).
 #include "model.h"
 
+#include <cstring>
+
 #include <cmath>
 #include <fstream>
 #include <sstream>
@@ -245,6 +247,46 @@ void build_gravity_tables(const ModelData& md, std::vector<GravEntry64>& t64, st
             f.h2 = (float)e.h2;
         }
     }
+}
+
+void build_lane_blob(const GravEntry64* t64, int L64, const GravEntry32* t32, int L32,
+    std::vector<uint8_t>& blob, uint32_t& off32)
+{
+    // column bases in 16-byte units: base(m) = m (mod 8), each column after the previous one
+    auto bases = [](int L, int quads_per_entry, std::vector<int>& b) {
+        b.assign(L + 2, 0);
+        int q = 0;
+        for (int m = 0; m <= L + 1; ++m) {
+            while (q % 8 != m % 8)
+                ++q;
+            b[m] = q;
+            if (m <= L)
+                q += quads_per_entry * (L - m + 1);
+        }
+    };
+    std::vector<int> b64, b32;
+    bases(L64, 4, b64);
+    const size_t bytes64 = (size_t)(b64[L64 + 1] + 4) * 16; // one zero entry past the end
+    off32 = (uint32_t)(((kLaneOff64 + bytes64) + 127) / 128 * 128);
+    size_t total = off32;
+    if (t32) {
+        bases(L32, 2, b32);
+        total += (size_t)(b32[L32 + 1] + 2) * 16;
+    }
+    blob.assign(total, 0);
+    int* cb64 = reinterpret_cast<int*>(blob.data());
+    int* cb32 = reinterpret_cast<int*>(blob.data() + 512);
+    for (int m = 0; m <= L64; ++m) {
+        cb64[m] = b64[m];
+        std::memcpy(blob.data() + kLaneOff64 + (size_t)b64[m] * 16, t64 + grav_col_offset(m, L64),
+            sizeof(GravEntry64) * (L64 - m + 1));
+    }
+    if (t32)
+        for (int m = 0; m <= L32; ++m) {
+            cb32[m] = b32[m];
+            std::memcpy(blob.data() + off32 + (size_t)b32[m] * 16, t32 + grav_col_offset(m, L32),
+                sizeof(GravEntry32) * (L32 - m + 1));
+        }
 }
 
 } // namespace gpop

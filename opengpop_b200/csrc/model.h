@@ -70,4 +70,16 @@ GPOP_HOST_DEVICE inline int grav_col_offset(int m, int L) { return m * (L + 1) -
 // Builds the FP64 and FP32 tables for degree L (= model degree).
 void build_gravity_tables(const ModelData& md, std::vector<GravEntry64>& t64, std::vector<GravEntry32>& t32);
 
+// Lane layout of the tables, for kernels whose lanes walk different columns at once (P lanes per
+// object, lane l on columns l, l + P, ...). Each column starts on the 16-byte slot m mod 8 of a
+// 128-byte shared-memory row, so eight lanes that read entry i of eight consecutive columns hit
+// eight different bank groups. Blob: int column bases (in 16-byte units from their table) at
+// byte 0 (FP64, up to 128 columns) and byte 512 (FP32), the FP64 table at kLaneOff64 and the
+// FP32 table (if any) at off32, a multiple of 128 bytes.
+constexpr uint32_t kLaneOff64 = 1024;
+constexpr int kLaneMaxDegree = 126;
+// t64 has degree L64 (column-major as grav_col_offset); t32 (may be NULL) degree L32.
+void build_lane_blob(const GravEntry64* t64, int L64, const GravEntry32* t32, int L32,
+    std::vector<uint8_t>& blob, uint32_t& off32);
+
 } // namespace gpop

@@ -319,7 +319,7 @@ __global__ void __launch_bounds__(512, 1) gj8_lanes_kernel(TableSrc ts, PropArgs
 {
     extern __shared__ __align__(128) uint8_t smem[];
     GravSmem g;
-    if (!bind_table<MIXED>(smem, ts, a.err, g))
+    if (!bind_lane_table(smem, ts, a.err, g))
         return;
     const int64_t o = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / P;
     const int lane = (int)(threadIdx.x & 31);
@@ -612,7 +612,7 @@ cudaError_t launch_gj8(const TableSrc& ts, const PropArgs& a, int num_sms, cudaS
     if (walk <= 0) // two objects per thread once every SM gets 64 threads, else one; the lane
                    // split (kWalkLanes) is taken only on request
         walk = a.n >= (int64_t)num_sms * 128 ? kWalkTwoObjects : kWalkOneObject;
-    if (walk == kWalkLanes && a.kind == 0) {
+    if (walk == kWalkLanes && a.kind == 0 && ts.lanes) {
         const int P = lanes_per_object(a.n, num_sms);
         const int64_t threads = a.n * P;
         const int block = (int)std::min<int64_t>(512, ((threads + 31) / 32) * 32);

@@ -107,16 +107,7 @@ __device__ __forceinline__ void gj8_step(const Eval& eval, double h, int ncorr, 
 
 __device__ __forceinline__ bool stage_table64(uint8_t* smem, const TableSrc& ts, unsigned* err, GravSmem& g)
 {
-    uint64_t* mbar = reinterpret_cast<uint64_t*>(smem);
-    uint8_t* tab = smem + 128;
-    const bool ok = stage_to_smem(tab, ts.src, ts.bytes, mbar, err);
-    g.L = ts.L;
-    g.Lt = ts.L;
-    g.radius = ts.radius;
-    g.gm = ts.gm;
-    g.t64 = reinterpret_cast<const GravEntry64*>(tab);
-    g.t32 = nullptr;
-    return ok;
+    return bind_lane_table(smem, ts, err, g); // FP64 lane-layout table
 }
 
 } // namespace
