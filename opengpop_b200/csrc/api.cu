@@ -134,8 +134,8 @@ gpop_status propagator_step(gpop_propagator* p, int steps, double* traj_r, doubl
     cudaError_t e = cudaSetDevice(ctx->cfg.device);
     if (e != cudaSuccess)
         return cuda_fail(ctx, e, "cudaSetDevice");
-    TableSrc ts = ctx->walk_mode == kWalkLanes && p->kind == GPOP_FORCE_GRAVITY ? ctx->lane_table(p->mixed)
-                                                                                : ctx->table(p->mixed);
+    const TableSrc ts = ctx->table(p->mixed);
+    const TableSrc lane_ts = ctx->lane_table(p->mixed);
     PropArgs a;
     a.n = p->n;
     a.h = p->h;
@@ -149,7 +149,7 @@ gpop_status propagator_step(gpop_propagator* p, int steps, double* traj_r, doubl
     a.r0 = p->r;
     a.v0 = p->v;
     if (!p->started) {
-        if ((e = launch_startup(ctx->table(p->mixed), a, ctx->num_sms, s)) != cudaSuccess)
+        if ((e = launch_startup(ts, a, ctx->num_sms, s)) != cudaSuccess)
             return cuda_fail(ctx, e, "startup kernel");
         ctx->launches++;
         p->started = true;
@@ -166,7 +166,8 @@ gpop_status propagator_step(gpop_propagator* p, int steps, double* traj_r, doubl
         const bool last = a.step_end == end;
         a.out_r = last ? p->r : nullptr;
         a.out_v = last ? p->v : nullptr;
-        if ((e = launch_gj8(ts, a, ctx->num_sms, s, ctx->block_override, ctx->walk_mode)) != cudaSuccess)
+        if ((e = launch_gj8(ts, a, ctx->num_sms, s, ctx->block_override, ctx->walk_mode, &lane_ts))
+            != cudaSuccess)
             return cuda_fail(ctx, e, "GJ8 kernel");
         ctx->launches++;
     }

@@ -61,8 +61,9 @@ enum WalkMode : int { kWalkOneObject = 1, kWalkTwoObjects = 2, kWalkLanes = 3 };
 // Lanes per object (1..32, a power of 2): the most that keep n objects in one wave of 512-thread
 // blocks, one per SM.
 int lanes_per_object(int64_t n, int num_sms);
+// lane_ts: the lane-layout table of the same precision (NULL: no lane-split walk).
 cudaError_t launch_gj8(const TableSrc& ts, const PropArgs& a, int num_sms, cudaStream_t s,
-    int block_override = 0, int walk = 0);
+    int block_override = 0, int walk = 0, const TableSrc* lane_ts = nullptr);
 cudaError_t launch_gravity(const TableSrc& ts, int64_t n, const double* r, const double* m9,
     double* a, unsigned* err, int num_sms, cudaStream_t s);
 cudaError_t launch_corrector_unit(int kind, double h, int op, double* r27, double* v27, double* a27,
