@@ -73,3 +73,32 @@ def test_closest_approach_matches_reference_build():
     # parity bar of the closest-approach path: TCA within 1 ms, miss distance within 1 m
     assert np.abs(t[close] - ref["time"][close]).max() < 1e-3
     assert np.abs(d[close] - ref["distance"][close]).max() < 1.0
+
+
+def test_fp64_build_at_least_as_fast_as_reference_build():
+    # the plain FP64 build against the reference's CUDA build on 16,384 objects of the mixed
+    # population at 70x70; the step-loop rate comes from two durations (startup cancels)
+    import time
+    import torch
+    import opengpop_b200 as G
+    from opengpop_b200 import orbits
+    n, h, s1, s2 = 16384, 30.0, 8, 40
+    r0, v0 = orbits.mixed_population(n, seed=42)
+    t_ref = [float(RB.run("propagate", START, h, s, r0, v0)["ms"]) * 1e-3 for s in (s1, s2)]
+    ctx = G.Context(precision=G.FP64)
+    t_ours = []
+    for s in (s1, s2):
+        r = torch.tensor(r0, dtype=torch.float64, device="cuda")
+        v = torch.tensor(v0, dtype=torch.float64, device="cuda")
+        ctx.propagate_device(START, h, 4, r.clone(), v.clone())  # warm-up
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ctx.propagate_device(START, h, s, r, v)
+        torch.cuda.synchronize()
+        t_ours.append(time.perf_counter() - t0)
+    ctx.close()
+    rate_ref = n * (s2 - s1) / max(t_ref[1] - t_ref[0], 1e-9)
+    rate_ours = n * (s2 - s1) / max(t_ours[1] - t_ours[0], 1e-9)
+    print("\n%d objects, 70x70: reference CUDA build %.3e object-steps/s, this FP64 build %.3e "
+          "(x%.1f)" % (n, rate_ref, rate_ours, rate_ours / rate_ref))
+    assert rate_ours >= rate_ref
