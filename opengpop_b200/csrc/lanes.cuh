@@ -61,101 +61,183 @@ __device__ __forceinline__ void cpow(double c1, double s1, int p, double& rc, do
     rs = xs;
 }
 
-// Gravity in the Earth-fixed frame with the columns split over the P lanes of an object
-// (lane l takes columns l, l + P, ...); the per-object totals are added across the P lanes.
+// Gravity in the Earth-fixed frame of K objects with the columns split over the P lanes of each
+// object's group (lane l takes columns l, l + P, ...); the per-object totals are added across the
+// P lanes. As gravity_itrs in mixed mode: the head columns m <= 8 are combined in FP64 (their
+// terms of degree > 8 summed in FP32 per column), the columns m > 8 are walked, combined and
+// summed in FP32 and added to the FP64 totals once.
+template <bool MIXED, int K>
+__device__ __forceinline__ void gravity_itrs_lk(const GravSmem& gs, int l, int P, const double (&x)[K],
+    const double (&y)[K], const double (&z)[K], double (&ax)[K], double (&ay)[K], double (&az)[K],
+    unsigned mask)
+{
+    const int L = gs.L;
+    double r[K], q[K], u[K], w[K], C1[K], S1[K], CP[K], SP[K], Cm[K], Sm[K], Cp[K], Sp[K], CPm1[K], SPm1[K];
+    double qm[K], qP[K], G[K], H[K], J[K], KK[K];
+    float uf[K], wf[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        r[k] = sqrt(x[k] * x[k] + y[k] * y[k] + z[k] * z[k]);
+        const double eps = z[k] / r[k];
+        q[k] = gs.radius / r[k];
+        u[k] = q[k] * eps;
+        w[k] = q[k] * q[k];
+        uf[k] = (float)u[k];
+        wf[k] = (float)w[k];
+        C1[k] = x[k] / r[k];
+        S1[k] = y[k] / r[k];
+        cpow(C1[k], S1[k], P, CP[k], SP[k]); // step between this lane's columns
+        cpow(C1[k], S1[k], l, Cm[k], Sm[k]);
+        if (l > 0)
+            cpow(C1[k], S1[k], l - 1, Cp[k], Sp[k]);
+        else
+            Cp[k] = Sp[k] = 0.0; // column 0 has no J, K or H part
+        cpow(C1[k], S1[k], P - 1, CPm1[k], SPm1[k]); // the m - 1 values of column P
+        qm[k] = 1.0;
+        qP[k] = 1.0;
+        for (int i = 0; i < l; ++i)
+            qm[k] *= q[k];
+        for (int i = 0; i < P; ++i)
+            qP[k] *= q[k];
+        G[k] = H[k] = J[k] = KK[k] = 0.0;
+    }
+    const int Lhead = (MIXED && L > kMixedSplit) ? kMixedSplit : L;
+    int m = l;
+    for (; m <= Lhead; m += P) {
+        ColSums64<K> s;
+        s.zero();
+        double Q1[K], Q2[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            Q1[k] = qm[k];
+            Q2[k] = 0.0;
+        }
+        const GravEntry64* e = lane_col64(gs, m); // mixed: the head table (n <= 8)
+        s.add(e, Q1);
+        column64<K>(e, 1, Lhead - m, u, w, Q1, Q2, s);
+        if constexpr (MIXED) {
+            if (L > kMixedSplit) {
+                ColSums32<K> f;
+                f.zero();
+                float Q1f[K], Q2f[K];
+#pragma unroll
+                for (int k = 0; k < K; ++k) {
+                    Q1f[k] = (float)Q1[k];
+                    Q2f[k] = (float)Q2[k];
+                }
+                column32k<K>(lane_col32(gs, m), kMixedSplit + 1 - m, L - m, uf, wf, Q1f, Q2f, f);
+#pragma unroll
+                for (int k = 0; k < K; ++k) {
+                    s.g1[k] += (double)f.g[k].x;
+                    s.g2[k] += (double)f.g[k].y;
+                    s.j1[k] += (double)f.j[k].x;
+                    s.j2[k] += (double)f.j[k].y;
+                    s.h1[k] += (double)f.h[k].x;
+                    s.h2[k] += (double)f.h[k].y;
+                }
+            }
+        }
+        const double dm = (double)m; // eq. 4-11
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            G[k] += Cm[k] * s.g1[k] + Sm[k] * s.g2[k];
+            J[k] += dm * (Cp[k] * s.j1[k] + Sp[k] * s.j2[k]);
+            KK[k] -= dm * (Sp[k] * s.j1[k] - Cp[k] * s.j2[k]);
+            H[k] += Cp[k] * s.h1[k] + Sp[k] * s.h2[k];
+            if (m == 0) {
+                Cp[k] = CPm1[k];
+                Sp[k] = SPm1[k];
+            } else {
+                cmul(Cp[k], Sp[k], CP[k], SP[k], Cp[k], Sp[k]);
+            }
+            cmul(Cm[k], Sm[k], CP[k], SP[k], Cm[k], Sm[k]);
+            qm[k] *= qP[k];
+        }
+    }
+    if constexpr (MIXED) {
+        if (m <= L) { // this lane's columns m > 8, in FP32
+            float cf[K], sf[K], cpf[K], spf[K], CPf[K], SPf[K], qmf[K], qPf[K];
+            float Gf[K], Hf[K], Jf[K], Kf[K];
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                cf[k] = (float)Cm[k];
+                sf[k] = (float)Sm[k];
+                cpf[k] = (float)Cp[k];
+                spf[k] = (float)Sp[k];
+                CPf[k] = (float)CP[k];
+                SPf[k] = (float)SP[k];
+                qmf[k] = (float)qm[k];
+                qPf[k] = (float)qP[k];
+                Gf[k] = Hf[k] = Jf[k] = Kf[k] = 0.f;
+            }
+            for (; m <= L; m += P) {
+                ColSums32<K> f;
+                const GravEntry32* e32 = lane_col32(gs, m);
+                const float4* p = reinterpret_cast<const float4*>(e32);
+                const float4 a = p[0], b = p[1];
+                float Q1f[K], Q2f[K];
+#pragma unroll
+                for (int k = 0; k < K; ++k) { // n = m term (Q = q^m)
+                    const float2 QQ = make_float2(qmf[k], qmf[k]);
+                    f.g[k] = __fmul2_rn(QQ, make_float2(a.z, a.w));
+                    f.j[k] = __fmul2_rn(QQ, make_float2(b.x, b.y));
+                    f.h[k] = __fmul2_rn(QQ, make_float2(b.z, b.w));
+                    Q1f[k] = qmf[k];
+                    Q2f[k] = 0.f;
+                }
+                column32k<K>(e32, 1, L - m, uf, wf, Q1f, Q2f, f);
+                const float dmf = (float)m;
+#pragma unroll
+                for (int k = 0; k < K; ++k) {
+                    Gf[k] += cf[k] * f.g[k].x + sf[k] * f.g[k].y;
+                    Jf[k] += dmf * (cpf[k] * f.j[k].x + spf[k] * f.j[k].y);
+                    Kf[k] -= dmf * (spf[k] * f.j[k].x - cpf[k] * f.j[k].y);
+                    Hf[k] += cpf[k] * f.h[k].x + spf[k] * f.h[k].y;
+                    const float c1 = cf[k] * CPf[k] - sf[k] * SPf[k], s1 = sf[k] * CPf[k] + cf[k] * SPf[k];
+                    const float c2 = cpf[k] * CPf[k] - spf[k] * SPf[k], s2 = spf[k] * CPf[k] + cpf[k] * SPf[k];
+                    cf[k] = c1;
+                    sf[k] = s1;
+                    cpf[k] = c2;
+                    spf[k] = s2;
+                    qmf[k] *= qPf[k];
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                G[k] += (double)Gf[k];
+                H[k] += (double)Hf[k];
+                J[k] += (double)Jf[k];
+                KK[k] += (double)Kf[k];
+            }
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        for (int o = P >> 1; o > 0; o >>= 1) {
+            G[k] += __shfl_xor_sync(mask, G[k], o);
+            H[k] += __shfl_xor_sync(mask, H[k], o);
+            J[k] += __shfl_xor_sync(mask, J[k], o);
+            KK[k] += __shfl_xor_sync(mask, KK[k], o);
+        }
+        const double Gt = G[k] + 1.0; // eq. 4-13
+        const double Lambda = Gt + z[k] * H[k] / r[k];
+        const double c = -gs.gm / (r[k] * r[k]);
+        ax[k] = c * (Lambda * x[k] / r[k] - J[k]);
+        ay[k] = c * (Lambda * y[k] / r[k] - KK[k]);
+        az[k] = c * (Lambda * z[k] / r[k] - H[k]);
+    }
+}
+
 template <bool MIXED>
 __device__ __forceinline__ void gravity_itrs_lanes(const GravSmem& gs, int l, int P, double x,
     double y, double z, double& ax, double& ay, double& az, unsigned mask = 0xffffffffu)
 {
-    const int L = gs.L;
-    const double r = sqrt(x * x + y * y + z * z);
-    const double eps = z / r;
-    const double q = gs.radius / r;
-    const double u = q * eps, w = q * q;
-    const float uf = (float)u, wf = (float)w;
-    const double C1 = x / r, S1 = y / r;
-    double CP, SP, Cm, Sm, Cp, Sp, CPm1, SPm1;
-    cpow(C1, S1, P, CP, SP); // step between this lane's columns
-    cpow(C1, S1, l, Cm, Sm);
-    if (l > 0)
-        cpow(C1, S1, l - 1, Cp, Sp);
-    else
-        Cp = Sp = 0.0; // column 0 has no J, K or H part
-    cpow(C1, S1, P - 1, CPm1, SPm1); // (C + iS)_{P-1}: the m-1 values of column P
-    double qm = 1.0, qP = 1.0;
-    for (int i = 0; i < l; ++i)
-        qm *= q;
-    for (int i = 0; i < P; ++i)
-        qP *= q;
-    double G = 0.0, H = 0.0, J = 0.0, KK = 0.0;
-    for (int m = l; m <= L; m += P) {
-        ColSums64<1> s;
-        s.zero();
-        double Q1[1] = { qm }, Q2[1] = { 0.0 };
-        const double uu[1] = { u }, ww[1] = { w };
-        if constexpr (!MIXED) {
-            const GravEntry64* e = lane_col64(gs, m);
-            s.add(e, Q1);
-            column64<1>(e, 1, L - m, uu, ww, Q1, Q2, s);
-        } else {
-            ColSums32<1> f;
-            f.zero();
-            const GravEntry32* e32 = lane_col32(gs, m);
-            float Q1f[1], Q2f[1];
-            const float ufa[1] = { uf }, wfa[1] = { wf };
-            if (m <= kMixedSplit) {
-                const int top = L < kMixedSplit ? L : kMixedSplit;
-                const GravEntry64* e = lane_col64(gs, m); // head table (n <= 8)
-                s.add(e, Q1);
-                column64<1>(e, 1, top - m, uu, ww, Q1, Q2, s);
-                Q1f[0] = (float)Q1[0];
-                Q2f[0] = (float)Q2[0];
-                column32k<1>(e32, kMixedSplit + 1 - m, L - m, ufa, wfa, Q1f, Q2f, f);
-            } else {
-                const float4* p = reinterpret_cast<const float4*>(e32);
-                const float4 a = p[0], b = p[1];
-                const float Qm = (float)qm;
-                const float2 QQ = make_float2(Qm, Qm);
-                f.g[0] = __fmul2_rn(QQ, make_float2(a.z, a.w));
-                f.j[0] = __fmul2_rn(QQ, make_float2(b.x, b.y));
-                f.h[0] = __fmul2_rn(QQ, make_float2(b.z, b.w));
-                Q1f[0] = Qm;
-                Q2f[0] = 0.f;
-                column32k<1>(e32, 1, L - m, ufa, wfa, Q1f, Q2f, f);
-            }
-            s.g1[0] += (double)f.g[0].x;
-            s.g2[0] += (double)f.g[0].y;
-            s.j1[0] += (double)f.j[0].x;
-            s.j2[0] += (double)f.j[0].y;
-            s.h1[0] += (double)f.h[0].x;
-            s.h2[0] += (double)f.h[0].y;
-        }
-        const double dm = (double)m; // eq. 4-11
-        G += Cm * s.g1[0] + Sm * s.g2[0];
-        J += dm * (Cp * s.j1[0] + Sp * s.j2[0]);
-        KK -= dm * (Sp * s.j1[0] - Cp * s.j2[0]);
-        H += Cp * s.h1[0] + Sp * s.h2[0];
-        if (m == 0) {
-            Cp = CPm1;
-            Sp = SPm1;
-        } else {
-            cmul(Cp, Sp, CP, SP, Cp, Sp);
-        }
-        cmul(Cm, Sm, CP, SP, Cm, Sm);
-        qm *= qP;
-    }
-    for (int o = P >> 1; o > 0; o >>= 1) {
-        G += __shfl_xor_sync(mask, G, o);
-        H += __shfl_xor_sync(mask, H, o);
-        J += __shfl_xor_sync(mask, J, o);
-        KK += __shfl_xor_sync(mask, KK, o);
-    }
-    const double Gt = G + 1.0; // eq. 4-13
-    const double Lambda = Gt + z * H / r;
-    const double c = -gs.gm / (r * r);
-    ax = c * (Lambda * x / r - J);
-    ay = c * (Lambda * y / r - KK);
-    az = c * (Lambda * z / r - H);
+    const double X[1] = { x }, Y[1] = { y }, Z[1] = { z };
+    double AX[1], AY[1], AZ[1];
+    gravity_itrs_lk<MIXED, 1>(gs, l, P, X, Y, Z, AX, AY, AZ, mask);
+    ax = AX[0];
+    ay = AY[0];
+    az = AZ[0];
 }
 
 template <bool MIXED>
