@@ -89,17 +89,127 @@ __global__ void __launch_bounds__(256) batch_startup_kernel(TableSrc ts, BatchAr
     }
 }
 
-// Persistent GJ8 kernel: warps pull work items until the queue is empty.
+// One work item on one warp: K = 2 objects per lane for single-lane items (up to 64 objects),
+// else one object per group of P lanes (up to 32 / P objects).
+template <bool MIXED, int K>
+__device__ __forceinline__ void run_item(const GravSmem& g0, const BatchArgs& a, const BatchItem& it,
+    const BatchReq& rq, int lane)
+{
+    const int64_t n = a.n_obj;
+    double* st = a.state;
+    const int P = K == 1 ? rq.lpo : 1;
+    const int sl = lane % P;
+    int64_t o[K];
+    bool valid[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        const int slot = K == 1 ? lane / P : lane + 32 * k;
+        valid[k] = slot < it.count;
+        o[k] = rq.obj0 + it.first + (valid[k] ? slot : 0); // idle slots shadow slot 0
+    }
+    const bool lead = sl == 0;
+    GravSmem g = g0;
+    g.L = rq.L;
+    const double h = rq.h;
+    double r[K][3], v[K][3], s[K][3], S[K][3];
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            r[k][j] = st[(kR + j) * n + o[k]];
+            v[k][j] = st[(kV + j) * n + o[k]];
+            s[k][j] = st[(kSs + j) * n + o[k]];
+            S[k][j] = st[(kSb + j) * n + o[k]];
+        }
+    for (int step = 1; step <= rq.steps; ++step) {
+        if (step <= 4) {
+#pragma unroll
+            for (int k = 0; k < K; ++k)
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    r[k][j] = st[(kRep + (step - 1) * 6 + j) * n + o[k]];
+                    v[k][j] = st[(kRep + (step - 1) * 6 + 3 + j) * n + o[k]];
+                }
+            continue;
+        }
+        const int ring0 = (step - 5) % 9;
+        double s1[K][3], s2[K][3], prev[K][3], a7[K][3], a8[K][3];
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            double hist[9][3];
+#pragma unroll
+            for (int c = 0; c < 9; ++c) {
+                int sl9 = ring0 + c;
+                sl9 -= sl9 >= 9 ? 9 : 0;
+#pragma unroll
+                for (int j = 0; j < 3; ++j)
+                    hist[c][j] = st[(kHist + sl9 * 3 + j) * n + o[k]];
+            }
+#pragma unroll
+            for (int j = 0; j < 3; ++j) { // predictor, as in gj8_kernel
+                double vt = 0.0, rt = 0.0;
+#pragma unroll
+                for (int c = 0; c < 9; ++c) {
+                    vt = fma(hist[c][j], c_SA[9][c], vt);
+                    rt = fma(hist[c][j], c_GJ[9][c], rt);
+                }
+                S[k][j] += s[k][j] + hist[8][j] / 2;
+                v[k][j] = (vt + s[k][j] + hist[8][j] / 2) * h;
+                r[k][j] = (rt + S[k][j]) * h * h;
+                double c1 = 0.0, c2 = 0.0;
+#pragma unroll
+                for (int c = 0; c < 8; ++c) {
+                    c1 = fma(hist[c + 1][j], c_SA[8][c], c1);
+                    c2 = fma(hist[c + 1][j], c_GJ[8][c], c2);
+                }
+                s1[k][j] = c1;
+                s2[k][j] = c2;
+                prev[k][j] = s[k][j];
+                a7[k][j] = hist[8][j];
+            }
+        }
+        const double* M = rq.prop_m + (size_t)(step + 4) * 9;
+        for (int itc = 0; itc < a.ncorr; ++itc) {
+            gravity_gcrs_lk<MIXED, K>(g, sl, P, M, r, a8, 0xffffffffu);
+#pragma unroll
+            for (int k = 0; k < K; ++k)
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    s[k][j] = prev[k][j] + (a8[k][j] + a7[k][j]) / 2;
+                    v[k][j] = h * (s1[k][j] + a8[k][j] * c_SA[8][8] + s[k][j]);
+                    r[k][j] = h * h * (s2[k][j] + a8[k][j] * c_GJ[8][8] + S[k][j]);
+                }
+        }
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+            if (lead && valid[k])
+                for (int j = 0; j < 3; ++j)
+                    st[(kHist + ring0 * 3 + j) * n + o[k]] = a8[k][j];
+        __syncwarp(); // the ring write precedes the other lanes' loads of the next step
+    }
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+        if (lead && valid[k])
+            for (int j = 0; j < 3; ++j) {
+                st[(kR + j) * n + o[k]] = r[k][j];
+                st[(kV + j) * n + o[k]] = v[k][j];
+                st[(kSs + j) * n + o[k]] = s[k][j];
+                st[(kSb + j) * n + o[k]] = S[k][j];
+                a.r_out[o[k] * 3 + j] = rq.steps > 0 ? r[k][j] : a.r0[o[k] * 3 + j];
+                a.v_out[o[k] * 3 + j] = rq.steps > 0 ? v[k][j] : a.v0[o[k] * 3 + j];
+            }
+}
+
+// Persistent GJ8 kernel: warps pull work items until the queue is empty. One 256-thread block per
+// SM: the two-object path needs the registers of 8 warps.
 template <bool MIXED>
-__global__ void __launch_bounds__(512, 1) batch_gj8_kernel(TableSrc ts, BatchArgs a)
+__global__ void __launch_bounds__(256, 1) batch_gj8_kernel(TableSrc ts, BatchArgs a)
 {
     extern __shared__ __align__(128) uint8_t smem[];
     GravSmem g0;
     if (!bind_lane_table(smem, ts, a.err, g0))
         return;
     const int lane = threadIdx.x & 31;
-    const int64_t n = a.n_obj;
-    double* st = a.state;
     for (;;) {
         int item = 0;
         if (lane == 0)
@@ -109,86 +219,10 @@ __global__ void __launch_bounds__(512, 1) batch_gj8_kernel(TableSrc ts, BatchArg
             break;
         const BatchItem it = a.items[item];
         const BatchReq rq = a.reqs[it.req];
-        const int P = rq.lpo;
-        const int slot = lane / P, sl = lane % P;
-        const bool valid = slot < it.count;
-        const int64_t o = rq.obj0 + it.first + (valid ? slot : 0); // idle slots shadow slot 0
-        const bool store = valid && sl == 0;
-        GravSmem g = g0;
-        g.L = rq.L;
-        const double h = rq.h;
-        double r[3], v[3], s[3], S[3];
-        for (int j = 0; j < 3; ++j) {
-            r[j] = st[(kR + j) * n + o];
-            v[j] = st[(kV + j) * n + o];
-            s[j] = st[(kSs + j) * n + o];
-            S[j] = st[(kSb + j) * n + o];
-        }
-        for (int step = 1; step <= rq.steps; ++step) {
-            if (step <= 4) {
-                for (int j = 0; j < 3; ++j) {
-                    r[j] = st[(kRep + (step - 1) * 6 + j) * n + o];
-                    v[j] = st[(kRep + (step - 1) * 6 + 3 + j) * n + o];
-                }
-                continue;
-            }
-            const int ring0 = (step - 5) % 9;
-            double hist[9][3];
-#pragma unroll
-            for (int c = 0; c < 9; ++c) {
-                int sl9 = ring0 + c;
-                sl9 -= sl9 >= 9 ? 9 : 0;
-#pragma unroll
-                for (int j = 0; j < 3; ++j)
-                    hist[c][j] = st[(kHist + sl9 * 3 + j) * n + o];
-            }
-            double s1[3], s2[3], prev[3], a7[3], a8[3];
-#pragma unroll
-            for (int j = 0; j < 3; ++j) { // predictor, as in gj8_kernel
-                double vt = 0.0, rt = 0.0;
-#pragma unroll
-                for (int c = 0; c < 9; ++c) {
-                    vt = fma(hist[c][j], c_SA[9][c], vt);
-                    rt = fma(hist[c][j], c_GJ[9][c], rt);
-                }
-                S[j] += s[j] + hist[8][j] / 2;
-                v[j] = (vt + s[j] + hist[8][j] / 2) * h;
-                r[j] = (rt + S[j]) * h * h;
-                double c1 = 0.0, c2 = 0.0;
-#pragma unroll
-                for (int c = 0; c < 8; ++c) {
-                    c1 = fma(hist[c + 1][j], c_SA[8][c], c1);
-                    c2 = fma(hist[c + 1][j], c_GJ[8][c], c2);
-                }
-                s1[j] = c1;
-                s2[j] = c2;
-                prev[j] = s[j];
-                a7[j] = hist[8][j];
-            }
-            const double* M = rq.prop_m + (size_t)(step + 4) * 9;
-            for (int itc = 0; itc < a.ncorr; ++itc) {
-                gravity_gcrs_lanes<MIXED>(g, sl, P, M, r, a8);
-#pragma unroll
-                for (int j = 0; j < 3; ++j) {
-                    s[j] = prev[j] + (a8[j] + a7[j]) / 2;
-                    v[j] = h * (s1[j] + a8[j] * c_SA[8][8] + s[j]);
-                    r[j] = h * h * (s2[j] + a8[j] * c_GJ[8][8] + S[j]);
-                }
-            }
-            if (store)
-                for (int j = 0; j < 3; ++j)
-                    st[(kHist + ring0 * 3 + j) * n + o] = a8[j];
-        }
-        if (store) {
-            for (int j = 0; j < 3; ++j) {
-                st[(kR + j) * n + o] = r[j];
-                st[(kV + j) * n + o] = v[j];
-                st[(kSs + j) * n + o] = s[j];
-                st[(kSb + j) * n + o] = S[j];
-                a.r_out[o * 3 + j] = rq.steps > 0 ? r[j] : a.r0[o * 3 + j];
-                a.v_out[o * 3 + j] = rq.steps > 0 ? v[j] : a.v0[o * 3 + j];
-            }
-        }
+        if (rq.lpo == 1)
+            run_item<MIXED, 2>(g0, a, it, rq, lane);
+        else
+            run_item<MIXED, 1>(g0, a, it, rq, lane);
     }
 }
 

@@ -24,8 +24,11 @@ struct BatchReq {
 struct BatchItem {
     int req;
     int first;
-    int count; // <= 32 / lpo
+    int count; // <= batch_item_objects(lpo)
 };
+
+// Objects per work item: two per lane with one lane per object, else 32 / lpo.
+inline int batch_item_objects(int lpo) { return lpo == 1 ? 64 : 32 / lpo; }
 
 struct BatchArgs {
     const BatchReq* reqs = nullptr;

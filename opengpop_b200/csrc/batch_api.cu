@@ -16,7 +16,7 @@ using namespace gpop;
 
 namespace {
 
-constexpr int kWarpsPerSm = 16; // persistent grid: one 512-thread block per SM
+constexpr int kWarpsPerSm = 8; // persistent grid: one 256-thread block per SM
 constexpr int kDegrees[4] = { 8, 20, 36, 70 };
 const double kNodesH[10] = { 0.0, 4.0 / 27.0, 2.0 / 9.0, 1.0 / 3.0, 1.0 / 2.0, 2.0 / 3.0, 1.0 / 6.0, 1.0, 5.0 / 6.0, 1.0 };
 
@@ -70,7 +70,8 @@ void choose_lanes(const std::vector<int64_t>& n, const std::vector<int>& steps, 
         double total = 0.0;
         for (size_t r = 0; r < R; ++r)
             if (steps[r] > 0)
-                total += (double)((n[r] + 32 / lpo[r] - 1) / (32 / lpo[r])) * item_time(r, lpo[r]);
+                total += (double)((n[r] + batch_item_objects(lpo[r]) - 1) / batch_item_objects(lpo[r]))
+                    * item_time(r, lpo[r]);
         const double bound = std::max(total / warps, crit);
         bool changed = false;
         for (size_t r = 0; r < R; ++r)
@@ -98,7 +99,7 @@ Plan make_plan(const gpop_ctx* ctx, const std::vector<int64_t>& n, const std::ve
     p.lpo.assign(R, 1);
     const double warps = (double)ctx->num_sms * kWarpsPerSm;
     auto item_time = [&](size_t r, int P) { // seconds for one warp to run its group through all steps
-        return (double)steps[r] * kWarpsPerSm * (32.0 / P) / eta(ctx, L[r], P);
+        return (double)steps[r] * kWarpsPerSm * batch_item_objects(P) / eta(ctx, L[r], P);
     };
     if (ctx->force_lpo > 0) // autotuner: fixed lanes per object
         p.lpo.assign(R, ctx->force_lpo);
@@ -109,7 +110,7 @@ Plan make_plan(const gpop_ctx* ctx, const std::vector<int64_t>& n, const std::ve
     for (size_t r = 0; r < R; ++r) {
         if (steps[r] <= 0)
             continue;
-        const int per = 32 / p.lpo[r];
+        const int per = batch_item_objects(p.lpo[r]);
         const double t = item_time(r, p.lpo[r]);
         for (int64_t f = 0; f < n[r]; f += per) {
             items.push_back({ t, BatchItem { (int)r, (int)f, (int)std::min<int64_t>(per, n[r] - f) } });
@@ -515,7 +516,7 @@ gpop_status gpop_tune(gpop_ctx* ctx, const char* cache_path)
         const int Lc = std::min(kDegrees[i], ctx->md.degree);
         for (int lp = 0; lp < 6; ++lp) {
             const int P = 1 << lp;
-            const int64_t nobj = (int64_t)ctx->num_sms * kWarpsPerSm * (32 / P);
+            const int64_t nobj = (int64_t)ctx->num_sms * kWarpsPerSm * batch_item_objects(P);
             std::vector<double> r(3 * nobj), v(3 * nobj), ro(3 * nobj), vo(3 * nobj);
             for (int64_t o = 0; o < nobj; ++o) {
                 const double ang = 0.001 * (double)o, a = 7.0e6 + 10.0 * (double)(o % 97);

@@ -240,6 +240,31 @@ __device__ __forceinline__ void gravity_itrs_lanes(const GravSmem& gs, int l, in
     az = AZ[0];
 }
 
+// K objects: GCRS positions r[k] with the ITRS<-GCRS matrix M of gravity_gcrs.
+template <bool MIXED, int K>
+__device__ __forceinline__ void gravity_gcrs_lk(const GravSmem& gs, int l, int P, const double* __restrict__ M,
+    const double (&r)[K][3], double (&a)[K][3], unsigned mask)
+{
+    double m[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i)
+        m[i] = __ldg(M + i);
+    double px[K], py[K], pz[K], ax[K], ay[K], az[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        px[k] = m[0] * r[k][0] + m[1] * r[k][1] + m[2] * r[k][2];
+        py[k] = m[3] * r[k][0] + m[4] * r[k][1] + m[5] * r[k][2];
+        pz[k] = m[6] * r[k][0] + m[7] * r[k][1] + m[8] * r[k][2];
+    }
+    gravity_itrs_lk<MIXED, K>(gs, l, P, px, py, pz, ax, ay, az, mask);
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        a[k][0] = m[0] * ax[k] + m[3] * ay[k] + m[6] * az[k];
+        a[k][1] = m[1] * ax[k] + m[4] * ay[k] + m[7] * az[k];
+        a[k][2] = m[2] * ax[k] + m[5] * ay[k] + m[8] * az[k];
+    }
+}
+
 template <bool MIXED>
 __device__ __forceinline__ void gravity_gcrs_lanes(const GravSmem& gs, int l, int P,
     const double* __restrict__ M, const double* r, double* a, unsigned mask = 0xffffffffu)
