@@ -157,6 +157,8 @@ int run(const Options& o)
         return rc;
     }
     Value out = Value::object();
+    std::vector<gpop_ca_record> ca_records;
+    bool streamed = false; // closestApproaches written record by record
     out.obj["propagationStart"] = write_time(start);
     out.obj["propagationSeconds"] = Value::integer(seconds);
     out.obj["positionsStart"] = write_vec3s(r.data(), n);
@@ -198,9 +200,21 @@ int run(const Options& o)
             gpop_destroy(ctx);
             return rc;
         }
-        Value arr = Value::array();
-        arr.arr.reserve(recs.size());
-        for (const gpop_ca_record& rc : recs) { // exec/runner.cu:96-106, main.cpp:35-36 keys
+        ca_records = std::move(recs);
+        gpop_ca_destroy(ca);
+        streamed = true;
+    }
+    const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    std::cerr << "Computed " << n << " objects x " << steps << " steps of " << h << " s in " << secs << " s\n";
+    gpop_destroy(ctx);
+    std::ofstream ofs(o.output);
+    if (!ofs.is_open()) {
+        std::cerr << "Error: cannot write " << o.output << "\n";
+        return 1;
+    }
+    if (streamed) {
+        gpop::json::dump_streaming(ofs, out, "closestApproaches", ca_records.size(), [&](size_t k) {
+            const gpop_ca_record& rc = ca_records[k]; // exec/runner.cu:96-106, main.cpp:35-36 keys
             Value x = Value::object();
             x.obj["objectIndex1"] = Value::integer(rc.object_index1);
             x.obj["objectIndex2"] = Value::integer(rc.object_index2);
@@ -212,20 +226,11 @@ int run(const Options& o)
             x.obj["positionBx"] = Value::number(rc.position_b[0]);
             x.obj["positionBy"] = Value::number(rc.position_b[1]);
             x.obj["positionBz"] = Value::number(rc.position_b[2]);
-            arr.arr.push_back(std::move(x));
-        }
-        out.obj["closestApproaches"] = std::move(arr);
-        gpop_ca_destroy(ca);
+            return x;
+        });
+    } else {
+        ofs << gpop::json::dump(out, 4);
     }
-    const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-    std::cerr << "Computed " << n << " objects x " << steps << " steps of " << h << " s in " << secs << " s\n";
-    gpop_destroy(ctx);
-    std::ofstream ofs(o.output);
-    if (!ofs.is_open()) {
-        std::cerr << "Error: cannot write " << o.output << "\n";
-        return 1;
-    }
-    ofs << gpop::json::dump(out, 4);
     std::cout << "Saved to: " << o.output << "\n";
     return 0;
 }

@@ -9,6 +9,7 @@
 #include <cmath>
 #include <cstdint>
 #include <map>
+#include <ostream>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -341,6 +342,47 @@ inline std::string dump(const Value& v, int indent = 4)
     std::string out;
     dump(v, out, indent, 0);
     return out;
+}
+
+// Writes `top` as dump(top, indent) would after setting top[key] to an array of `count` elements,
+// element k given by element(k), without holding the array: the elements are formatted and
+// written one at a time (closest-approach outputs run to tens of millions of records).
+template <class Element>
+void dump_streaming(std::ostream& os, const Value& top, const std::string& key, size_t count,
+    const Element& element, int indent = 4)
+{
+    std::map<std::string, const Value*> keys;
+    for (const auto& kv : top.obj)
+        keys[kv.first] = &kv.second;
+    keys[key] = nullptr;
+    const std::string pad((size_t)indent, ' '), pad2((size_t)indent * 2, ' ');
+    std::string buf = "{\n";
+    size_t k = 0;
+    for (const auto& kv : keys) {
+        buf += pad;
+        escape(buf, kv.first);
+        buf += ": ";
+        if (kv.second) {
+            dump(*kv.second, buf, indent, 1);
+        } else if (count == 0) {
+            buf += "[]";
+        } else {
+            buf += "[\n";
+            for (size_t e = 0; e < count; ++e) {
+                buf += pad2;
+                dump(element(e), buf, indent, 2);
+                buf += e + 1 < count ? ",\n" : "\n";
+                if (buf.size() > (1u << 20)) {
+                    os << buf;
+                    buf.clear();
+                }
+            }
+            buf += pad + "]";
+        }
+        buf += ++k < keys.size() ? ",\n" : "\n";
+    }
+    buf += "}";
+    os << buf;
 }
 
 } // namespace json

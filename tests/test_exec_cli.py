@@ -99,3 +99,14 @@ def test_cli_closest_approach_matches_library(tmp_path):
     d = json.loads(out.read_text())
     assert all(x["distance"] < 5000 for x in d["closestApproaches"])
     assert len(d["closestApproaches"]) == sum(1 for x in lib if x.distance < 5000)
+
+
+def test_streaming_json_writer_matches_whole_document(tmp_path):
+    # the closest-approach output is written record by record; the bytes must equal those of the
+    # whole-document writer (the reference's dump(4) layout)
+    import subprocess
+    exe = str(tmp_path / "json_stream_check")
+    subprocess.run(["g++", "-std=c++17", "-O1", "-I", os.path.join(ROOT, "opengpop_b200", "csrc"),
+                    os.path.join(ROOT, "tests", "cpp", "json_stream_check.cpp"), "-o", exe],
+                   check=True, capture_output=True, text=True)
+    assert subprocess.run([exe]).returncode == 0
