@@ -50,6 +50,11 @@ def fp32_flops_per_object_step(L=DEGREE):
     return 7 * 24 * (terms(L) - terms(8))
 
 
+# DRAM bytes (read + write) of one mixed GJ8 launch over 65,536 objects, from an ncu capture
+# (dram__bytes_read.sum 20.6 MB, dram__bytes_write.sum 0).
+MIXED_GJ8_DRAM_BYTES = 20.6e6
+
+
 def env_int(k, d):
     try:
         return int(os.environ.get(k, d))
@@ -574,7 +579,11 @@ def main():
                     "call": "gpop_propagate, %d GJ8 steps per call incl. startup" % e2e_steps},
             "roofline": {"bound": "fp64+fp32", "achieved": achieved, "peak": eff_peak,
                          "unit": "TFLOP/s", "frac": achieved / eff_peak if eff_peak else None,
-                         "traffic": None,
+                         "traffic": MIXED_GJ8_DRAM_BYTES,
+                         "traffic_note": "dram read+write bytes of one launch of this kernel "
+                                         "(ncu, 65,536 objects, 4-step launch: the state is read "
+                                         "once per launch, later steps hit L2); algorithmic "
+                                         "state bytes per launch %d" % (600 * n),
                          "peaks_measured": {"fp64_tflops": peak64, "fp32_tflops": peak32,
                                             "how": "live FMA-chain probe (libgpop_probe.so)"}},
             "cpu_baseline": cpu,
