@@ -186,6 +186,15 @@ gpop_status gpop_miss_gradient(gpop_ctx* ctx, const gpop_time* start, double h, 
     int64_t n, const double* r_in, const double* v_in, int64_t n_pairs, const int32_t* pairs,
     double* tca, double* miss, double* grad);
 
+/* ---- Monte Carlo ensembles ---- */
+/* PerturbationGenerator::generatePerturbedSatellites (perturbation_generator.cu:21-79): n
+ * samples of one object, r = r_nominal + sigma_r z, v = v_nominal + sigma_v z', z and z' standard
+ * normal (the reference perturbs the velocity only: sigma_r = 0). Philox4x32-10 counter-based
+ * generator keyed by seed, Box-Muller; sample i depends only on (seed, i). Not the reference's
+ * curand sequence. r_nominal, v_nominal: host [3]; r_dev, v_dev: device [n][3]. */
+gpop_status gpop_sample_states(gpop_ctx* ctx, const double* r_nominal, const double* v_nominal,
+    double sigma_r, double sigma_v, uint64_t seed, int64_t n, double* r_dev, double* v_dev, void* stream);
+
 /* ---- startup and integrator pieces (device buffers, one object each) ---- */
 /* GpuStartup::Startup (gpu_startup.cu:55-68). Outputs 9 columns x 3 (column 4 = epoch):
  * r27, v27, a27, s27, S27 (device). n_corrections = 0 returns the RK8 guess only. */

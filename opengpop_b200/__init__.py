@@ -31,7 +31,7 @@ EXPORTS = (
     "gpop_propagate_device_noalloc", "gpop_propagate_trajectory", "gpop_propagator_create", "gpop_propagator_step",
     "gpop_propagator_steps_done", "gpop_propagator_destroy", "gpop_propagate_analytic",
     "gpop_propagate_batch", "gpop_batch_plan", "gpop_tune", "gpop_batch_device_seconds", "gpop_gravity_jacobian", "gpop_stm", "gpop_propagate_vjp",
-    "gpop_miss_gradient", "gpop_startup", "gpop_corrector_unit",
+    "gpop_miss_gradient", "gpop_sample_states", "gpop_startup", "gpop_corrector_unit",
     "gpop_predict_unit", "gpop_finalize_correction_unit", "gpop_gravity", "gpop_frame_matrices",
     "gpop_ca_create", "gpop_ca_create_analytic", "gpop_ca_propagate", "gpop_ca_find", "gpop_ca_pairs", "gpop_ca_num_pairs",
     "gpop_ca_trajectory", "gpop_ca_device_seconds", "gpop_ca_destroy",
@@ -105,6 +105,7 @@ def load_library(path=LIB_PATH):
         "gpop_tune": (i32, [_VP, C.c_char_p]),
         "gpop_batch_device_seconds": (f64, [_VP]),
         "gpop_gravity_jacobian": (i32, [_VP, i64, _VP, _VP, _VP, _VP, _VP]),
+        "gpop_sample_states": (i32, [_VP, _VP, _VP, f64, f64, C.c_uint64, i64, _VP, _VP, _VP]),
         "gpop_stm": (i32, [_VP, C.POINTER(Time), f64, i32, i64] + [_VP] * 5),
         "gpop_propagate_vjp": (i32, [_VP, C.POINTER(Time), f64, i32, i64] + [_VP] * 6),
         "gpop_miss_gradient": (i32, [_VP, C.POINTER(Time), f64, i32, i64, _VP, _VP, i64]
@@ -319,6 +320,14 @@ class Context:
             self._h, None if cache_path is None else cache_path.encode()))
 
     # ---- variational equations and adjoint (FP64) ----
+    def sample_states(self, r_nominal, v_nominal, sigma_r, sigma_v, seed, r_out, v_out, stream=None):
+        """Monte Carlo ensemble on the device: r_out, v_out [n, 3] CUDA tensors."""
+        rn = np.ascontiguousarray(r_nominal, dtype=np.float64).reshape(3)
+        vn = np.ascontiguousarray(v_nominal, dtype=np.float64).reshape(3)
+        self._check(load_library().gpop_sample_states(
+            self._h, rn.ctypes.data, vn.ctypes.data, float(sigma_r), float(sigma_v), int(seed),
+            int(r_out.shape[0]), _dptr(r_out), _dptr(v_out), _stream_ptr(stream)))
+
     def gravity_jacobian(self, r, jac, frame9=None, acc=None, stream=None):
         """FP64 acceleration Jacobian [n, 3, 3] (device tensors) at GCRS positions r [n, 3]."""
         self._check(load_library().gpop_gravity_jacobian(
