@@ -355,12 +355,13 @@ def run_adjoint(args, torch, G, dev):
     ctx.close()
     tm, ts = float(np.mean(t_miss)), float(np.mean(t_stm))
     # work of the miss-gradient call: forward propagation of 2 n_pairs objects, then per unit
-    # (pair side) a recomputed forward pass (7 W per step), the reverse pass (7 Jacobian
-    # evaluations per step) and the tangent startup (145 Jacobian evaluations)
+    # (pair side) a recomputed forward pass (7 W + 500 per step), the reverse pass (one Jacobian
+    # per step) and the tangent startup (145 Jacobian evaluations); of the STM: the primal step,
+    # one Jacobian and six tangent steps per object-step
     W = 24 * terms(DEGREE) + 15 * DEGREE + 60
     units = 2 * n_pairs
-    f_miss = units * steps * (2 * flops_per_object_step() + 7 * w_jac(DEGREE)) + units * 145 * w_jac(DEGREE)
-    f_stm = n_stm * steps * (7 * w_jac(DEGREE) + 6 * 500) + n_stm * 145 * w_jac(DEGREE)
+    f_miss = units * steps * (2 * flops_per_object_step() + w_jac(DEGREE)) + units * 145 * w_jac(DEGREE)
+    f_stm = n_stm * steps * (flops_per_object_step() + w_jac(DEGREE) + 6 * 500) + n_stm * 145 * w_jac(DEGREE)
     peak64 = probe_peak(torch, True, dev)
     ach = f_miss / tm / 1e12
     _common(args, "miss-distance gradients/s (adjoint, FP64)", n_pairs / tm, "pairs/s", "f64",
@@ -373,7 +374,7 @@ def run_adjoint(args, torch, G, dev):
                      "d2h_bytes_per_step": n_pairs * 14 * 8, "call": "gpop_miss_gradient"},
              "roofline": {"bound": "fp64", "achieved": ach, "peak": peak64, "unit": "TFLOP/s",
                           "frac": ach / peak64 if peak64 else None, "traffic": None,
-                          "per_unit": "per unit-step 2 (7 W + 500) + 7 W_J, W(70) = %d, "
+                          "per_unit": "per unit-step 2 (7 W + 500) + W_J, W(70) = %d, "
                                       "W_J(70) = %d flops" % (W, w_jac(DEGREE))},
              "cpu_baseline": None, "clocks": clocks})
     return 0

@@ -104,7 +104,7 @@ gpop_status run_adjoint(gpop_ctx* ctx, gpop_propagator& p, int32_t steps, int64_
     const double* r0, const double* v0, const DevBuf& ckpt, int64_t n_units, const int* unit_obj,
     const int* seed_step0, const double* seeds, double* grad, DevBuf& scratch, cudaStream_t s)
 {
-    const size_t scr = (size_t)kCheckpointSteps * ctx->cfg.n_corrections * 3 * n_units;
+    const size_t scr = (size_t)kCheckpointSteps * 3 * n_units;
     cudaError_t e = scratch.ensure(scr * sizeof(double));
     if (e != cudaSuccess)
         return fail(ctx, GPOP_ERR_NOMEM, std::string("adjoint scratch: ") + cudaGetErrorString(e));

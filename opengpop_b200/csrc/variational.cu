@@ -5,17 +5,18 @@
 // gravity columns (lanes.cuh) and share the acceleration and its Jacobian; lane d < 6 carries the
 // tangent of initial-state direction d. The integrator is the same discrete map as the forward
 // propagation (startup: integrator.cuh; GJ8 step: gpu_propagator.cu:28-119 as in gj8_kernel),
-// so the tangents and adjoints are the exact derivatives of that map, corrector iterations
-// included (each corrector pass evaluates gravity at its own iterate, so the Jacobian is taken at
-// every iterate).
+// so the tangents and adjoints are the derivatives of that map with one simplification: the
+// Jacobian of a GJ8 step's corrector passes is taken once, at the step's last evaluation point
+// (the corrector converges, so the passes' iterates differ by far less than the truncation error);
+// the startup is differentiated exactly. Forward tangents and the reverse sweep make the same
+// choice, so they are exact transposes of each other.
 //
 // Adjoint of one GJ8 step n (K = number of corrector passes, iterates r(0..K-1), a(i) = f(r(i))):
 //   S' = S + s + h8/2,  r(0) = h^2 (sum_c GJ[9][c] h_c + S'),  s1 = sum_c SA[8][c] h_(c+1),
 //   s2 = sum_c GJ[8][c] h_(c+1),  r(i+1) = h^2 (s2 + GJ[8][8] a(i) + S'),
 //   s_n = s + (a(K-1) + h8)/2,  v_n = h (s1 + SA[8][8] a(K-1) + s_n),  history <- (h_1..h_8, a(K-1)).
-// The reverse pass below applies the transposes of these maps in the opposite order; the
-// transposed Jacobian J(r(i))^T is applied at every iterate, which is recomputed from the
-// checkpoint of the step's 64-step segment.
+// The reverse pass below applies the transposes of these maps in the opposite order, with J^T at
+// the last evaluation point r(K-1), recomputed from the checkpoint of the step's 64-step segment.
 #include "common.cuh"
 #include "gj8_tables.cuh"
 #include "gravity.cuh"
@@ -134,36 +135,58 @@ __global__ void __launch_bounds__(256, 1) stm_kernel(TableSrc ts, VarArgs a)
         r0[j] = Tan(a.r0[o * 3 + j], dir == j ? 1.0 : 0.0);
         v0[j] = Tan(a.v0[o * 3 + j], dir == 3 + j ? 1.0 : 0.0);
     }
-    Tan r[3], v[3];
+    // primal state (every lane) and the tangent of this lane's direction
+    double hist[9][3], s[3], S[3], r[3], v[3], dh[9][3], ds[3], dS[3], dr[3], dv[3];
     {
-        StartupMatsT<Tan> m;
+        StartupMatsT<Tan> m; // the startup: exact tangents, Jacobian at every evaluation
         run_startup(f, a.h, a.ncorr, r0, v0, m);
-        Tan hist[9][3], s[3], S[3];
+        const int rep = a.steps < 4 ? a.steps : 4; // steps 1..4 replay the startup columns
 #pragma unroll
         for (int j = 0; j < 3; ++j) {
-            for (int c = 0; c < 9; ++c)
-                hist[c][j] = m.a[c][j];
-            s[j] = m.s[8][j];
-            S[j] = m.S[8][j];
-            const int rep = a.steps < 4 ? a.steps : 4; // steps 1..4 replay the startup columns
-            r[j] = m.r[4 + rep][j];
-            v[j] = m.v[4 + rep][j];
+            for (int c = 0; c < 9; ++c) {
+                hist[c][j] = m.a[c][j].v;
+                dh[c][j] = m.a[c][j].d;
+            }
+            s[j] = m.s[8][j].v;
+            ds[j] = m.s[8][j].d;
+            S[j] = m.S[8][j].v;
+            dS[j] = m.S[8][j].d;
+            r[j] = m.r[4 + rep][j].v;
+            dr[j] = m.r[4 + rep][j].d;
+            v[j] = m.v[4 + rep][j].v;
+            dv[j] = m.v[4 + rep][j].d;
         }
-        for (int step = 5; step <= a.steps; ++step) {
-            const double* M = a.prop_m + (size_t)(step + 4) * 9;
-            auto eval = [&](const Tan* rr, Tan* aa, int) { f.eval(M, rr, aa); };
-            gj8_step<Tan>(eval, a.h, a.ncorr, hist, s, S, r, v);
-        }
+    }
+    for (int step = 5; step <= a.steps; ++step) {
+        const double* M = a.prop_m + (size_t)(step + 4) * 9;
+        // primal passes; the Jacobian at the last evaluation point serves every pass of the
+        // tangent step (as in the reverse sweep)
+        double rl[3];
+        auto evalp = [&](const double* rr, double* aa, int it) {
+            if (it == a.ncorr - 1)
+                for (int j = 0; j < 3; ++j)
+                    rl[j] = rr[j];
+            gravity_gcrs_lanes<false>(g, l, P, M, rr, aa, mask);
+        };
+        gj8_step<double>(evalp, a.h, a.ncorr, hist, s, S, r, v);
+        double av[3], J[3][3];
+        gravity_jac_gcrs_lanes(g, l, P, M, rl, av, J, mask);
+        auto evalt = [&](const double* rr, double* aa, int) {
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+                aa[i] = J[i][0] * rr[0] + J[i][1] * rr[1] + J[i][2] * rr[2];
+        };
+        gj8_step<double>(evalt, a.h, a.ncorr, dh, ds, dS, dr, dv);
     }
     if (l == 0 && a.r_out)
         for (int j = 0; j < 3; ++j) {
-            a.r_out[o * 3 + j] = r[j].v;
-            a.v_out[o * 3 + j] = v[j].v;
+            a.r_out[o * 3 + j] = r[j];
+            a.v_out[o * 3 + j] = v[j];
         }
     if (dir >= 0)
         for (int i = 0; i < 3; ++i) {
-            a.phi[(o * 6 + i) * 6 + dir] = r[i].d;
-            a.phi[(o * 6 + 3 + i) * 6 + dir] = v[i].d;
+            a.phi[(o * 6 + i) * 6 + dir] = dr[i];
+            a.phi[(o * 6 + 3 + i) * 6 + dir] = dv[i];
         }
 }
 
@@ -172,6 +195,9 @@ namespace {
 
 // Reverse of one GJ8 step (see the header comment). hb: history adjoints in logical order after
 // the step on entry, before it on exit; sb, Sb: adjoints of s and S likewise.
+// iter: the step's last evaluation point r(K-1) (3 values, stride apart); its Jacobian stands for
+// every corrector pass (the corrector converges: the iterates differ by far less than the step's
+// truncation error, and the forward tangents make the same choice).
 __device__ __forceinline__ void gj8_reverse_step(const GravSmem& g, int l, int P, unsigned mask,
     const double* M, double h, int ncorr, const double* iter, int64_t stride, const double* seed,
     double (&hb)[9][3], double (&sb)[3], double (&Sb)[3])
@@ -199,12 +225,15 @@ __device__ __forceinline__ void gj8_reverse_step(const GravSmem& g, int l, int P
         abar[j] += h2 * c_GJ[8][8] * rb;
         Spb[j] = Sb[j] + h2 * rb;
     }
-    for (int it = ncorr - 1; it >= 0; --it) {
-        double ri[3], av[3], J[3][3];
+    double J[3][3];
+    {
+        double ri[3], av[3];
 #pragma unroll
         for (int j = 0; j < 3; ++j)
-            ri[j] = iter[((int64_t)it * 3 + j) * stride];
+            ri[j] = iter[(int64_t)j * stride];
         gravity_jac_gcrs_lanes(g, l, P, M, ri, av, J, mask);
+    }
+    for (int it = ncorr - 1; it >= 0; --it) {
         double rb[3];
 #pragma unroll
         for (int k = 0; k < 3; ++k)
@@ -286,12 +315,12 @@ __global__ void __launch_bounds__(256, 1) adjoint_kernel(TableSrc ts, AdjArgs a)
             }
             for (int step = lo; step <= hi; ++step) {
                 const double* M = a.prop_m + (size_t)(step + 4) * 9;
-                double* it_base = a.scratch + (size_t)(step - lo) * K * 3 * U + u;
+                double* it_base = a.scratch + (size_t)(step - lo) * 3 * U + u;
                 auto eval = [&](const double* rr, double* aa, int it) {
-                    if (l == 0)
+                    if (l == 0 && it == K - 1)
 #pragma unroll
                         for (int j = 0; j < 3; ++j)
-                            it_base[((int64_t)it * 3 + j) * U] = rr[j];
+                            it_base[(int64_t)j * U] = rr[j];
                     gravity_gcrs_lanes<false>(g, l, P, M, rr, aa, mask);
                 };
                 gj8_step<double>(eval, a.h, K, hist, s, S, r, v);
@@ -299,7 +328,7 @@ __global__ void __launch_bounds__(256, 1) adjoint_kernel(TableSrc ts, AdjArgs a)
             __syncwarp(mask);
             for (int step = hi; step >= lo; --step) {
                 const double* M = a.prop_m + (size_t)(step + 4) * 9;
-                const double* it_base = a.scratch + (size_t)(step - lo) * K * 3 * U + u;
+                const double* it_base = a.scratch + (size_t)(step - lo) * 3 * U + u;
                 const int node = step - k0;
                 const double* seed = (node >= 0 && node < 3) ? seeds + node * 9 : nullptr;
                 gj8_reverse_step(g, l, P, mask, M, a.h, K, it_base, U, seed, hb, sb, Sb);

@@ -45,7 +45,7 @@ struct AdjArgs {
     const double* r0 = nullptr; // AoS [n_obj][3] initial state
     const double* v0 = nullptr;
     const double* ckpt = nullptr; // [segments][kCheckpointArrays][n_obj]; segment 0 = after startup
-    double* scratch = nullptr; // [kCheckpointSteps][ncorr][3][n_units] corrector iterates
+    double* scratch = nullptr; // [kCheckpointSteps][3][n_units] last evaluation point of each step
     double* grad = nullptr; // [n_units][6] d(seeded sum) / d(r0, v0)
     unsigned* err = nullptr;
 };
