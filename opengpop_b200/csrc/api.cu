@@ -243,7 +243,7 @@ gpop_status gpop_create(const gpop_config* cfg_in, gpop_ctx** out)
     if (const char* spl = std::getenv("GPOP_STEPS_PER_LAUNCH"))
         ctx->steps_per_launch = std::max(1, atoi(spl));
     if (const char* wm = std::getenv("GPOP_WALK_MODE"))
-        ctx->walk_mode = std::min(3, std::max(0, atoi(wm)));
+        ctx->walk_mode = std::min(4, std::max(0, atoi(wm)));
     cudaError_t e = cudaSetDevice(cfg.device);
     if (e != cudaSuccess)
         return cuda_fail(ctx, e, "cudaSetDevice");

@@ -57,7 +57,8 @@ LaunchShape pick_shape(int64_t n, int max_block, int num_sms);
 cudaError_t launch_startup(const TableSrc& ts, const PropArgs& a, int num_sms, cudaStream_t s);
 // How many objects a GJ8 thread carries through the gravity triangle walk (0 = by problem size).
 // kWalkLanes: P lanes per object split the gravity columns (few objects; P from lanes_per_object).
-enum WalkMode : int { kWalkOneObject = 1, kWalkTwoObjects = 2, kWalkLanes = 3 };
+// kWalkLanesTwo: two lanes per group of two objects.
+enum WalkMode : int { kWalkOneObject = 1, kWalkTwoObjects = 2, kWalkLanes = 3, kWalkLanesTwo = 4 };
 // Lanes per object (1..32, a power of 2): the most that keep n objects in one wave of 512-thread
 // blocks, one per SM.
 int lanes_per_object(int64_t n, int num_sms);

@@ -310,48 +310,63 @@ __global__ void __launch_bounds__(K == 1 ? 512 : 256, 1) gj8_kernel(F f, TableSr
     }
 }
 
-// ---- GJ8 step with P lanes per object (few objects) ----
-// Same step as gj8_kernel; the P lanes of an object's aligned group split the gravity columns
-// (lanes.cuh) and hold identical state, and lane 0 of the group stores. Used when the objects
-// alone leave most warp slots of the GPU empty (a few tens of thousands of objects or fewer).
-template <bool MIXED>
-__global__ void __launch_bounds__(512, 1) gj8_lanes_kernel(TableSrc ts, PropArgs a, int P)
+// ---- GJ8 step with P lanes per group of K objects (few objects) ----
+// Same step as gj8_kernel; the P lanes of a group split the gravity columns of its K objects
+// (lanes.cuh, lane-layout table) and hold identical state; lane 0 of the group stores. Object k
+// of group g is g + k * (groups in the grid). Used when the objects alone leave most warp slots of
+// the GPU empty.
+template <bool MIXED, int K>
+__global__ void __launch_bounds__(K == 1 ? 512 : 256, 1) gj8_lanes_kernel(TableSrc ts, PropArgs a, int P)
 {
     extern __shared__ __align__(128) uint8_t smem[];
     GravSmem g;
     if (!bind_lane_table(smem, ts, a.err, g))
         return;
-    const int64_t o = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / P;
+    const int64_t grp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / P;
+    const int64_t groups = ((int64_t)gridDim.x * blockDim.x) / P;
     const int lane = (int)(threadIdx.x & 31);
     const int l = lane & (P - 1);
-    if (o >= a.n)
+    const int64_t n = a.n;
+    if (grp >= n)
         return; // whole groups leave: shuffles name the group only
     const unsigned mask = P == 32 ? 0xffffffffu : ((1u << P) - 1u) << (lane & ~(P - 1));
     const bool lead = l == 0;
-    const int64_t n = a.n;
+    int64_t obj[K];
+    bool live[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        const int64_t o = grp + k * groups;
+        live[k] = o < n;
+        obj[k] = live[k] ? o : grp; // idle slots shadow the group's first object and never store
+    }
     double* st = a.state;
     const double h = a.h;
-    double r[3], v[3], s[3], S[3];
+    double r[K][3], v[K][3], s[K][3], S[K][3];
 #pragma unroll
-    for (int j = 0; j < 3; ++j) {
-        r[j] = st[(kR + j) * n + o];
-        v[j] = st[(kV + j) * n + o];
-        s[j] = st[(kSs + j) * n + o];
-        S[j] = st[(kSb + j) * n + o];
-    }
+    for (int k = 0; k < K; ++k)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            r[k][j] = st[(kR + j) * n + obj[k]];
+            v[k][j] = st[(kV + j) * n + obj[k]];
+            s[k][j] = st[(kSs + j) * n + obj[k]];
+            S[k][j] = st[(kSb + j) * n + obj[k]];
+        }
     for (int step = a.step_begin; step < a.step_end; ++step) {
-        double ae[3];
+        double ae[K][3];
         if (step <= 4) {
 #pragma unroll
-            for (int j = 0; j < 3; ++j) {
-                r[j] = st[(kRep + (step - 1) * 6 + j) * n + o];
-                v[j] = st[(kRep + (step - 1) * 6 + 3 + j) * n + o];
-                ae[j] = st[(kRepA + (step - 1) * 3 + j) * n + o];
-            }
+            for (int k = 0; k < K; ++k)
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    r[k][j] = st[(kRep + (step - 1) * 6 + j) * n + obj[k]];
+                    v[k][j] = st[(kRep + (step - 1) * 6 + 3 + j) * n + obj[k]];
+                    ae[k][j] = st[(kRepA + (step - 1) * 3 + j) * n + obj[k]];
+                }
         } else {
             const int ring0 = (step - 5) % 9;
-            double s1[3], s2[3], prev[3], a7[3], a8[3];
-            {
+            double s1[K][3], s2[K][3], prev[K][3], a7[K][3], a8[K][3];
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
                 double hist[9][3];
 #pragma unroll
                 for (int c = 0; c < 9; ++c) {
@@ -359,7 +374,7 @@ __global__ void __launch_bounds__(512, 1) gj8_lanes_kernel(TableSrc ts, PropArgs
                     slot -= slot >= 9 ? 9 : 0;
 #pragma unroll
                     for (int j = 0; j < 3; ++j)
-                        hist[c][j] = st[(kHist + slot * 3 + j) * n + o];
+                        hist[c][j] = st[(kHist + slot * 3 + j) * n + obj[k]];
                 }
 #pragma unroll
                 for (int j = 0; j < 3; ++j) { // as gj8_kernel
@@ -369,63 +384,77 @@ __global__ void __launch_bounds__(512, 1) gj8_lanes_kernel(TableSrc ts, PropArgs
                         vt = fma(hist[c][j], c_SA[9][c], vt);
                         rt = fma(hist[c][j], c_GJ[9][c], rt);
                     }
-                    S[j] += s[j] + hist[8][j] / 2;
-                    v[j] = (vt + s[j] + hist[8][j] / 2) * h;
-                    r[j] = (rt + S[j]) * h * h;
+                    S[k][j] += s[k][j] + hist[8][j] / 2;
+                    v[k][j] = (vt + s[k][j] + hist[8][j] / 2) * h;
+                    r[k][j] = (rt + S[k][j]) * h * h;
                     double c1 = 0.0, c2 = 0.0;
 #pragma unroll
                     for (int c = 0; c < 8; ++c) {
                         c1 = fma(hist[c + 1][j], c_SA[8][c], c1);
                         c2 = fma(hist[c + 1][j], c_GJ[8][c], c2);
                     }
-                    s1[j] = c1;
-                    s2[j] = c2;
-                    prev[j] = s[j];
-                    a7[j] = hist[8][j];
+                    s1[k][j] = c1;
+                    s2[k][j] = c2;
+                    prev[k][j] = s[k][j];
+                    a7[k][j] = hist[8][j];
                 }
             }
             const double* M = a.prop_m + (size_t)(step + 4) * 9;
             for (int it = 0; it < a.ncorr; ++it) {
-                gravity_gcrs_lanes<MIXED>(g, l, P, M, r, a8, mask);
+                gravity_gcrs_lk<MIXED, K>(g, l, P, M, r, a8, mask);
+#pragma unroll
+                for (int k = 0; k < K; ++k)
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) {
+                        s[k][j] = prev[k][j] + (a8[k][j] + a7[k][j]) / 2;
+                        v[k][j] = h * (s1[k][j] + a8[k][j] * c_SA[8][8] + s[k][j]);
+                        r[k][j] = h * h * (s2[k][j] + a8[k][j] * c_GJ[8][8] + S[k][j]);
+                    }
+            }
+#pragma unroll
+            for (int k = 0; k < K; ++k)
 #pragma unroll
                 for (int j = 0; j < 3; ++j) {
-                    s[j] = prev[j] + (a8[j] + a7[j]) / 2;
-                    v[j] = h * (s1[j] + a8[j] * c_SA[8][8] + s[j]);
-                    r[j] = h * h * (s2[j] + a8[j] * c_GJ[8][8] + S[j]);
+                    if (lead && live[k])
+                        st[(kHist + ring0 * 3 + j) * n + obj[k]] = a8[k][j];
+                    ae[k][j] = a8[k][j];
                 }
-            }
-#pragma unroll
-            for (int j = 0; j < 3; ++j) {
-                if (lead)
-                    st[(kHist + ring0 * 3 + j) * n + o] = a8[j];
-                ae[j] = a8[j];
-            }
         }
         __syncwarp(mask); // the group's ring write precedes its next step's loads
         if (lead) {
             const int64_t t = step - a.traj_step0;
-            for (int j = 0; j < 3; ++j) {
-                if (a.traj_r)
-                    a.traj_r[(t * 3 + j) * n + o] = r[j];
-                if (a.traj_v)
-                    a.traj_v[(t * 3 + j) * n + o] = v[j];
-                if (a.traj_a)
-                    a.traj_a[(t * 3 + j) * n + o] = ae[j];
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                if (!live[k])
+                    continue;
+                for (int j = 0; j < 3; ++j) {
+                    if (a.traj_r)
+                        a.traj_r[(t * 3 + j) * n + obj[k]] = r[k][j];
+                    if (a.traj_v)
+                        a.traj_v[(t * 3 + j) * n + obj[k]] = v[k][j];
+                    if (a.traj_a)
+                        a.traj_a[(t * 3 + j) * n + obj[k]] = ae[k][j];
+                }
             }
         }
     }
     if (!lead)
         return;
 #pragma unroll
-    for (int j = 0; j < 3; ++j) {
-        st[(kR + j) * n + o] = r[j];
-        st[(kV + j) * n + o] = v[j];
-        st[(kSs + j) * n + o] = s[j];
-        st[(kSb + j) * n + o] = S[j];
-        if (a.out_r)
-            a.out_r[o * 3 + j] = r[j];
-        if (a.out_v)
-            a.out_v[o * 3 + j] = v[j];
+    for (int k = 0; k < K; ++k) {
+        if (!live[k])
+            continue;
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            st[(kR + j) * n + obj[k]] = r[k][j];
+            st[(kV + j) * n + obj[k]] = v[k][j];
+            st[(kSs + j) * n + obj[k]] = s[k][j];
+            st[(kSb + j) * n + obj[k]] = S[k][j];
+            if (a.out_r)
+                a.out_r[obj[k] * 3 + j] = r[k][j];
+            if (a.out_v)
+                a.out_v[obj[k] * 3 + j] = v[k][j];
+        }
     }
 }
 
@@ -609,35 +638,56 @@ cudaError_t launch_gj8(const TableSrc& ts, const PropArgs& a, int num_sms, cudaS
 {
     if (a.n <= 0 || a.step_end <= a.step_begin)
         return cudaSuccess;
-    // Default walk (measured on B200 at 70x70): two objects per thread from 128 objects per SM;
-    // below that 4 or more lanes per object (2.8x faster at 4,096 objects, 4.9x at 1,024 than one
-    // object per thread); one object per thread when no lane-layout table is at hand.
+    // Default walk (measured on B200 at 70x70): two objects per thread from 320 objects per SM;
+    // from 128 to 320 objects per SM two lanes per pair of objects (mixed: 20,000 objects 52 ->
+    // 61 M object-steps/s, 37,000 94 -> 110 M; FP64 +4 %); below 128, 4 or more lanes per object
+    // (2.8x faster at 4,096 objects, 4.9x at 1,024 than one object per thread). One or two objects
+    // per thread when no lane-layout table is at hand.
     if (walk <= 0) {
-        if (a.n >= (int64_t)num_sms * 128)
+        const bool lanes = lane_ts && a.kind == 0;
+        if (a.n >= (int64_t)num_sms * 320 || (!lanes && a.n >= (int64_t)num_sms * 128))
             walk = kWalkTwoObjects;
+        else if (a.n >= (int64_t)num_sms * 128)
+            walk = kWalkLanesTwo;
         else
-            walk = (lane_ts && a.kind == 0) ? kWalkLanes : kWalkOneObject;
+            walk = lanes ? kWalkLanes : kWalkOneObject;
     }
-    if (walk == kWalkLanes && a.kind == 0 && lane_ts) {
+    if ((walk == kWalkLanes || walk == kWalkLanesTwo) && a.kind == 0 && lane_ts) {
         const TableSrc& lt = *lane_ts;
-        const int P = lanes_per_object(a.n, num_sms);
-        const int64_t threads = a.n * P;
+        const int K = walk == kWalkLanesTwo ? 2 : 1;
+        const int64_t groups = (a.n + K - 1) / K;
+        const int P = walk == kWalkLanesTwo ? 2 : lanes_per_object(a.n, num_sms);
+        const int64_t threads = groups * P;
         const int64_t per_sm = (threads + num_sms - 1) / num_sms; // spread over every SM
-        const int block = (int)std::min<int64_t>(512, std::max<int64_t>(32, ((per_sm + 31) / 32) * 32));
+        const int cap = K == 1 ? 512 : 256;
+        const int block = (int)std::min<int64_t>(cap, std::max<int64_t>(32, ((per_sm + 31) / 32) * 32));
+        const unsigned grid = (unsigned)((threads + block - 1) / block);
         const size_t smem = table_smem_bytes(lt);
         cudaError_t e;
         if (lt.mixed) {
-            if ((e = set_smem(gj8_lanes_kernel<true>, smem)) != cudaSuccess)
-                return e;
-            gj8_lanes_kernel<true><<<(unsigned)((threads + block - 1) / block), block, smem, s>>>(lt, a, P);
+            if (K == 1) {
+                if ((e = set_smem(gj8_lanes_kernel<true, 1>, smem)) != cudaSuccess)
+                    return e;
+                gj8_lanes_kernel<true, 1><<<grid, block, smem, s>>>(lt, a, P);
+            } else {
+                if ((e = set_smem(gj8_lanes_kernel<true, 2>, smem)) != cudaSuccess)
+                    return e;
+                gj8_lanes_kernel<true, 2><<<grid, block, smem, s>>>(lt, a, P);
+            }
         } else {
-            if ((e = set_smem(gj8_lanes_kernel<false>, smem)) != cudaSuccess)
-                return e;
-            gj8_lanes_kernel<false><<<(unsigned)((threads + block - 1) / block), block, smem, s>>>(lt, a, P);
+            if (K == 1) {
+                if ((e = set_smem(gj8_lanes_kernel<false, 1>, smem)) != cudaSuccess)
+                    return e;
+                gj8_lanes_kernel<false, 1><<<grid, block, smem, s>>>(lt, a, P);
+            } else {
+                if ((e = set_smem(gj8_lanes_kernel<false, 2>, smem)) != cudaSuccess)
+                    return e;
+                gj8_lanes_kernel<false, 2><<<grid, block, smem, s>>>(lt, a, P);
+            }
         }
         return cudaGetLastError();
     }
-    if (walk == kWalkLanes)
+    if (walk == kWalkLanes || walk == kWalkLanesTwo)
         walk = kWalkOneObject;
     if (a.kind == 0) {
         if (ts.mixed) {
