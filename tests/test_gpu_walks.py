@@ -1,0 +1,56 @@
+"""The GJ8 walks of the propagation kernels (one or two objects per thread; 4..32 lanes per object;
+two lanes per pair of objects) give the same propagation to rounding, FP64 and mixed, and the
+FP64 walks agree with the CPU oracle. The walk is forced per context with GPOP_WALK_MODE."""
+import os
+
+import numpy as np
+import pytest
+
+import oracle_api as O
+
+pytestmark = pytest.mark.gpu
+
+START = (2024, 1, 1, 0, 0, 0.0)
+
+
+def _run(walk, precision, r, v, steps):
+    import opengpop_b200 as G
+    old = os.environ.get("GPOP_WALK_MODE")
+    os.environ["GPOP_WALK_MODE"] = str(walk)
+    try:
+        c = G.Context(precision=precision)
+    finally:
+        if old is None:
+            del os.environ["GPOP_WALK_MODE"]
+        else:
+            os.environ["GPOP_WALK_MODE"] = old
+    try:
+        return c.propagate(START, 30.0, steps, r, v)
+    finally:
+        c.close()
+
+
+@pytest.mark.parametrize("n", [37, 3000, 20000])
+@pytest.mark.parametrize("precision", [0, 1])
+def test_walks_agree(n, precision):
+    from opengpop_b200 import orbits
+    r, v = orbits.mixed_population(n, seed=60 + n)
+    steps = 40
+    ref_r, ref_v = _run(2, precision, r, v, steps)  # two objects per thread
+    for walk in (1, 3, 4):
+        rr, vv = _run(walk, precision, r, v, steps)
+        # summation order differs between walks: FP64 agrees to rounding; the mixed walks differ
+        # by FP32 rounding of the degree > 8 sums
+        tol_r, tol_v = (1e-6, 1e-9) if precision == 0 else (1e-3, 1e-6)
+        assert np.abs(rr - ref_r).max() < tol_r, (walk, np.abs(rr - ref_r).max())
+        assert np.abs(vv - ref_v).max() < tol_v
+
+
+def test_lane_walks_match_oracle(oracle_data):
+    from opengpop_b200 import orbits
+    r, v = orbits.mixed_population(24, seed=71)
+    steps = 30
+    ro, vo = O.propagate(oracle_data, "gravity", START, 30.0, steps, r, v)
+    for walk in (3, 4):
+        rr, vv = _run(walk, 0, r, v, steps)
+        assert np.abs(rr - ro).max() < 1e-6 and np.abs(vv - vo).max() < 1e-9
