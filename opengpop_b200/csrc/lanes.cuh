@@ -102,8 +102,13 @@ __device__ __forceinline__ void gravity_itrs_lk(const GravSmem& gs, int l, int P
         G[k] = H[k] = J[k] = KK[k] = 0.0;
     }
     const int Lhead = (MIXED && L > kMixedSplit) ? kMixedSplit : L;
+    // column bases of the lane's next column are read one column ahead (they are shared-memory
+    // loads the walk's first table read depends on)
+    int b64 = gs.cb64[l], b32 = gs.cb32[l];
     int m = l;
     for (; m <= Lhead; m += P) {
+        const int mn = m + P < 127 ? m + P : 127;
+        const int nb64 = gs.cb64[mn], nb32 = gs.cb32[mn];
         ColSums64<K> s;
         s.zero();
         double Q1[K], Q2[K];
@@ -112,7 +117,7 @@ __device__ __forceinline__ void gravity_itrs_lk(const GravSmem& gs, int l, int P
             Q1[k] = qm[k];
             Q2[k] = 0.0;
         }
-        const GravEntry64* e = lane_col64(gs, m); // mixed: the head table (n <= 8)
+        const GravEntry64* e = reinterpret_cast<const GravEntry64*>(reinterpret_cast<const uint4*>(gs.t64) + b64);
         s.add(e, Q1);
         column64<K>(e, 1, Lhead - m, u, w, Q1, Q2, s);
         if constexpr (MIXED) {
@@ -125,7 +130,8 @@ __device__ __forceinline__ void gravity_itrs_lk(const GravSmem& gs, int l, int P
                     Q1f[k] = (float)Q1[k];
                     Q2f[k] = (float)Q2[k];
                 }
-                column32k<K>(lane_col32(gs, m), kMixedSplit + 1 - m, L - m, uf, wf, Q1f, Q2f, f);
+                column32k<K>(reinterpret_cast<const GravEntry32*>(reinterpret_cast<const uint4*>(gs.t32) + b32),
+                    kMixedSplit + 1 - m, L - m, uf, wf, Q1f, Q2f, f);
 #pragma unroll
                 for (int k = 0; k < K; ++k) {
                     s.g1[k] += (double)f.g[k].x;
@@ -153,6 +159,8 @@ __device__ __forceinline__ void gravity_itrs_lk(const GravSmem& gs, int l, int P
             cmul(Cm[k], Sm[k], CP[k], SP[k], Cm[k], Sm[k]);
             qm[k] *= qP[k];
         }
+        b64 = nb64;
+        b32 = nb32;
     }
     if constexpr (MIXED) {
         if (m <= L) { // this lane's columns m > 8, in FP32
@@ -171,8 +179,9 @@ __device__ __forceinline__ void gravity_itrs_lk(const GravSmem& gs, int l, int P
                 Gf[k] = Hf[k] = Jf[k] = Kf[k] = 0.f;
             }
             for (; m <= L; m += P) {
+                const int nb = gs.cb32[m + P < 127 ? m + P : 127];
                 ColSums32<K> f;
-                const GravEntry32* e32 = lane_col32(gs, m);
+                const GravEntry32* e32 = reinterpret_cast<const GravEntry32*>(reinterpret_cast<const uint4*>(gs.t32) + b32);
                 const float4* p = reinterpret_cast<const float4*>(e32);
                 const float4 a = p[0], b = p[1];
                 float Q1f[K], Q2f[K];
@@ -201,6 +210,7 @@ __device__ __forceinline__ void gravity_itrs_lk(const GravSmem& gs, int l, int P
                     spf[k] = s2;
                     qmf[k] *= qPf[k];
                 }
+                b32 = nb;
             }
 #pragma unroll
             for (int k = 0; k < K; ++k) {
