@@ -224,14 +224,22 @@ def _common(args, metric, value, unit, dtype, config, extra):
 
 
 def run_batch(args, torch, G, dev):
-    """Batched uneven requests: 4,096 requests in one persistent launch under a captured graph."""
-    from opengpop_b200 import orbits
-    reqs = orbits.batch_requests(args.batch_requests, SEED, max_days=args.batch_max_days)
+    """Batched uneven requests: 4,096 requests in one persistent launch under a captured graph.
+    Under torchrun the requests are split over the ranks by longest-processing-time bin packing of
+    the cost model (no exchange while propagating); the time is the max over ranks."""
+    import torch.distributed as dist
+    from opengpop_b200 import orbits, sharding
+    rank, world = env_int("RANK", 0), env_int("WORLD_SIZE", 1)
+    all_reqs = orbits.batch_requests(args.batch_requests, SEED, max_days=args.batch_max_days)
+    bins = sharding.lpt_partition([sharding.request_cost(q["r"].shape[0], q["steps"], q["degree"])
+                                   for q in all_reqs], world)
+    reqs = [all_reqs[i] for i in bins[rank]]
+    osteps_all = sum(q["r"].shape[0] * q["steps"] for q in all_reqs)
     osteps = sum(q["r"].shape[0] * q["steps"] for q in reqs)
     f_total = sum(q["r"].shape[0] * q["steps"] * flops_per_object_step(q["degree"]) for q in reqs)
     f32 = sum(q["r"].shape[0] * q["steps"] * fp32_flops_per_object_step(q["degree"])
               for q in reqs if q["degree"] > 8)
-    ctx = G.Context(precision=G.MIXED)
+    ctx = G.Context(device=dev.index, precision=G.MIXED)
     t0 = time.perf_counter()
     if not args.no_tune:
         ctx.tune()
@@ -251,22 +259,31 @@ def run_batch(args, torch, G, dev):
     clocks = sampler.stop()
     launches = ctx.kernel_launches - launches0
     ctx.close()
-    t = sum(dev_t) / len(dev_t)
+    t = sharding.max_over_ranks(sum(dev_t) / len(dev_t), dev)
+    t_wall = sharding.max_over_ranks(sum(wall_t) / len(wall_t), dev)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
     peak64, peak32 = _peaks(torch, dev)
     achieved = f_total / t / 1e12
     t_min = (f_total - f32) / (peak64 * 1e12) + f32 / (peak32 * 1e12) if peak64 and peak32 else None
-    io = sum(q["r"].shape[0] for q in reqs) * 6 * 8
-    _common(args, "object-steps/s, batched uneven requests (mixed precision)", osteps / t,
+    io = sum(q["r"].shape[0] for q in all_reqs) * 6 * 8
+    args.gpus = world
+    _common(args, "object-steps/s, batched uneven requests (mixed precision)", osteps_all / t,
             "object-steps/s", "f64+f32",
             {"workload": "%d requests (objects log-uniform 1-512, 1 h-7 d, h in {10,30,60,120} s, "
                          "degree in {8,20,36,70}, seed %d), one persistent launch per batch"
-                         % (len(reqs), SEED),
-             "object_steps_per_batch": osteps, "l2": "inputs (and state) larger than L2",
+                         % (len(all_reqs), SEED),
+             "object_steps_per_batch": osteps_all, "l2": "inputs (and state) larger than L2",
+             "parallelism": "replicas" if world == 1 else "requests over %d ranks (LPT)" % world,
              "lanes_per_object_histogram": np.bincount(lpo, minlength=33)[[1, 2, 4, 8, 16, 32]].tolist(),
              "planner_estimate_s": est, "tune_s": tune_s},
-            {"ms_per_step": 1e3 * t,
-             "requests_per_s": len(reqs) / t,
-             "e2e": {"value": osteps / (sum(wall_t) / len(wall_t)), "unit": "object-steps/s",
+            {"n_gpus": world, "scaling": "strong",
+             "ms_per_step": 1e3 * t,
+             "requests_per_s": len(all_reqs) / t,
+             "e2e": {"value": osteps_all / t_wall, "unit": "object-steps/s",
                      "h2d_bytes_per_step": io, "d2h_bytes_per_step": io,
                      "call": "gpop_propagate_batch (host buffers, packing, copies)"},
              "roofline": {"bound": "fp64+fp32", "achieved": achieved,
@@ -431,14 +448,19 @@ def main():
     if args.impl == "reference":
         return run_reference(args)
     if args.workload != "propagate":
-        if env_int("RANK", 0) != 0:
-            return 0
         import torch
         import opengpop_b200 as G
         dev = torch.device("cuda", env_int("LOCAL_RANK", 0))
         torch.cuda.set_device(dev)
-        return {"batch": run_batch, "screen": run_screen, "adjoint": run_adjoint}[args.workload](
-            args, torch, G, dev)
+        if args.workload == "batch":
+            if env_int("WORLD_SIZE", 1) > 1:
+                import datetime
+                import torch.distributed as dist
+                dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+            return run_batch(args, torch, G, dev)
+        if env_int("RANK", 0) != 0:
+            return 0
+        return {"screen": run_screen, "adjoint": run_adjoint}[args.workload](args, torch, G, dev)
 
     import torch
     import torch.distributed as dist
