@@ -28,6 +28,7 @@
 #include <cstdlib>
 #include <stdexcept>
 #include <string>
+#include <utility>
 #include <vector>
 
 typedef struct cublasContext* cublasHandle_t;
@@ -92,8 +93,8 @@ public:
             cudaFree(_frames);
         if (_tmp)
             cudaFree(_tmp);
-        if (_ctx)
-            gpop_destroy(_ctx);
+        for (auto& kv : _contexts)
+            gpop_destroy(kv.second);
     }
     ForceModel(const ForceModel&) = delete;
     ForceModel& operator=(const ForceModel&) = delete;
@@ -128,14 +129,13 @@ public:
         evaluate(devPosition, stepNum, devAcceleration + 3 * returnColumnIndex, 27);
     }
 
-    // The library context (FP64, numCorrections corrector passes), created on first use.
+    // The library context (FP64, numCorrections corrector passes), created on first use and kept
+    // until the ForceModel is destroyed (propagators built on it may still be alive).
     gpop_ctx* context(int numCorrections)
     {
-        if (_ctx && _ncorr == numCorrections)
-            return _ctx;
-        if (_ctx)
-            gpop_destroy(_ctx);
-        _ctx = nullptr;
+        for (auto& kv : _contexts)
+            if (kv.first == numCorrections)
+                return _ctx = kv.second, _ncorr = numCorrections, _ctx;
         gpop_config cfg;
         gpop_config_default(&cfg);
         cfg.data_dir = DataDirectory().c_str();
@@ -148,6 +148,7 @@ public:
                 gpop_destroy(c);
             throw std::runtime_error("ForceModel: " + msg);
         }
+        _contexts.push_back({ numCorrections, c });
         _ctx = c;
         _ncorr = numCorrections;
         return _ctx;
@@ -159,7 +160,8 @@ private:
     unsigned _n;
     double _h;
     FullPerturbationParameters* _params;
-    gpop_ctx* _ctx = nullptr;
+    std::vector<std::pair<int, gpop_ctx*>> _contexts;
+    gpop_ctx* _ctx = nullptr; // the most recently used of _contexts
     int _ncorr = 0;
     double* _frames = nullptr;
     int _count = 0;
