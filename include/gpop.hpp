@@ -134,8 +134,11 @@ public:
     gpop_ctx* context(int numCorrections)
     {
         for (auto& kv : _contexts)
-            if (kv.first == numCorrections)
-                return _ctx = kv.second, _ncorr = numCorrections, _ctx;
+            if (kv.first == numCorrections) {
+                _ctx = kv.second;
+                _ncorr = numCorrections;
+                return _ctx;
+            }
         gpop_config cfg;
         gpop_config_default(&cfg);
         cfg.data_dir = DataDirectory().c_str();
