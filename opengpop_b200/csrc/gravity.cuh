@@ -8,7 +8,8 @@
 // object: 3 FP64 ops for the recursion and 6 FMAs into per-column sums; per column the sums are
 // combined with the cos/sin(m lambda) recursion of eq. 3-18. The (R/r)^n factor of eq. 4-12 rides
 // in the recursion variable, so no per-degree sums are needed. With K objects per thread every
-// table entry loaded from shared memory feeds K independent chains.
+// table entry loaded from shared memory feeds K independent chains; with two objects the columns
+// are also walked two at a time, so each thread carries two independent recursions.
 //
 // Mixed precision: terms of degree n <= 8 (and all per-column combining, the central term, frame
 // rotations and the final assembly) stay FP64; the n > 8 recursion and sums run in FP32 with
@@ -31,8 +32,32 @@ constexpr int kMixedSplit = 8; // highest degree kept in FP64 in the mixed mode
 #ifndef GPOP_COL64_UNROLL
 #define GPOP_COL64_UNROLL 4
 #endif
+// Two objects per thread walk the columns two at a time (two independent recursions per thread
+// hide each other's latency). Measured on B200, 65,536 objects at 70x70, with the corrector state
+// in shared memory: mixed 123.9 -> 139.4 M object-steps/s (pair unroll 4: 137.6, 8: 139.4, 12:
+// 139.0; three columns at a time 130.5, four 121.3), FP64 72.3 -> 73.8 M (pair unroll 2).
+#ifndef GPOP_COLPAIR_UNROLL
+#define GPOP_COLPAIR_UNROLL 8
+#endif
+#ifndef GPOP_COLGROUP_UNROLL
+#define GPOP_COLGROUP_UNROLL 4
+#endif
+#ifndef GPOP_PAIR_COLUMNS
+#define GPOP_PAIR_COLUMNS 1
+#endif
+#ifndef GPOP_PAIR_COLUMNS64
+#define GPOP_PAIR_COLUMNS64 1
+#endif
+#ifndef GPOP_COL64PAIR_UNROLL
+#define GPOP_COL64PAIR_UNROLL 2
+#endif
 constexpr int kCol32x2Unroll = GPOP_COL32X2_UNROLL;
 constexpr int kCol64Unroll = GPOP_COL64_UNROLL;
+constexpr int kColPairUnroll = GPOP_COLPAIR_UNROLL;
+constexpr int kColGroupUnroll = GPOP_COLGROUP_UNROLL;
+constexpr bool kPairColumns = GPOP_PAIR_COLUMNS != 0;
+constexpr bool kPairColumns64 = GPOP_PAIR_COLUMNS64 != 0;
+constexpr int kCol64PairUnroll = GPOP_COL64PAIR_UNROLL;
 
 struct GravSmem {
     const GravEntry64* t64; // FP64 mode: full table; mixed mode: head table (n <= 8)
@@ -68,6 +93,23 @@ template <int K> struct ColSums64 {
     }
 };
 
+// One FP64 term at entry e: t2 holds c(n) w Q(n-2) on entry and c(n+1) w Q(n-1) on exit.
+template <int K>
+__device__ __forceinline__ void term64(const GravEntry64* __restrict__ e, const double (&u)[K],
+    const double (&w)[K], double (&Q1)[K], double (&Q2)[K], double (&t2)[K], ColSums64<K>& s)
+{
+    const double cn = reinterpret_cast<const double2*>(e + 1)[0].x;
+    double Q[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        Q[k] = fma(u[k], Q1[k], -t2[k]);
+        t2[k] = (cn * w[k]) * Q1[k];
+        Q2[k] = Q1[k];
+        Q1[k] = Q[k];
+    }
+    s.add(e, Q);
+}
+
 // Walks column entries e[first..last] in FP64, continuing the recursion from Q1 = Q(n-1),
 // Q2 = Q(n-2) of each object. The product c(n+1) w Q(n-1) of the next term is formed while the
 // current term accumulates, so one FMA separates consecutive Q values on the dependency chain.
@@ -86,17 +128,34 @@ __device__ __forceinline__ void column64(const GravEntry64* __restrict__ e, int 
             t2[k] = (c * w[k]) * Q2[k];
     }
 #pragma unroll(kCol64Unroll)
-    for (int i = first; i <= last; ++i) {
-        const double cn = reinterpret_cast<const double2*>(e + i + 1)[0].x;
-        double Q[K];
+    for (int i = first; i <= last; ++i)
+        term64<K>(e + i, u, w, Q1, Q2, t2, s);
+}
+
+// Two FP64 columns walked side by side: N terms at entries ea[0..N-1] and eb[0..N-1], each with
+// the operations of column64 in its order (bit-identical sums).
+template <int K>
+__device__ __forceinline__ void column64_pair(const GravEntry64* __restrict__ ea,
+    const GravEntry64* __restrict__ eb, int N, const double (&u)[K], const double (&w)[K],
+    double (&Qa1)[K], double (&Qa2)[K], ColSums64<K>& sa, double (&Qb1)[K], double (&Qb2)[K],
+    ColSums64<K>& sb)
+{
+    if (N <= 0)
+        return;
+    double ta[K], tb[K];
+    {
+        const double ca = reinterpret_cast<const double2*>(ea)[0].x;
+        const double cb = reinterpret_cast<const double2*>(eb)[0].x;
 #pragma unroll
         for (int k = 0; k < K; ++k) {
-            Q[k] = fma(u[k], Q1[k], -t2[k]);
-            t2[k] = (cn * w[k]) * Q1[k];
-            Q2[k] = Q1[k];
-            Q1[k] = Q[k];
+            ta[k] = (ca * w[k]) * Qa2[k];
+            tb[k] = (cb * w[k]) * Qb2[k];
         }
-        s.add(e + i, Q);
+    }
+#pragma unroll(kCol64PairUnroll)
+    for (int t = 0; t < N; ++t) {
+        term64<K>(ea + t, u, w, Qa1, Qa2, ta, sa);
+        term64<K>(eb + t, u, w, Qb1, Qb2, tb, sb);
     }
 }
 
@@ -134,31 +193,62 @@ __device__ __forceinline__ void column32(const GravEntry32* __restrict__ e, int 
 }
 
 // Two objects: the recursion of both objects is one packed chain (Q = (Q_A, Q_B)).
+// One term at entry e: t2 holds -c(n) w Q(n-2) on entry and -c(n+1) w Q(n-1) on exit.
+__device__ __forceinline__ void term32x2(const GravEntry32* __restrict__ e, float2 u, float2 w,
+    float2& Q1, float2& Q2, float2& t2, ColSums32<2>& s)
+{
+    const float4* p = reinterpret_cast<const float4*>(e);
+    const float4 a = p[0], b = p[1];
+    const float4 an = reinterpret_cast<const float4*>(e + 1)[0];
+    const float2 Q = __ffma2_rn(u, Q1, t2);
+    t2 = __fmul2_rn(__fmul2_rn(make_float2(an.x, an.y), w), Q1);
+    const float2 QA = make_float2(Q.x, Q.x), QB = make_float2(Q.y, Q.y);
+    const float2 cg = make_float2(a.z, a.w), cj = make_float2(b.x, b.y), ch = make_float2(b.z, b.w);
+    s.g[0] = __ffma2_rn(QA, cg, s.g[0]);
+    s.j[0] = __ffma2_rn(QA, cj, s.j[0]);
+    s.h[0] = __ffma2_rn(QA, ch, s.h[0]);
+    s.g[1] = __ffma2_rn(QB, cg, s.g[1]);
+    s.j[1] = __ffma2_rn(QB, cj, s.j[1]);
+    s.h[1] = __ffma2_rn(QB, ch, s.h[1]);
+    Q2 = Q1;
+    Q1 = Q;
+}
+
+__device__ __forceinline__ float2 first_t2(const GravEntry32* __restrict__ e, float2 w, float2 Q2)
+{
+    const float4 a0 = reinterpret_cast<const float4*>(e)[0];
+    return __fmul2_rn(__fmul2_rn(make_float2(a0.x, a0.y), w), Q2);
+}
+
+// The single term at entry e of a column whose walk ends there (t2 formed from Q2 first).
+__device__ __forceinline__ void last_term32x2(const GravEntry32* __restrict__ e, float2 u, float2 w,
+    float2& Q1, float2& Q2, ColSums32<2>& s)
+{
+    const float4* p = reinterpret_cast<const float4*>(e);
+    const float4 a = p[0], b = p[1];
+    const float2 t2 = __fmul2_rn(__fmul2_rn(make_float2(a.x, a.y), w), Q2);
+    const float2 Q = __ffma2_rn(u, Q1, t2);
+    const float2 QA = make_float2(Q.x, Q.x), QB = make_float2(Q.y, Q.y);
+    const float2 cg = make_float2(a.z, a.w), cj = make_float2(b.x, b.y), ch = make_float2(b.z, b.w);
+    s.g[0] = __ffma2_rn(QA, cg, s.g[0]);
+    s.j[0] = __ffma2_rn(QA, cj, s.j[0]);
+    s.h[0] = __ffma2_rn(QA, ch, s.h[0]);
+    s.g[1] = __ffma2_rn(QB, cg, s.g[1]);
+    s.j[1] = __ffma2_rn(QB, cj, s.j[1]);
+    s.h[1] = __ffma2_rn(QB, ch, s.h[1]);
+    Q2 = Q1;
+    Q1 = Q;
+}
+
 __device__ __forceinline__ void column32x2(const GravEntry32* __restrict__ e, int first, int last,
     float2 u, float2 w, float2& Q1, float2& Q2, ColSums32<2>& s)
 {
     if (first > last)
         return;
-    const float4 a0 = reinterpret_cast<const float4*>(e + first)[0];
-    float2 t2 = __fmul2_rn(__fmul2_rn(make_float2(a0.x, a0.y), w), Q2);
+    float2 t2 = first_t2(e + first, w, Q2);
 #pragma unroll(kCol32x2Unroll)
-    for (int i = first; i <= last; ++i) {
-        const float4* p = reinterpret_cast<const float4*>(e + i);
-        const float4 a = p[0], b = p[1];
-        const float4 an = reinterpret_cast<const float4*>(e + i + 1)[0];
-        const float2 Q = __ffma2_rn(u, Q1, t2);
-        t2 = __fmul2_rn(__fmul2_rn(make_float2(an.x, an.y), w), Q1);
-        const float2 QA = make_float2(Q.x, Q.x), QB = make_float2(Q.y, Q.y);
-        const float2 cg = make_float2(a.z, a.w), cj = make_float2(b.x, b.y), ch = make_float2(b.z, b.w);
-        s.g[0] = __ffma2_rn(QA, cg, s.g[0]);
-        s.j[0] = __ffma2_rn(QA, cj, s.j[0]);
-        s.h[0] = __ffma2_rn(QA, ch, s.h[0]);
-        s.g[1] = __ffma2_rn(QB, cg, s.g[1]);
-        s.j[1] = __ffma2_rn(QB, cj, s.j[1]);
-        s.h[1] = __ffma2_rn(QB, ch, s.h[1]);
-        Q2 = Q1;
-        Q1 = Q;
-    }
+    for (int i = first; i <= last; ++i)
+        term32x2(e + i, u, w, Q1, Q2, t2, s);
 }
 
 template <int K>
@@ -179,11 +269,304 @@ __device__ __forceinline__ void column32k(const GravEntry32* __restrict__ e, int
     }
 }
 
+// C FP32 columns of two objects walked side by side: N terms at entries e[c][0..N-1], each column
+// with the operations of column32x2 in its order (bit-identical sums).
+template <int C>
+__device__ __forceinline__ void column32x2_group(const GravEntry32* const (&e)[C], int N, float2 u,
+    float2 w, float2 (&Q1)[C], float2 (&Q2)[C], ColSums32<2> (&s)[C])
+{
+    if (N <= 0)
+        return;
+    float2 t[C];
+#pragma unroll
+    for (int c = 0; c < C; ++c)
+        t[c] = first_t2(e[c], w, Q2[c]);
+#pragma unroll(C == 2 ? kColPairUnroll : kColGroupUnroll)
+    for (int i = 0; i < N; ++i)
+#pragma unroll
+        for (int c = 0; c < C; ++c)
+            term32x2(e[c] + i, u, w, Q1[c], Q2[c], t[c], s[c]);
+}
+
+// Mixed precision, two objects, degree L > 8: the walk of gravity_itrs<true, 2> with the FP32
+// parts of the columns taken kHeadGroup (columns m <= 8) or kTailGroup (m > 8) columns at a time.
+// Every column's sums, their combination and the order of the combinations are those of the
+// one-column walk, so the accelerations are bit-identical to it.
+struct MixedWalk2 {
+    static constexpr int K = 2;
+    const GravSmem& gs;
+    int L;
+    double q[K], u[K], w[K], C1[K], S1[K], Cm[K], Sm[K], Cp[K], Sp[K], qm[K];
+    double G[K], H[K], J[K], KK[K];
+    float2 uf, wf;
+    float cf[K], sf[K], cpf[K], spf[K], qmf[K], c1f[K], s1f[K], qf[K];
+    float Gf[K], Hf[K], Jf[K], Kf[K];
+
+    __device__ __forceinline__ MixedWalk2(const GravSmem& g, const double (&r)[K], const double (&x)[K],
+        const double (&y)[K], const double (&z)[K])
+        : gs(g)
+        , L(g.L)
+    {
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const double eps = z[k] / r[k];
+            q[k] = gs.radius / r[k];
+            u[k] = q[k] * eps;
+            w[k] = q[k] * q[k];
+            C1[k] = x[k] / r[k];
+            S1[k] = y[k] / r[k];
+            Cm[k] = 1.0;
+            Sm[k] = 0.0;
+            Cp[k] = 0.0;
+            Sp[k] = 0.0;
+            qm[k] = 1.0;
+            G[k] = H[k] = J[k] = KK[k] = 0.0;
+        }
+        uf = make_float2((float)u[0], (float)u[1]);
+        wf = make_float2((float)w[0], (float)w[1]);
+    }
+    // eq. 4-11 for column m in FP64, then the cos/sin(m lambda) and q^m recursions step on
+    __device__ __forceinline__ void combine64(int m, const ColSums64<K>& s)
+    {
+        const double dm = (double)m;
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            G[k] += Cm[k] * s.g1[k] + Sm[k] * s.g2[k];
+            J[k] += dm * (Cp[k] * s.j1[k] + Sp[k] * s.j2[k]);
+            KK[k] -= dm * (Sp[k] * s.j1[k] - Cp[k] * s.j2[k]);
+            H[k] += Cp[k] * s.h1[k] + Sp[k] * s.h2[k];
+            Cp[k] = Cm[k];
+            Sp[k] = Sm[k];
+            const double Cn = C1[k] * Cm[k] - S1[k] * Sm[k];
+            const double Sn = S1[k] * Cm[k] + C1[k] * Sm[k];
+            Cm[k] = Cn;
+            Sm[k] = Sn;
+            qm[k] *= q[k];
+        }
+    }
+    // columns m .. m + C - 1 (<= 8): FP64 terms n <= 8 of each, then the FP32 terms 9..L of all
+    // of them side by side (L - 8 terms each), then the combinations in order
+    template <int C> __device__ __forceinline__ void head_group(int m)
+    {
+        ColSums64<K> s[C];
+        ColSums32<K> f[C];
+        float2 Q1f[C], Q2f[C];
+        const GravEntry32* e[C];
+        double qs[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+            qs[k] = qm[k];
+        double Q1[C][K], Q2[C][K];
+        const GravEntry64* e64[C];
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            if (c > 0) {
+#pragma unroll
+                for (int k = 0; k < K; ++k)
+                    qs[k] = qs[k] * q[k]; // the value combine64 gives qm at column m + c
+            }
+            s[c].zero();
+            f[c].zero();
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                Q1[c][k] = qs[k];
+                Q2[c][k] = 0.0;
+            }
+            e64[c] = gs.t64 + grav_col_offset(m + c, kMixedSplit);
+            s[c].add(e64[c], Q1[c]);
+            e[c] = gs.t32 + grav_col_offset(m + c, gs.Lt) + (kMixedSplit + 1 - m - c);
+        }
+        if constexpr (C == 2) { // FP64 terms of both columns side by side; column m has one more
+            column64_pair<K>(e64[0] + 1, e64[1] + 1, kMixedSplit - m - 1, u, w, Q1[0], Q2[0], s[0],
+                Q1[1], Q2[1], s[1]);
+            column64<K>(e64[0], kMixedSplit - m, kMixedSplit - m, u, w, Q1[0], Q2[0], s[0]);
+        } else {
+#pragma unroll
+            for (int c = 0; c < C; ++c)
+                column64<K>(e64[c], 1, kMixedSplit - m - c, u, w, Q1[c], Q2[c], s[c]);
+        }
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            Q1f[c] = make_float2((float)Q1[c][0], (float)Q1[c][1]);
+            Q2f[c] = make_float2((float)Q2[c][0], (float)Q2[c][1]);
+        }
+        if constexpr (C == 1)
+            column32x2(e[0], 0, L - kMixedSplit - 1, uf, wf, Q1f[0], Q2f[0], f[0]);
+        else
+            column32x2_group<C>(e, L - kMixedSplit, uf, wf, Q1f, Q2f, f);
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                s[c].g1[k] += (double)f[c].g[k].x;
+                s[c].g2[k] += (double)f[c].g[k].y;
+                s[c].j1[k] += (double)f[c].j[k].x;
+                s[c].j2[k] += (double)f[c].j[k].y;
+                s[c].h1[k] += (double)f[c].h[k].x;
+                s[c].h2[k] += (double)f[c].h[k].y;
+            }
+            combine64(m + c, s[c]);
+        }
+    }
+    // FP32 state of the columns m > 8 from the FP64 recursions after column 8
+    __device__ __forceinline__ void to_tail()
+    {
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            cf[k] = (float)Cm[k];
+            sf[k] = (float)Sm[k];
+            cpf[k] = (float)Cp[k];
+            spf[k] = (float)Sp[k];
+            qmf[k] = (float)qm[k];
+            c1f[k] = (float)C1[k];
+            s1f[k] = (float)S1[k];
+            qf[k] = (float)q[k];
+            Gf[k] = Hf[k] = Jf[k] = Kf[k] = 0.f;
+        }
+    }
+    __device__ __forceinline__ void combine32(int m, const ColSums32<K>& f)
+    {
+        const float dm = (float)m;
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            Gf[k] += cf[k] * f.g[k].x + sf[k] * f.g[k].y;
+            Jf[k] += dm * (cpf[k] * f.j[k].x + spf[k] * f.j[k].y);
+            Kf[k] -= dm * (spf[k] * f.j[k].x - cpf[k] * f.j[k].y);
+            Hf[k] += cpf[k] * f.h[k].x + spf[k] * f.h[k].y;
+            cpf[k] = cf[k];
+            spf[k] = sf[k];
+            const float cn = c1f[k] * cf[k] - s1f[k] * sf[k];
+            const float sn = s1f[k] * cf[k] + c1f[k] * sf[k];
+            cf[k] = cn;
+            sf[k] = sn;
+            qmf[k] *= qf[k];
+        }
+    }
+    // columns m .. m + C - 1 (> 8, m + C - 1 <= L) in FP32: the n = m term (Q = q^m) of each, the
+    // L - m - C + 1 terms all of them have left side by side, the remaining terms of the longer
+    // columns one column at a time, then the combinations in order
+    template <int C> __device__ __forceinline__ void tail_group(int m)
+    {
+        ColSums32<K> f[C];
+        float2 Q1f[C], Q2f[C];
+        const GravEntry32* e[C];
+        float qs[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+            qs[k] = qmf[k];
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            if (c > 0) {
+#pragma unroll
+                for (int k = 0; k < K; ++k)
+                    qs[k] = qs[k] * qf[k]; // the value combine32 gives qmf at column m + c
+            }
+            const GravEntry32* base = gs.t32 + grav_col_offset(m + c, gs.Lt);
+            const float4* p = reinterpret_cast<const float4*>(base);
+            const float4 a = p[0], b = p[1];
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                const float2 QQ = make_float2(qs[k], qs[k]);
+                f[c].g[k] = __fmul2_rn(QQ, make_float2(a.z, a.w));
+                f[c].j[k] = __fmul2_rn(QQ, make_float2(b.x, b.y));
+                f[c].h[k] = __fmul2_rn(QQ, make_float2(b.z, b.w));
+            }
+            Q1f[c] = make_float2(qs[0], qs[1]);
+            Q2f[c] = make_float2(0.f, 0.f);
+            e[c] = base + 1;
+        }
+        const int N = L - m - (C - 1);
+        if constexpr (C > 1) {
+            column32x2_group<C>(e, N, uf, wf, Q1f, Q2f, f);
+            if constexpr (C == 2) {
+                last_term32x2(e[0] + N, uf, wf, Q1f[0], Q2f[0], f[0]); // column m: one term more
+            } else {
+#pragma unroll
+                for (int c = 0; c + 1 < C; ++c) // column m + c has C - 1 - c terms more
+                    column32x2(e[c] - 1, N + 1, L - m - c, uf, wf, Q1f[c], Q2f[c], f[c]);
+            }
+        } else {
+            column32x2(e[0] - 1, 1, L - m, uf, wf, Q1f[0], Q2f[0], f[0]);
+        }
+#pragma unroll
+        for (int c = 0; c < C; ++c)
+            combine32(m + c, f[c]);
+    }
+};
+
+#ifndef GPOP_HEAD_GROUP
+#define GPOP_HEAD_GROUP 2
+#endif
+#ifndef GPOP_TAIL_GROUP
+#define GPOP_TAIL_GROUP 2
+#endif
+constexpr int kHeadGroup = GPOP_HEAD_GROUP;
+
+constexpr int kTailGroup = GPOP_TAIL_GROUP;
+
+__device__ __forceinline__ void gravity_itrs_groups(const GravSmem& gs, const double (&x)[2],
+    const double (&y)[2], const double (&z)[2], double (&ax)[2], double (&ay)[2], double (&az)[2])
+{
+    constexpr int K = 2;
+    double r[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+        r[k] = sqrt(x[k] * x[k] + y[k] * y[k] + z[k] * z[k]);
+    MixedWalk2 W(gs, r, x, y, z);
+    const int L = gs.L;
+    int m = 0;
+#pragma unroll 1
+    for (; m + kHeadGroup - 1 <= kMixedSplit; m += kHeadGroup)
+        W.head_group<kHeadGroup>(m);
+    if constexpr (kHeadGroup > 1) { // 9 head columns: what the groups left
+        constexpr int rest = (kMixedSplit + 1) % kHeadGroup;
+        if constexpr (rest > 0)
+            W.head_group<rest>(m);
+    }
+    W.to_tail();
+    m = kMixedSplit + 1;
+#pragma unroll 1
+    for (; m + kTailGroup - 1 <= L; m += kTailGroup)
+        W.tail_group<kTailGroup>(m);
+    if constexpr (kTailGroup > 2) {
+        if (m + 1 <= L) {
+            W.tail_group<2>(m);
+            m += 2;
+        }
+    }
+    if constexpr (kTailGroup > 1) {
+        if (m <= L)
+            W.tail_group<1>(m);
+    }
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        W.G[k] += (double)W.Gf[k];
+        W.H[k] += (double)W.Hf[k];
+        W.J[k] += (double)W.Jf[k];
+        W.KK[k] += (double)W.Kf[k];
+    }
+#pragma unroll
+    for (int k = 0; k < K; ++k) { // eq. 4-13
+        const double Gk = W.G[k] + 1.0;
+        const double Lambda = Gk + z[k] * W.H[k] / r[k];
+        const double c = -gs.gm / (r[k] * r[k]);
+        ax[k] = c * (Lambda * x[k] / r[k] - W.J[k]);
+        ay[k] = c * (Lambda * y[k] / r[k] - W.KK[k]);
+        az[k] = c * (Lambda * z[k] / r[k] - W.H[k]);
+    }
+}
+
 // Accelerations of K objects in the Earth-fixed frame (eq. 4-13 of gravity_source_device.cu:212-239).
 template <bool MIXED, int K>
 __device__ __forceinline__ void gravity_itrs(const GravSmem& gs, const double (&x)[K],
     const double (&y)[K], const double (&z)[K], double (&ax)[K], double (&ay)[K], double (&az)[K])
 {
+    if constexpr (MIXED && K == 2 && kPairColumns) {
+        if (gs.L > kMixedSplit) {
+            gravity_itrs_groups(gs, x, y, z, ax, ay, az);
+            return;
+        }
+    }
     const int L = gs.L;
     double r[K], q[K], u[K], w[K], C1[K], S1[K], Cm[K], Sm[K], Cp[K], Sp[K], qm[K];
     double G[K], H[K], J[K], KK[K];
@@ -208,6 +591,56 @@ __device__ __forceinline__ void gravity_itrs(const GravSmem& gs, const double (&
     }
     // Mixed mode: columns m <= 8 are combined in FP64 below; the columns m > 8 (every term of
     // degree > 8) are walked, combined and summed in FP32 after this loop.
+    if constexpr (!MIXED && K == 2 && kPairColumns64) {
+        // FP64, two objects: columns (0, 1), (2, 3), ... walked side by side, each combined in
+        // order as below (bit-identical)
+        auto combine = [&](int m, const ColSums64<K>& s) {
+            const double dm = (double)m;
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                G[k] += Cm[k] * s.g1[k] + Sm[k] * s.g2[k];
+                J[k] += dm * (Cp[k] * s.j1[k] + Sp[k] * s.j2[k]);
+                KK[k] -= dm * (Sp[k] * s.j1[k] - Cp[k] * s.j2[k]);
+                H[k] += Cp[k] * s.h1[k] + Sp[k] * s.h2[k];
+                Cp[k] = Cm[k];
+                Sp[k] = Sm[k];
+                const double Cn = C1[k] * Cm[k] - S1[k] * Sm[k];
+                const double Sn = S1[k] * Cm[k] + C1[k] * Sm[k];
+                Cm[k] = Cn;
+                Sm[k] = Sn;
+                qm[k] *= q[k];
+            }
+        };
+#pragma unroll 1
+        for (int m = 0; m <= L; m += 2) {
+            ColSums64<K> sa, sb;
+            double Qa1[K], Qa2[K], Qb1[K], Qb2[K];
+            sa.zero();
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                Qa1[k] = qm[k];
+                Qa2[k] = 0.0;
+            }
+            const GravEntry64* ea = gs.t64 + grav_col_offset(m, gs.Lt);
+            sa.add(ea, Qa1);
+            if (m < L) {
+                sb.zero();
+#pragma unroll
+                for (int k = 0; k < K; ++k) {
+                    Qb1[k] = qm[k] * q[k];
+                    Qb2[k] = 0.0;
+                }
+                const GravEntry64* eb = gs.t64 + grav_col_offset(m + 1, gs.Lt);
+                sb.add(eb, Qb1);
+                column64_pair<K>(ea + 1, eb + 1, L - m - 1, u, w, Qa1, Qa2, sa, Qb1, Qb2, sb);
+                column64<K>(ea, L - m, L - m, u, w, Qa1, Qa2, sa);
+                combine(m, sa);
+                combine(m + 1, sb);
+            } else {
+                combine(m, sa);
+            }
+        }
+    } else {
     const int Lhead = (MIXED && L > kMixedSplit) ? kMixedSplit : L;
     for (int m = 0; m <= Lhead; ++m) {
         ColSums64<K> s;
@@ -280,6 +713,7 @@ __device__ __forceinline__ void gravity_itrs(const GravSmem& gs, const double (&
             Sm[k] = Sn;
             qm[k] *= q[k];
         }
+    }
     }
     if constexpr (MIXED) {
         if (L > kMixedSplit) {
