@@ -58,6 +58,11 @@ constexpr int kColGroupUnroll = GPOP_COLGROUP_UNROLL;
 constexpr bool kPairColumns = GPOP_PAIR_COLUMNS != 0;
 constexpr bool kPairColumns64 = GPOP_PAIR_COLUMNS64 != 0;
 constexpr int kCol64PairUnroll = GPOP_COL64PAIR_UNROLL;
+// the FP32 group walk runs its last N mod U terms in blocks of two (mixed 139.4 -> 140.5 M)
+#ifndef GPOP_BLOCK_REMAINDER
+#define GPOP_BLOCK_REMAINDER 1
+#endif
+constexpr bool kBlockRemainder = GPOP_BLOCK_REMAINDER != 0;
 
 struct GravSmem {
     const GravEntry64* t64; // FP64 mode: full table; mixed mode: head table (n <= 8)
@@ -281,11 +286,36 @@ __device__ __forceinline__ void column32x2_group(const GravEntry32* const (&e)[C
 #pragma unroll
     for (int c = 0; c < C; ++c)
         t[c] = first_t2(e[c], w, Q2[c]);
-#pragma unroll(C == 2 ? kColPairUnroll : kColGroupUnroll)
-    for (int i = 0; i < N; ++i)
+    if constexpr (kBlockRemainder) {
+        // blocks of U terms, then blocks of 2, then at most one term: every block is straight-line
+        // code whose loads can all be issued before its first term
+        constexpr int U = C == 2 ? kColPairUnroll : kColGroupUnroll;
+        int i = 0;
+#pragma unroll 1
+        for (; i + U <= N; i += U)
 #pragma unroll
-        for (int c = 0; c < C; ++c)
-            term32x2(e[c] + i, u, w, Q1[c], Q2[c], t[c], s[c]);
+            for (int j = 0; j < U; ++j)
+#pragma unroll
+                for (int c = 0; c < C; ++c)
+                    term32x2(e[c] + i + j, u, w, Q1[c], Q2[c], t[c], s[c]);
+#pragma unroll 1
+        for (; i + 2 <= N; i += 2)
+#pragma unroll
+            for (int j = 0; j < 2; ++j)
+#pragma unroll
+                for (int c = 0; c < C; ++c)
+                    term32x2(e[c] + i + j, u, w, Q1[c], Q2[c], t[c], s[c]);
+        if (i < N)
+#pragma unroll
+            for (int c = 0; c < C; ++c)
+                term32x2(e[c] + i, u, w, Q1[c], Q2[c], t[c], s[c]);
+    } else {
+#pragma unroll(C == 2 ? kColPairUnroll : kColGroupUnroll)
+        for (int i = 0; i < N; ++i)
+#pragma unroll
+            for (int c = 0; c < C; ++c)
+                term32x2(e[c] + i, u, w, Q1[c], Q2[c], t[c], s[c]);
+    }
 }
 
 // Mixed precision, two objects, degree L > 8: the walk of gravity_itrs<true, 2> with the FP32
@@ -503,6 +533,7 @@ struct MixedWalk2 {
 constexpr int kHeadGroup = GPOP_HEAD_GROUP;
 
 constexpr int kTailGroup = GPOP_TAIL_GROUP;
+
 
 __device__ __forceinline__ void gravity_itrs_groups(const GravSmem& gs, const double (&x)[2],
     const double (&y)[2], const double (&z)[2], double (&ax)[2], double (&ay)[2], double (&az)[2])
