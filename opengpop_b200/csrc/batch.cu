@@ -89,12 +89,29 @@ __global__ void __launch_bounds__(256) batch_startup_kernel(TableSrc ts, BatchAr
     }
 }
 
+// Two objects per lane may walk the gravity columns two at a time (as gj8_kernel does), in
+// batches whose items all have one lane per object (BatchArgs::pair_walk).
+#ifndef GPOP_BATCH_PAIRS
+#define GPOP_BATCH_PAIRS 1
+#endif
+constexpr bool kBatchPairs = GPOP_BATCH_PAIRS != 0;
+// Two-object items park the corrector's constants (s1, s2, prev, a7: 12 doubles per object) in
+// shared memory while the gravity walk runs, as gj8_kernel does, when that fits beside the table.
+#ifndef GPOP_BATCH_STAGE
+#define GPOP_BATCH_STAGE 1
+#endif
+constexpr bool kBatchStage = GPOP_BATCH_STAGE != 0;
+constexpr int kBatchStageDoubles = 24; // two objects x 12
+
 // One work item on one warp: K = 2 objects per lane for single-lane items (up to 64 objects),
 // else one object per group of P lanes (up to 32 / P objects).
-template <bool MIXED, int K>
+template <bool MIXED, int K, bool STAGE, bool PAIRS>
 __device__ __forceinline__ void run_item(const GravSmem& g0, const BatchArgs& a, const BatchItem& it,
-    const BatchReq& rq, int lane)
+    const BatchReq& rq, int lane, double* stage)
 {
+    constexpr bool kStage = K == 2 && STAGE;
+    // staged value q (0..3: s1, s2, prev, a7) of object k, axis j
+    auto slot = [&](int q, int k, int j) { return stage + (size_t)((q * K + k) * 3 + j) * blockDim.x; };
     const int64_t n = a.n_obj;
     double* st = a.state;
     const int P = K == 1 ? rq.lpo : 1;
@@ -166,15 +183,36 @@ __device__ __forceinline__ void run_item(const GravSmem& g0, const BatchArgs& a,
                 s2[k][j] = c2;
                 prev[k][j] = s[k][j];
                 a7[k][j] = hist[8][j];
+                if constexpr (kStage) {
+                    st_stage(slot(0, k, j), s1[k][j]);
+                    st_stage(slot(1, k, j), s2[k][j]);
+                    st_stage(slot(2, k, j), prev[k][j]);
+                    st_stage(slot(3, k, j), a7[k][j]);
+                }
             }
         }
         const double* M = rq.prop_m + (size_t)(step + 4) * 9;
         for (int itc = 0; itc < a.ncorr; ++itc) {
-            gravity_gcrs_lk<MIXED, K>(g, sl, P, M, r, a8, 0xffffffffu);
+            if constexpr (K == 2 && PAIRS) {
+                // two objects per lane: the two-column walk on the lane-layout tables (mixed
+                // needs degree > 8 for it)
+                if (!MIXED || g.L > kMixedSplit)
+                    gravity_gcrs<MIXED, 2, true>(g, M, r, a8);
+                else
+                    gravity_gcrs_lk<MIXED, K>(g, sl, P, M, r, a8, 0xffffffffu);
+            } else {
+                gravity_gcrs_lk<MIXED, K>(g, sl, P, M, r, a8, 0xffffffffu);
+            }
 #pragma unroll
             for (int k = 0; k < K; ++k)
 #pragma unroll
                 for (int j = 0; j < 3; ++j) {
+                    if constexpr (kStage) {
+                        s1[k][j] = ld_stage(slot(0, k, j));
+                        s2[k][j] = ld_stage(slot(1, k, j));
+                        prev[k][j] = ld_stage(slot(2, k, j));
+                        a7[k][j] = ld_stage(slot(3, k, j));
+                    }
                     s[k][j] = prev[k][j] + (a8[k][j] + a7[k][j]) / 2;
                     v[k][j] = h * (s1[k][j] + a8[k][j] * c_SA[8][8] + s[k][j]);
                     r[k][j] = h * h * (s2[k][j] + a8[k][j] * c_GJ[8][8] + S[k][j]);
@@ -202,7 +240,7 @@ __device__ __forceinline__ void run_item(const GravSmem& g0, const BatchArgs& a,
 
 // Persistent GJ8 kernel: warps pull work items until the queue is empty. One 256-thread block per
 // SM: the two-object path needs the registers of 8 warps.
-template <bool MIXED>
+template <bool MIXED, bool STAGE, bool PAIRS>
 __global__ void __launch_bounds__(256, 1) batch_gj8_kernel(TableSrc ts, BatchArgs a)
 {
     extern __shared__ __align__(128) uint8_t smem[];
@@ -210,6 +248,7 @@ __global__ void __launch_bounds__(256, 1) batch_gj8_kernel(TableSrc ts, BatchArg
     if (!bind_lane_table(smem, ts, a.err, g0))
         return;
     const int lane = threadIdx.x & 31;
+    double* stage = reinterpret_cast<double*>(smem + stage_offset(ts)) + threadIdx.x;
     for (;;) {
         int item = 0;
         if (lane == 0)
@@ -220,9 +259,9 @@ __global__ void __launch_bounds__(256, 1) batch_gj8_kernel(TableSrc ts, BatchArg
         const BatchItem it = a.items[item];
         const BatchReq rq = a.reqs[it.req];
         if (rq.lpo == 1)
-            run_item<MIXED, 2>(g0, a, it, rq, lane);
+            run_item<MIXED, 2, STAGE, PAIRS>(g0, a, it, rq, lane, stage);
         else
-            run_item<MIXED, 1>(g0, a, it, rq, lane);
+            run_item<MIXED, 1, false, false>(g0, a, it, rq, lane, stage);
     }
 }
 
@@ -250,22 +289,38 @@ cudaError_t launch_batch_startup(const TableSrc& ts, const BatchArgs& a, int num
     return cudaGetLastError();
 }
 
+template <bool MIXED, bool STAGE, bool PAIRS>
+static cudaError_t launch_batch_gj8_k(const TableSrc& ts, const BatchArgs& a, int blocks, int block,
+    size_t smem, cudaStream_t s)
+{
+    cudaError_t e = set_smem(batch_gj8_kernel<MIXED, STAGE, PAIRS>, smem);
+    if (e != cudaSuccess)
+        return e;
+    batch_gj8_kernel<MIXED, STAGE, PAIRS><<<blocks, block, smem, s>>>(ts, a);
+    return cudaGetLastError();
+}
+
+template <bool MIXED>
+static cudaError_t launch_batch_gj8_m(const TableSrc& ts, const BatchArgs& a, int blocks, int block,
+    cudaStream_t s)
+{
+    const size_t staged = stage_offset(ts) + (size_t)kBatchStageDoubles * 8 * block;
+    const bool stage = kBatchStage && staged <= max_smem_optin();
+    const bool pairs = kBatchPairs && a.pair_walk;
+    const size_t smem = stage ? staged : table_smem_bytes(ts);
+    if (stage)
+        return pairs ? launch_batch_gj8_k<MIXED, true, true>(ts, a, blocks, block, smem, s)
+                     : launch_batch_gj8_k<MIXED, true, false>(ts, a, blocks, block, smem, s);
+    return pairs ? launch_batch_gj8_k<MIXED, false, true>(ts, a, blocks, block, smem, s)
+                 : launch_batch_gj8_k<MIXED, false, false>(ts, a, blocks, block, smem, s);
+}
+
 cudaError_t launch_batch_gj8(const TableSrc& ts, const BatchArgs& a, int blocks, int block, cudaStream_t s)
 {
     if (a.n_items <= 0)
         return cudaSuccess;
-    const size_t smem = table_smem_bytes(ts);
-    cudaError_t e;
-    if (ts.mixed) {
-        if ((e = set_smem(batch_gj8_kernel<true>, smem)) != cudaSuccess)
-            return e;
-        batch_gj8_kernel<true><<<blocks, block, smem, s>>>(ts, a);
-    } else {
-        if ((e = set_smem(batch_gj8_kernel<false>, smem)) != cudaSuccess)
-            return e;
-        batch_gj8_kernel<false><<<blocks, block, smem, s>>>(ts, a);
-    }
-    return cudaGetLastError();
+    return ts.mixed ? launch_batch_gj8_m<true>(ts, a, blocks, block, s)
+                    : launch_batch_gj8_m<false>(ts, a, blocks, block, s);
 }
 
 // ---- epoch tables of many requests: epoch e uses calendar cal[5 * epoch_req[e]] ----

@@ -47,6 +47,7 @@ struct BatchArgs {
     double* v_out = nullptr;
     unsigned* err = nullptr;
     int Ltab = 0; // degree of the staged table layout
+    bool pair_walk = false; // two-object items walk two gravity columns at a time
 };
 
 cudaError_t launch_batch_startup(const TableSrc& ts, const BatchArgs& a, int num_sms, cudaStream_t s);

@@ -298,8 +298,17 @@ gpop_status gpop_propagate_batch(gpop_ctx* ctx, const gpop_request* reqs, int32_
         t_off[t] = E;
         E += 80 + table_len[t];
     }
+    // Two-object items walk the gravity columns two at a time only in batches that hold nothing
+    // else: beside many-lane items the larger kernel code slows the many-lane items (4,096 uneven
+    // requests: 174 -> 165 M object-steps/s), while a batch of 64-object items gains (one
+    // 65,536-object 70x70 request: mixed 97 -> 115 M). The autotuner's fixed-lane runs keep the
+    // one-column walk, so its single-lane figures hold for uneven batches.
+    bool pair_walk = ctx->force_lpo == 0;
+    for (int i = 0; i < n_req; ++i)
+        pair_walk = pair_walk && plan.lpo[i] == 1;
     // shape signature: the graph is replayed only for an identical plan and layout
-    std::vector<int64_t> sig { (int64_t)ctx->cfg.precision, (int64_t)ctx->cfg.flags, N, E, (int64_t)n_req };
+    std::vector<int64_t> sig { (int64_t)ctx->cfg.precision, (int64_t)ctx->cfg.flags, N, E, (int64_t)n_req,
+        (int64_t)pair_walk };
     for (int i = 0; i < n_req; ++i) {
         sig.push_back(n[i]);
         sig.push_back(steps[i]);
@@ -437,6 +446,7 @@ gpop_status gpop_propagate_batch(gpop_ctx* ctx, const gpop_request* reqs, int32_
         a.v_out = dio + 9 * N;
         a.err = ctx->err_word.as<unsigned>();
         a.Ltab = ctx->md.degree;
+        a.pair_walk = pair_walk;
         cudaGraph_t graph = nullptr;
         if ((e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
             return cuda_fail(ctx, e, "graph capture");

@@ -73,4 +73,17 @@ __device__ __forceinline__ bool stage_to_smem(void* smem_dst, const void* gsrc, 
     return true;
 }
 
+// Stores and loads of per-thread values parked in shared memory across a long computation. The
+// asm keeps the compiler from forwarding the stored value (which would keep it in a register).
+__device__ __forceinline__ void st_stage(double* p, double v)
+{
+    asm volatile("st.shared.f64 [%0], %1;" ::"r"(smem_u32(p)), "d"(v) : "memory");
+}
+__device__ __forceinline__ double ld_stage(const double* p)
+{
+    double v;
+    asm volatile("ld.shared.f64 %0, [%1];" : "=d"(v) : "r"(smem_u32(p)) : "memory");
+    return v;
+}
+
 } // namespace gpop

@@ -74,6 +74,33 @@ struct GravSmem {
     const int* cb32 = nullptr; // lane layout: the same for the FP32 table
 };
 
+// Columns of the lane-layout tables (build_lane_blob): column m starts at 16-byte unit cb[m].
+__device__ __forceinline__ const GravEntry64* lane_col64(const GravSmem& g, int m)
+{
+    return reinterpret_cast<const GravEntry64*>(reinterpret_cast<const uint4*>(g.t64) + g.cb64[m]);
+}
+__device__ __forceinline__ const GravEntry32* lane_col32(const GravSmem& g, int m)
+{
+    return reinterpret_cast<const GravEntry32*>(reinterpret_cast<const uint4*>(g.t32) + g.cb32[m]);
+}
+// Column m of the FP64 table (degree Lt64: the full table, or the n <= 8 head in mixed mode) and of
+// the FP32 table, in the plain (LANE = false) or the lane layout.
+template <bool LANE>
+__device__ __forceinline__ const GravEntry64* col64(const GravSmem& g, int m, int Lt64)
+{
+    if constexpr (LANE)
+        return lane_col64(g, m);
+    else
+        return g.t64 + grav_col_offset(m, Lt64);
+}
+template <bool LANE> __device__ __forceinline__ const GravEntry32* col32(const GravSmem& g, int m)
+{
+    if constexpr (LANE)
+        return lane_col32(g, m);
+    else
+        return g.t32 + grav_col_offset(m, g.Lt);
+}
+
 template <int K> struct ColSums64 {
     double g1[K], g2[K], j1[K], j2[K], h1[K], h2[K];
     __device__ __forceinline__ void zero()
@@ -322,7 +349,7 @@ __device__ __forceinline__ void column32x2_group(const GravEntry32* const (&e)[C
 // parts of the columns taken kHeadGroup (columns m <= 8) or kTailGroup (m > 8) columns at a time.
 // Every column's sums, their combination and the order of the combinations are those of the
 // one-column walk, so the accelerations are bit-identical to it.
-struct MixedWalk2 {
+template <bool LANE> struct MixedWalk2 {
     static constexpr int K = 2;
     const GravSmem& gs;
     int L;
@@ -402,9 +429,9 @@ struct MixedWalk2 {
                 Q1[c][k] = qs[k];
                 Q2[c][k] = 0.0;
             }
-            e64[c] = gs.t64 + grav_col_offset(m + c, kMixedSplit);
+            e64[c] = col64<LANE>(gs, m + c, kMixedSplit);
             s[c].add(e64[c], Q1[c]);
-            e[c] = gs.t32 + grav_col_offset(m + c, gs.Lt) + (kMixedSplit + 1 - m - c);
+            e[c] = col32<LANE>(gs, m + c) + (kMixedSplit + 1 - m - c);
         }
         if constexpr (C == 2) { // FP64 terms of both columns side by side; column m has one more
             column64_pair<K>(e64[0] + 1, e64[1] + 1, kMixedSplit - m - 1, u, w, Q1[0], Q2[0], s[0],
@@ -491,7 +518,7 @@ struct MixedWalk2 {
                 for (int k = 0; k < K; ++k)
                     qs[k] = qs[k] * qf[k]; // the value combine32 gives qmf at column m + c
             }
-            const GravEntry32* base = gs.t32 + grav_col_offset(m + c, gs.Lt);
+            const GravEntry32* base = col32<LANE>(gs, m + c);
             const float4* p = reinterpret_cast<const float4*>(base);
             const float4 a = p[0], b = p[1];
 #pragma unroll
@@ -535,6 +562,7 @@ constexpr int kHeadGroup = GPOP_HEAD_GROUP;
 constexpr int kTailGroup = GPOP_TAIL_GROUP;
 
 
+template <bool LANE>
 __device__ __forceinline__ void gravity_itrs_groups(const GravSmem& gs, const double (&x)[2],
     const double (&y)[2], const double (&z)[2], double (&ax)[2], double (&ay)[2], double (&az)[2])
 {
@@ -543,31 +571,31 @@ __device__ __forceinline__ void gravity_itrs_groups(const GravSmem& gs, const do
 #pragma unroll
     for (int k = 0; k < K; ++k)
         r[k] = sqrt(x[k] * x[k] + y[k] * y[k] + z[k] * z[k]);
-    MixedWalk2 W(gs, r, x, y, z);
+    MixedWalk2<LANE> W(gs, r, x, y, z);
     const int L = gs.L;
     int m = 0;
 #pragma unroll 1
     for (; m + kHeadGroup - 1 <= kMixedSplit; m += kHeadGroup)
-        W.head_group<kHeadGroup>(m);
+        W.template head_group<kHeadGroup>(m);
     if constexpr (kHeadGroup > 1) { // 9 head columns: what the groups left
         constexpr int rest = (kMixedSplit + 1) % kHeadGroup;
         if constexpr (rest > 0)
-            W.head_group<rest>(m);
+            W.template head_group<rest>(m);
     }
     W.to_tail();
     m = kMixedSplit + 1;
 #pragma unroll 1
     for (; m + kTailGroup - 1 <= L; m += kTailGroup)
-        W.tail_group<kTailGroup>(m);
+        W.template tail_group<kTailGroup>(m);
     if constexpr (kTailGroup > 2) {
         if (m + 1 <= L) {
-            W.tail_group<2>(m);
+            W.template tail_group<2>(m);
             m += 2;
         }
     }
     if constexpr (kTailGroup > 1) {
         if (m <= L)
-            W.tail_group<1>(m);
+            W.template tail_group<1>(m);
     }
 #pragma unroll
     for (int k = 0; k < K; ++k) {
@@ -587,6 +615,89 @@ __device__ __forceinline__ void gravity_itrs_groups(const GravSmem& gs, const do
     }
 }
 
+// FP64, two objects: columns (0, 1), (2, 3), ... walked side by side, each combined in order as
+// the one-column walk does (bit-identical accelerations).
+template <bool LANE>
+__device__ __forceinline__ void gravity_itrs_pairs64(const GravSmem& gs, const double (&x)[2],
+    const double (&y)[2], const double (&z)[2], double (&ax)[2], double (&ay)[2], double (&az)[2])
+{
+    constexpr int K = 2;
+    const int L = gs.L;
+    double r[K], q[K], u[K], w[K], C1[K], S1[K], Cm[K], Sm[K], Cp[K], Sp[K], qm[K];
+    double G[K], H[K], J[K], KK[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        r[k] = sqrt(x[k] * x[k] + y[k] * y[k] + z[k] * z[k]);
+        const double eps = z[k] / r[k];
+        q[k] = gs.radius / r[k];
+        u[k] = q[k] * eps;
+        w[k] = q[k] * q[k];
+        C1[k] = x[k] / r[k];
+        S1[k] = y[k] / r[k];
+        Cm[k] = 1.0;
+        Sm[k] = 0.0;
+        Cp[k] = 0.0;
+        Sp[k] = 0.0;
+        qm[k] = 1.0;
+        G[k] = H[k] = J[k] = KK[k] = 0.0;
+    }
+    auto combine = [&](int m, const ColSums64<K>& s) {
+        const double dm = (double)m;
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            G[k] += Cm[k] * s.g1[k] + Sm[k] * s.g2[k];
+            J[k] += dm * (Cp[k] * s.j1[k] + Sp[k] * s.j2[k]);
+            KK[k] -= dm * (Sp[k] * s.j1[k] - Cp[k] * s.j2[k]);
+            H[k] += Cp[k] * s.h1[k] + Sp[k] * s.h2[k];
+            Cp[k] = Cm[k];
+            Sp[k] = Sm[k];
+            const double Cn = C1[k] * Cm[k] - S1[k] * Sm[k];
+            const double Sn = S1[k] * Cm[k] + C1[k] * Sm[k];
+            Cm[k] = Cn;
+            Sm[k] = Sn;
+            qm[k] *= q[k];
+        }
+    };
+#pragma unroll 1
+    for (int m = 0; m <= L; m += 2) {
+        ColSums64<K> sa, sb;
+        double Qa1[K], Qa2[K], Qb1[K], Qb2[K];
+        sa.zero();
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            Qa1[k] = qm[k];
+            Qa2[k] = 0.0;
+        }
+        const GravEntry64* ea = col64<LANE>(gs, m, gs.Lt);
+        sa.add(ea, Qa1);
+        if (m < L) {
+            sb.zero();
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                Qb1[k] = qm[k] * q[k];
+                Qb2[k] = 0.0;
+            }
+            const GravEntry64* eb = col64<LANE>(gs, m + 1, gs.Lt);
+            sb.add(eb, Qb1);
+            column64_pair<K>(ea + 1, eb + 1, L - m - 1, u, w, Qa1, Qa2, sa, Qb1, Qb2, sb);
+            column64<K>(ea, L - m, L - m, u, w, Qa1, Qa2, sa);
+            combine(m, sa);
+            combine(m + 1, sb);
+        } else {
+            combine(m, sa);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < K; ++k) { // eq. 4-13
+        const double Gk = G[k] + 1.0;
+        const double Lambda = Gk + z[k] * H[k] / r[k];
+        const double c = -gs.gm / (r[k] * r[k]);
+        ax[k] = c * (Lambda * x[k] / r[k] - J[k]);
+        ay[k] = c * (Lambda * y[k] / r[k] - KK[k]);
+        az[k] = c * (Lambda * z[k] / r[k] - H[k]);
+    }
+}
+
 // Accelerations of K objects in the Earth-fixed frame (eq. 4-13 of gravity_source_device.cu:212-239).
 template <bool MIXED, int K>
 __device__ __forceinline__ void gravity_itrs(const GravSmem& gs, const double (&x)[K],
@@ -594,9 +705,13 @@ __device__ __forceinline__ void gravity_itrs(const GravSmem& gs, const double (&
 {
     if constexpr (MIXED && K == 2 && kPairColumns) {
         if (gs.L > kMixedSplit) {
-            gravity_itrs_groups(gs, x, y, z, ax, ay, az);
+            gravity_itrs_groups<false>(gs, x, y, z, ax, ay, az);
             return;
         }
+    }
+    if constexpr (!MIXED && K == 2 && kPairColumns64) {
+        gravity_itrs_pairs64<false>(gs, x, y, z, ax, ay, az);
+        return;
     }
     const int L = gs.L;
     double r[K], q[K], u[K], w[K], C1[K], S1[K], Cm[K], Sm[K], Cp[K], Sp[K], qm[K];
@@ -622,56 +737,6 @@ __device__ __forceinline__ void gravity_itrs(const GravSmem& gs, const double (&
     }
     // Mixed mode: columns m <= 8 are combined in FP64 below; the columns m > 8 (every term of
     // degree > 8) are walked, combined and summed in FP32 after this loop.
-    if constexpr (!MIXED && K == 2 && kPairColumns64) {
-        // FP64, two objects: columns (0, 1), (2, 3), ... walked side by side, each combined in
-        // order as below (bit-identical)
-        auto combine = [&](int m, const ColSums64<K>& s) {
-            const double dm = (double)m;
-#pragma unroll
-            for (int k = 0; k < K; ++k) {
-                G[k] += Cm[k] * s.g1[k] + Sm[k] * s.g2[k];
-                J[k] += dm * (Cp[k] * s.j1[k] + Sp[k] * s.j2[k]);
-                KK[k] -= dm * (Sp[k] * s.j1[k] - Cp[k] * s.j2[k]);
-                H[k] += Cp[k] * s.h1[k] + Sp[k] * s.h2[k];
-                Cp[k] = Cm[k];
-                Sp[k] = Sm[k];
-                const double Cn = C1[k] * Cm[k] - S1[k] * Sm[k];
-                const double Sn = S1[k] * Cm[k] + C1[k] * Sm[k];
-                Cm[k] = Cn;
-                Sm[k] = Sn;
-                qm[k] *= q[k];
-            }
-        };
-#pragma unroll 1
-        for (int m = 0; m <= L; m += 2) {
-            ColSums64<K> sa, sb;
-            double Qa1[K], Qa2[K], Qb1[K], Qb2[K];
-            sa.zero();
-#pragma unroll
-            for (int k = 0; k < K; ++k) {
-                Qa1[k] = qm[k];
-                Qa2[k] = 0.0;
-            }
-            const GravEntry64* ea = gs.t64 + grav_col_offset(m, gs.Lt);
-            sa.add(ea, Qa1);
-            if (m < L) {
-                sb.zero();
-#pragma unroll
-                for (int k = 0; k < K; ++k) {
-                    Qb1[k] = qm[k] * q[k];
-                    Qb2[k] = 0.0;
-                }
-                const GravEntry64* eb = gs.t64 + grav_col_offset(m + 1, gs.Lt);
-                sb.add(eb, Qb1);
-                column64_pair<K>(ea + 1, eb + 1, L - m - 1, u, w, Qa1, Qa2, sa, Qb1, Qb2, sb);
-                column64<K>(ea, L - m, L - m, u, w, Qa1, Qa2, sa);
-                combine(m, sa);
-                combine(m + 1, sb);
-            } else {
-                combine(m, sa);
-            }
-        }
-    } else {
     const int Lhead = (MIXED && L > kMixedSplit) ? kMixedSplit : L;
     for (int m = 0; m <= Lhead; ++m) {
         ColSums64<K> s;
@@ -744,7 +809,6 @@ __device__ __forceinline__ void gravity_itrs(const GravSmem& gs, const double (&
             Sm[k] = Sn;
             qm[k] *= q[k];
         }
-    }
     }
     if constexpr (MIXED) {
         if (L > kMixedSplit) {
@@ -821,7 +885,9 @@ __device__ __forceinline__ void gravity_itrs(const GravSmem& gs, const double (&
 // GCRS accelerations of K objects at GCRS positions r[k] with the ITRS->GCRS matrix M
 // (column-major): r_itrs = M^T r, a = M a_itrs (the two cublasDgemvStridedBatched of
 // gravity_source.cu:176-210).
-template <bool MIXED, int K>
+// LANE: the tables are in the lane layout, two objects (K = 2) and, in mixed mode, L > 8; the
+// walk is then the two-column walk (the other cases have no plain-walk form in that layout).
+template <bool MIXED, int K, bool LANE = false>
 __device__ __forceinline__ void gravity_gcrs(const GravSmem& gs, const double* __restrict__ M,
     const double (&r)[K][3], double (&a)[K][3])
 {
@@ -836,7 +902,15 @@ __device__ __forceinline__ void gravity_gcrs(const GravSmem& gs, const double* _
         py[k] = m[3] * r[k][0] + m[4] * r[k][1] + m[5] * r[k][2];
         pz[k] = m[6] * r[k][0] + m[7] * r[k][1] + m[8] * r[k][2];
     }
-    gravity_itrs<MIXED, K>(gs, px, py, pz, ax, ay, az);
+    if constexpr (LANE) {
+        static_assert(K == 2, "the lane-layout two-column walk carries two objects");
+        if constexpr (MIXED)
+            gravity_itrs_groups<true>(gs, px, py, pz, ax, ay, az);
+        else
+            gravity_itrs_pairs64<true>(gs, px, py, pz, ax, ay, az);
+    } else {
+        gravity_itrs<MIXED, K>(gs, px, py, pz, ax, ay, az);
+    }
 #pragma unroll
     for (int k = 0; k < K; ++k) {
         a[k][0] = m[0] * ax[k] + m[3] * ay[k] + m[6] * az[k];

@@ -17,6 +17,13 @@ struct TableSrc {
     bool lanes = false; // lane layout (build_lane_blob): column bases, FP64 at kLaneOff64, FP32 at off32
 };
 
+// Byte offset, in a kernel's dynamic shared memory, of what follows a staged table (the 128-byte
+// mbarrier slot and the table, rounded up to 16 bytes).
+inline __host__ __device__ size_t stage_offset(const TableSrc& ts)
+{
+    return (128 + (size_t)ts.bytes + 15) & ~(size_t)15;
+}
+
 // Per-object propagation state, SoA: array k (n doubles each) at state + k * n.
 enum StateSlot : int {
     kR = 0, kV = 3, kSs = 6, kSb = 9, kHist = 12, kRep = 39, kRepA = 63, kStateArrays = 75
@@ -53,6 +60,8 @@ struct LaunchShape {
 
 size_t table_smem_bytes(const TableSrc& ts);
 LaunchShape pick_shape(int64_t n, int max_block, int num_sms);
+// Dynamic shared memory one block of the current device may opt in to (0 if it cannot be read).
+size_t max_smem_optin();
 
 cudaError_t launch_startup(const TableSrc& ts, const PropArgs& a, int num_sms, cudaStream_t s);
 // How many objects a GJ8 thread carries through the gravity triangle walk (0 = by problem size).

@@ -11,16 +11,6 @@
 
 namespace gpop {
 
-// Columns of the lane-layout tables (build_lane_blob).
-__device__ __forceinline__ const GravEntry64* lane_col64(const GravSmem& g, int m)
-{
-    return reinterpret_cast<const GravEntry64*>(reinterpret_cast<const uint4*>(g.t64) + g.cb64[m]);
-}
-__device__ __forceinline__ const GravEntry32* lane_col32(const GravSmem& g, int m)
-{
-    return reinterpret_cast<const GravEntry32*>(reinterpret_cast<const uint4*>(g.t32) + g.cb32[m]);
-}
-
 // Stages a lane-layout blob into shared memory (after a 128-byte mbarrier slot) and binds it.
 __device__ __forceinline__ bool bind_lane_table(uint8_t* smem, const TableSrc& ts, unsigned* err, GravSmem& g)
 {

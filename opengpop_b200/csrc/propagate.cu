@@ -187,24 +187,12 @@ template <class F> constexpr bool stage_corrector()
     return F::kTable && (F::kMixed || GPOP_STAGE_FP64 != 0) && GPOP_STAGE_CORRECTOR != 0;
 }
 
-__device__ __forceinline__ void st_stage(double* p, double v)
-{
-    asm volatile("st.shared.f64 [%0], %1;" ::"r"(smem_u32(p)), "d"(v) : "memory");
-}
-__device__ __forceinline__ double ld_stage(const double* p)
-{
-    double v;
-    asm volatile("ld.shared.f64 %0, [%1];" : "=d"(v) : "r"(smem_u32(p)) : "memory");
-    return v;
-}
 
-__host__ __device__ inline size_t stage_offset(const TableSrc& ts) { return (128 + (size_t)ts.bytes + 15) & ~(size_t)15; }
-
-template <class F, int K>
+template <class F, int K, bool STAGE>
 __global__ void __launch_bounds__(K == 1 ? 512 : 256, 1) gj8_kernel(F f, TableSrc ts, PropArgs a)
 {
     extern __shared__ __align__(128) uint8_t smem[];
-    constexpr bool kStage = stage_corrector<F>();
+    constexpr bool kStage = STAGE && stage_corrector<F>();
     double* stage = nullptr;
     if constexpr (F::kTable) {
         if (!bind_table<std::is_same<F, ForceGravity<true>>::value>(smem, ts, a.err, f.g))
@@ -610,6 +598,15 @@ LaunchShape pick_shape(int64_t n, int max_block, int num_sms)
     return ls;
 }
 
+size_t max_smem_optin()
+{
+    int dev = 0, v = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess
+        || cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
+        return 0;
+    return (size_t)v;
+}
+
 template <class K> static cudaError_t set_smem(K kernel, size_t bytes)
 {
     return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
@@ -656,14 +653,24 @@ static cudaError_t launch_gj8_k(F f, const TableSrc& ts, const PropArgs& a, int 
         ls.block = block_override;
         ls.grid = (int)((threads + block_override - 1) / block_override);
     }
-    size_t smem = 0;
     if constexpr (F::kTable) {
-        smem = stage_offset(ts) + (stage_corrector<F>() ? (size_t)kStageDoubles * K * 8 * ls.block : 0);
-        cudaError_t e = set_smem(gj8_kernel<F, K>, smem);
-        if (e != cudaSuccess)
-            return e;
+        // the corrector state is parked in shared memory when it fits beside the table
+        const size_t staged = stage_offset(ts) + (size_t)kStageDoubles * K * 8 * ls.block;
+        if (stage_corrector<F>() && staged <= max_smem_optin()) {
+            cudaError_t e = set_smem(gj8_kernel<F, K, true>, staged);
+            if (e != cudaSuccess)
+                return e;
+            gj8_kernel<F, K, true><<<ls.grid, ls.block, staged, s>>>(f, ts, a);
+        } else {
+            const size_t smem = table_smem_bytes(ts);
+            cudaError_t e = set_smem(gj8_kernel<F, K, false>, smem);
+            if (e != cudaSuccess)
+                return e;
+            gj8_kernel<F, K, false><<<ls.grid, ls.block, smem, s>>>(f, ts, a);
+        }
+    } else {
+        gj8_kernel<F, K, false><<<ls.grid, ls.block, 0, s>>>(f, ts, a);
     }
-    gj8_kernel<F, K><<<ls.grid, ls.block, smem, s>>>(f, ts, a);
     return cudaGetLastError();
 }
 
@@ -689,16 +696,18 @@ cudaError_t launch_gj8(const TableSrc& ts, const PropArgs& a, int num_sms, cudaS
 {
     if (a.n <= 0 || a.step_end <= a.step_begin)
         return cudaSuccess;
-    // Default walk (measured on B200 at 70x70): two objects per thread from 320 objects per SM;
-    // from 128 to 320 objects per SM two lanes per pair of objects (mixed: 20,000 objects 52 ->
-    // 61 M object-steps/s, 37,000 94 -> 110 M; FP64 +4 %); below 128, 4 or more lanes per object
-    // (2.8x faster at 4,096 objects, 4.9x at 1,024 than one object per thread). One or two objects
-    // per thread when no lane-layout table is at hand.
+    // Default walk (measured on B200 at 70x70, LEO objects, mixed / FP64 M object-steps/s with the
+    // two-column walk): two objects per thread above 128 objects per SM (20,000 objects: 66.5 /
+    // 35.3 against 57.2 / 34.3 with two lanes per pair; 37,000: 120 / 64 against 104 / 62); two
+    // lanes per pair of objects from 112 to 128 per SM, where they fill the four schedulers with
+    // one warp each (18,944 objects: 67.7 / 41.2 against 63.3 / 33.6 with two objects per thread);
+    // below, 2 or more lanes per object (9,472 objects: 48.2 / 31.0 against 34.0 / 20.8). One or
+    // two objects per thread when no lane-layout table is at hand.
     if (walk <= 0) {
         const bool lanes = lane_ts && a.kind == 0;
-        if (a.n >= (int64_t)num_sms * 320 || (!lanes && a.n >= (int64_t)num_sms * 128))
+        if (a.n > (int64_t)num_sms * 128 || (!lanes && a.n >= (int64_t)num_sms * 128))
             walk = kWalkTwoObjects;
-        else if (a.n >= (int64_t)num_sms * 128)
+        else if (a.n >= (int64_t)num_sms * 112)
             walk = kWalkLanesTwo;
         else
             walk = lanes ? kWalkLanes : kWalkOneObject;
