@@ -175,6 +175,13 @@ __global__ void __launch_bounds__(256) startup_kernel(F f, TableSrc ts, PropArgs
 // object) and S wait in shared memory while the gravity walk runs, which leaves the walk the
 // registers they would hold (two objects, 65,536 objects at 70x70 on B200, with the paired column
 // walks: mixed 125.5 -> 131.5 M object-steps/s, FP64 72.3 -> 73.8 M).
+// Largest block of the one-object-per-thread kernel (its register budget is 65,536 / this; at 256
+// the FP64 two-column walk fits without spills).
+#ifndef GPOP_ONE_OBJECT_BLOCK
+#define GPOP_ONE_OBJECT_BLOCK 256
+#endif
+constexpr int kOneObjectBlock = GPOP_ONE_OBJECT_BLOCK;
+
 #ifndef GPOP_STAGE_CORRECTOR
 #define GPOP_STAGE_CORRECTOR 1
 #endif
@@ -189,7 +196,7 @@ template <class F> constexpr bool stage_corrector()
 
 
 template <class F, int K, bool STAGE>
-__global__ void __launch_bounds__(K == 1 ? 512 : 256, 1) gj8_kernel(F f, TableSrc ts, PropArgs a)
+__global__ void __launch_bounds__(K == 1 ? kOneObjectBlock : 256, 1) gj8_kernel(F f, TableSrc ts, PropArgs a)
 {
     extern __shared__ __align__(128) uint8_t smem[];
     constexpr bool kStage = STAGE && stage_corrector<F>();
@@ -648,7 +655,7 @@ static cudaError_t launch_gj8_k(F f, const TableSrc& ts, const PropArgs& a, int 
     cudaStream_t s, int block_override)
 {
     const int64_t threads = (a.n + K - 1) / K;
-    LaunchShape ls = pick_shape(threads, K == 1 ? 512 : 256, num_sms);
+    LaunchShape ls = pick_shape(threads, K == 1 ? kOneObjectBlock : 256, num_sms);
     if (block_override > 0) {
         ls.block = block_override;
         ls.grid = (int)((threads + block_override - 1) / block_override);
@@ -698,15 +705,18 @@ cudaError_t launch_gj8(const TableSrc& ts, const PropArgs& a, int num_sms, cudaS
         return cudaSuccess;
     // Default walk (measured on B200 at 70x70, LEO objects, mixed / FP64 M object-steps/s with the
     // two-column walk): two objects per thread above 128 objects per SM (20,000 objects: 66.5 /
-    // 35.3 against 57.2 / 34.3 with two lanes per pair; 37,000: 120 / 64 against 104 / 62); two
-    // lanes per pair of objects from 112 to 128 per SM, where they fill the four schedulers with
-    // one warp each (18,944 objects: 67.7 / 41.2 against 63.3 / 33.6 with two objects per thread);
-    // below, 2 or more lanes per object (9,472 objects: 48.2 / 31.0 against 34.0 / 20.8). One or
-    // two objects per thread when no lane-layout table is at hand.
+    // 35.3 against 57.2 / 34.3 with two lanes per pair; 37,000: 120 / 64 against 104 / 62), except
+    // that FP64 takes one object per thread up to 256 objects per SM, where two objects per thread
+    // leave at most one warp per scheduler (20,000 objects: 40.0 against 35.3; 30,000: 57.2 against
+    // 52.7; 37,000: 65.1 against 64.5); two lanes per pair of objects from 112 to 128 per SM, where
+    // they fill the four schedulers with one warp each (18,944 objects: 67.7 / 41.2 against 63.3 /
+    // 33.6 with two objects per thread); below, 2 or more lanes per object (9,472 objects: 48.2 /
+    // 31.0 against 34.0 / 20.8). One or two objects per thread when no lane-layout table is at hand.
     if (walk <= 0) {
         const bool lanes = lane_ts && a.kind == 0;
+        const bool fp64_gravity = a.kind == 0 && !ts.mixed;
         if (a.n > (int64_t)num_sms * 128 || (!lanes && a.n >= (int64_t)num_sms * 128))
-            walk = kWalkTwoObjects;
+            walk = fp64_gravity && a.n <= (int64_t)num_sms * 256 ? kWalkOneObject : kWalkTwoObjects;
         else if (a.n >= (int64_t)num_sms * 112)
             walk = kWalkLanesTwo;
         else
