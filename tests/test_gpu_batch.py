@@ -87,6 +87,23 @@ def test_batch_mixed_precision(contexts):
     _compare(outs, reqs, lambda q: contexts(q["degree"]), 1e-3, 1e-6)
 
 
+@pytest.mark.parametrize("precision", [0, 1])
+def test_batch_of_single_lane_items(contexts, precision):
+    # enough objects that every request keeps one lane per object: the persistent kernel then
+    # walks two gravity columns at a time on the lane-layout table (degree 8 in mixed mode takes
+    # the one-column lane walk inside the same kernel)
+    ctx = contexts(70, precision)
+    # (more degree-70 items than warps, so none of them is longer than the mean warp load; the
+    # degree-36 and degree-8 items are shorter still)
+    reqs = _requests([(20000, 6, 30.0, 70), (20000, 6, 60.0, 70), (20000, 6, 10.0, 70),
+                      (20000, 6, 120.0, 70), (8000, 4, 30.0, 36), (8000, 10, 60.0, 8)], 6)
+    lpo, _ = ctx.batch_plan(reqs)
+    assert all(int(p) == 1 for p in lpo), lpo
+    outs = ctx.propagate_batch(reqs)
+    tol = (1e-6, 1e-9) if precision == 0 else (1e-3, 1e-6)
+    _compare(outs, reqs, lambda q: contexts(q["degree"]), *tol)
+
+
 def test_batch_graph_replay_new_inputs(contexts):
     ctx = contexts(70)
     a = _requests(SPEC[:6], 4)
