@@ -73,8 +73,9 @@ inline double lpt_makespan(std::vector<std::pair<double, int64_t>>& groups, doub
 // load and the shortest possible item of the longest request -- doubles its lanes while that
 // shortens the item -- except that a batch whose items fit one wave of warps keeps them in one
 // wave (lanes cost efficiency; a second wave of split items costs more). Measured on B200:
-// 4,096 uneven requests 9.3 s; one 65,536-object request at 70x70 keeps one lane per object
-// (95 M object-steps/s, against 75 M with two).
+// 4,096 uneven requests 8.8 s; one 65,536-object request at 70x70 keeps one lane per object
+// (115 M object-steps/s with the two-column walk; 75 M with two lanes per object and the
+// one-column walk).
 template <class ItemTime>
 double choose_lanes(const std::vector<int64_t>& n, const std::vector<int>& steps, double warps,
     const ItemTime& item_time, std::vector<int>& lpo, bool fixed)
