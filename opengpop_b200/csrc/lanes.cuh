@@ -11,6 +11,14 @@
 
 namespace gpop {
 
+// Lane setup by prefix products over the object's lanes (log2 P shuffle steps) instead of each
+// lane's own powers of (C1 + i S1) and q (tuned batch rates on B200, object-steps/s per SM:
+// degree 8 with 32 lanes 3.5e5 -> 4.7e5, degree 70 with 32 lanes 1.49e5 -> 1.65e5).
+#ifndef GPOP_LANE_SCAN
+#define GPOP_LANE_SCAN 1
+#endif
+constexpr bool kLaneScan = GPOP_LANE_SCAN != 0;
+
 // Stages a lane-layout blob into shared memory (after a 128-byte mbarrier slot) and binds it.
 __device__ __forceinline__ bool bind_lane_table(uint8_t* smem, const TableSrc& ts, unsigned* err, GravSmem& g)
 {
@@ -76,6 +84,35 @@ __device__ __forceinline__ void gravity_itrs_lk(const GravSmem& gs, int l, int P
         wf[k] = (float)w[k];
         C1[k] = x[k] / r[k];
         S1[k] = y[k] / r[k];
+        G[k] = H[k] = J[k] = KK[k] = 0.0;
+        if (kLaneScan && P > 1) {
+            // prefix products over the group's lanes (segments of width P): lane l ends with
+            // z^(l+1) and q^(l+1), z = C1 + i S1; the lane's first column, the step between its
+            // columns and the m - 1 values follow by shuffles
+            double zc = C1[k], zs = S1[k], zq = q[k];
+            for (int o = 1; o < P; o <<= 1) {
+                const double pc = __shfl_up_sync(mask, zc, o, P), ps = __shfl_up_sync(mask, zs, o, P);
+                const double pq = __shfl_up_sync(mask, zq, o, P);
+                if (l >= o) {
+                    cmul(pc, ps, zc, zs, zc, zs);
+                    zq = pq * zq;
+                }
+            }
+            const double c1 = __shfl_up_sync(mask, zc, 1, P), s1 = __shfl_up_sync(mask, zs, 1, P);
+            const double q1 = __shfl_up_sync(mask, zq, 1, P);
+            const double c2 = __shfl_up_sync(mask, zc, 2, P), s2 = __shfl_up_sync(mask, zs, 2, P);
+            Cm[k] = l >= 1 ? c1 : 1.0; // z^l
+            Sm[k] = l >= 1 ? s1 : 0.0;
+            qm[k] = l >= 1 ? q1 : 1.0; // q^l
+            Cp[k] = l >= 2 ? c2 : (l == 1 ? 1.0 : 0.0); // z^(l-1); column 0 has no J, K or H part
+            Sp[k] = l >= 2 ? s2 : 0.0;
+            CP[k] = __shfl_sync(mask, zc, P - 1, P); // z^P: step between this lane's columns
+            SP[k] = __shfl_sync(mask, zs, P - 1, P);
+            qP[k] = __shfl_sync(mask, zq, P - 1, P);
+            CPm1[k] = __shfl_sync(mask, zc, P - 2, P); // z^(P-1): the m - 1 values of column P
+            SPm1[k] = __shfl_sync(mask, zs, P - 2, P);
+            continue;
+        }
         cpow(C1[k], S1[k], P, CP[k], SP[k]); // step between this lane's columns
         cpow(C1[k], S1[k], l, Cm[k], Sm[k]);
         if (l > 0)
@@ -89,7 +126,6 @@ __device__ __forceinline__ void gravity_itrs_lk(const GravSmem& gs, int l, int P
             qm[k] *= q[k];
         for (int i = 0; i < P; ++i)
             qP[k] *= q[k];
-        G[k] = H[k] = J[k] = KK[k] = 0.0;
     }
     const int Lhead = (MIXED && L > kMixedSplit) ? kMixedSplit : L;
     // column bases of the lane's next column are read one column ahead (they are shared-memory
