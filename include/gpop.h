@@ -212,6 +212,48 @@ gpop_status gpop_predict_unit(gpop_ctx* ctx, int32_t kind, double h, int32_t ste
 gpop_status gpop_finalize_correction_unit(gpop_ctx* ctx, double h, double* r3, double* v3,
     const double* a27, const double* s3, const double* S3, void* stream);
 
+/* ---- integrator pieces between force evaluations (n objects, caller-supplied accelerations) ----
+ * The path of the reference's GpuStartup, Predictor and GpuPropagator with an arbitrary
+ * IForceModel: the caller evaluates the model's hooks between these calls. Buffers are device
+ * AoS in the reference's layouts: x, v, r, s3, S3, prev3, sum1, sum2 [n][3]; R27, V27, A27, s27,
+ * S27 [n][9][3]; Kx30, Kv30 [n][10][3]. None of them allocates. ctx may be NULL (the current
+ * device; no error text). */
+/* RK8::step stage k of startup step `step` (+-1..4) (gpu_startup.cu:108-135): writes the stage
+ * state to x_dev, v_dev and the stage velocity to Kx30 slot k; stages 1..9 read Kx30 and Kv30
+ * slots 0..k-1 (Kv30: the generation accelerations the hook wrote). */
+gpop_status gpop_rk8_stage(gpop_ctx* ctx, int64_t n, double h, int32_t step, int32_t k,
+    const double* R27, const double* V27, double* Kx30, const double* Kv30, double* x_dev,
+    double* v_dev, void* stream);
+/* RK8::step end (gpu_startup.cu:136-144): column 4 + step of R27, V27 from the ten stages. */
+gpop_status gpop_rk8_finish(gpop_ctx* ctx, int64_t n, double h, int32_t step, double* R27,
+    double* V27, const double* Kx30, const double* Kv30, void* stream);
+/* GpuStartup before its predictor (gpu_startup.cu:55-60): column 4 of R27, V27 = r, v; the rest
+ * of R27, V27 and all of A27, s27, S27 (each may be NULL) zeroed. */
+gpop_status gpop_startup_init(gpop_ctx* ctx, int64_t n, const double* r_dev, const double* v_dev,
+    double* R27, double* V27, double* A27, double* s27, double* S27, void* stream);
+/* StartupCorrector::Correct without its force evaluations (gpu_startup.cu:247-290): s27, S27
+ * from A27, then the state columns other than the epoch's. */
+gpop_status gpop_startup_correct(gpop_ctx* ctx, int64_t n, double h, double* R27, double* V27,
+    const double* A27, double* s27, double* S27, void* stream);
+/* Predictor::Predict without its force evaluation (prediction.cu:49-70): r, v predicted, S3
+ * advanced, A27 shifted one column (column 8 is then the hook's), and prev3 = s3 and the corrector
+ * sums sum1, sum2 of GpuPropagator::Correct (gpu_propagator.cu:86-100). */
+gpop_status gpop_gj8_predict(gpop_ctx* ctx, int64_t n, double h, double* r_dev, double* v_dev,
+    double* A27, const double* s3, double* S3, double* prev3, double* sum1, double* sum2, void* stream);
+/* One pass of GpuPropagator::Correct after its force evaluation wrote A27 column 8
+ * (gpu_propagator.cu:101-117): s3, v, r. */
+gpop_status gpop_gj8_correct(gpop_ctx* ctx, int64_t n, double h, double* r_dev, double* v_dev,
+    const double* A27, double* s3, const double* S3, const double* prev3, const double* sum1,
+    const double* sum2, void* stream);
+/* Column col of an [n][cols][3] matrix copied to the [n][3] vector v3_dev (to_matrix = 0) or
+ * from it (CopyStartupStateKernel, MoveColumnToVectorKernel, CopySKernel). */
+gpop_status gpop_matrix_column(gpop_ctx* ctx, int64_t n, double* m_dev, int32_t cols, int32_t col,
+    double* v3_dev, int32_t to_matrix, void* stream);
+/* The Gauss-Jackson (a90) and summed-Adams (b90) ordinate tables in the layout of the reference's
+ * devA / devB (gpu_constants::createCoefficients): entry 10 k + c is the coefficient of history
+ * column k in row c. Either may be NULL. */
+gpop_status gpop_gj8_coefficients(gpop_ctx* ctx, double* a90_dev, double* b90_dev, void* stream);
+
 /* ---- force model ---- */
 /* GravitySource::ComputeAcceleration (gravity_source.cu:168-211): r_dev, a_dev [n][3] GCRS;
  * frame9_dev = ITRS->GCRS column-major 3x3 (NULL = identity). precision: gpop_precision. */
@@ -240,6 +282,17 @@ gpop_status gpop_ca_create(gpop_ctx* ctx, const gpop_time* start, double h, int6
  * used by unit_tests/closest_approach_test.cu): same screen and refinement, analytic force kind. */
 gpop_status gpop_ca_create_analytic(gpop_ctx* ctx, int32_t kind, double h, int64_t n,
     const double* r_in, const double* v_in, const uint32_t* set_ids, gpop_ca** out);
+/* ClosestApproach over an arbitrary IForceModel (closest_approach.cu:47-157 with a force model
+ * that is not the library's): the same partition, screen and refinement, with the trajectory
+ * supplied by the caller through gpop_ca_append (r_in, v_in: host epoch state, kept for
+ * gpop_ca_trajectory). gpop_ca_propagate is refused on such an object. */
+gpop_status gpop_ca_create_external(gpop_ctx* ctx, double h, int64_t n, const double* r_in,
+    const double* v_in, const uint32_t* set_ids, gpop_ca** out);
+/* The next `steps` propagated steps of an external object: device AoS [steps][n][3] positions,
+ * velocities and the steps' exported accelerations (GpuPropagator::Step's devAccelerationVector);
+ * runs the screen over them (UpdateClosestApproachKernel, closest_approach.cu:138-146). */
+gpop_status gpop_ca_append(gpop_ca* ca, int32_t steps, const double* r_dev, const double* v_dev,
+    const double* a_dev);
 /* ClosestApproach::Propagate (closest_approach.cu:129-157): steps more steps; running minima
  * persist across calls. */
 gpop_status gpop_ca_propagate(gpop_ca* ca, int32_t steps);

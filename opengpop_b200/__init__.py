@@ -32,8 +32,10 @@ EXPORTS = (
     "gpop_propagator_steps_done", "gpop_propagator_destroy", "gpop_propagate_analytic",
     "gpop_propagate_batch", "gpop_batch_plan", "gpop_tune", "gpop_batch_device_seconds", "gpop_gravity_jacobian", "gpop_stm", "gpop_propagate_vjp",
     "gpop_miss_gradient", "gpop_sample_states", "gpop_startup", "gpop_corrector_unit",
-    "gpop_predict_unit", "gpop_finalize_correction_unit", "gpop_gravity", "gpop_frame_matrices",
-    "gpop_ca_create", "gpop_ca_create_analytic", "gpop_ca_propagate", "gpop_ca_find", "gpop_ca_pairs", "gpop_ca_num_pairs",
+    "gpop_predict_unit", "gpop_finalize_correction_unit", "gpop_rk8_stage", "gpop_rk8_finish",
+    "gpop_startup_init", "gpop_startup_correct", "gpop_gj8_predict", "gpop_gj8_correct",
+    "gpop_matrix_column", "gpop_gj8_coefficients", "gpop_gravity", "gpop_frame_matrices",
+    "gpop_ca_create", "gpop_ca_create_analytic", "gpop_ca_create_external", "gpop_ca_append", "gpop_ca_propagate", "gpop_ca_find", "gpop_ca_pairs", "gpop_ca_num_pairs",
     "gpop_ca_trajectory", "gpop_ca_device_seconds", "gpop_ca_destroy",
 )
 

@@ -113,6 +113,80 @@ gpop_status refine(gpop_ca* ca, cudaStream_t s)
     return GPOP_OK;
 }
 
+constexpr int kExternalKind = -1; // trajectory supplied by gpop_ca_append
+
+// AoS rows [steps][n][3] of r, v, a into the trajectory store's SoA rows [step][3][n].
+__global__ void append_rows_kernel(int64_t n, int64_t count, const double* __restrict__ r,
+    const double* __restrict__ v, const double* __restrict__ a, double* __restrict__ tr,
+    double* __restrict__ tv, double* __restrict__ ta)
+{
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= count)
+        return;
+    const int64_t s = t / n, i = t - s * n;
+    for (int j = 0; j < 3; ++j) {
+        const int64_t src = (s * n + i) * 3 + j, dst = (s * 3 + j) * n + i;
+        tr[dst] = r[src];
+        tv[dst] = v[src];
+        ta[dst] = a[src];
+    }
+}
+
+// Grows the trajectory store to `need` steps, keeping the rows already written.
+gpop_status grow_store(gpop_ca* ca, int need)
+{
+    gpop_ctx* ctx = ca->ctx;
+    if (need <= ca->cap_steps)
+        return GPOP_OK;
+    const size_t row = (size_t)ca->n * 3 * sizeof(double);
+    DevBuf nr, nv, na;
+    cudaError_t e;
+    if ((e = nr.ensure(row * need)) != cudaSuccess || (e = nv.ensure(row * need)) != cudaSuccess
+        || (e = na.ensure(row * need)) != cudaSuccess) {
+        nr.release();
+        nv.release();
+        na.release();
+        return fail(ctx, GPOP_ERR_NOMEM, "trajectory store (" + std::to_string(3 * row * need >> 20) + " MiB)");
+    }
+    if (ca->total_steps > 0) {
+        const size_t used = row * ca->total_steps;
+        cudaMemcpy(nr.p, ca->traj_r.p, used, cudaMemcpyDeviceToDevice);
+        cudaMemcpy(nv.p, ca->traj_v.p, used, cudaMemcpyDeviceToDevice);
+        cudaMemcpy(na.p, ca->traj_a.p, used, cudaMemcpyDeviceToDevice);
+    }
+    ca->traj_r.release();
+    ca->traj_v.release();
+    ca->traj_a.release();
+    ca->traj_r = nr;
+    ca->traj_v = nv;
+    ca->traj_a = na;
+    nr.p = nv.p = na.p = nullptr;
+    ca->cap_steps = need;
+    return GPOP_OK;
+}
+
+// UpdateClosestApproachKernel over steps [total_steps, need) of the store (running minima).
+gpop_status screen_steps(gpop_ca* ca, int need, cudaStream_t s)
+{
+    ScreenArgs a;
+    a.n = ca->n;
+    a.traj_r = ca->traj_r.as<double>();
+    a.bound = ca->bound.as<int>();
+    a.base = ca->base.as<int64_t>();
+    a.tiles = ca->tiles.as<int2>();
+    a.min_d2 = ca->min_d2.as<double>();
+    a.min_step = ca->min_step.as<uint32_t>();
+    a.step_lo = ca->total_steps;
+    a.step_hi = need;
+    a.step_offset = 0;
+    a.init = ca->total_steps == 0 ? 1 : 0;
+    const cudaError_t e = launch_screen(a, ca->num_tiles, s);
+    if (e != cudaSuccess)
+        return cuda_fail(ca->ctx, e, "screen kernel");
+    ca->ctx->launches++;
+    return GPOP_OK;
+}
+
 } // namespace
 
 extern "C" {
@@ -230,6 +304,56 @@ gpop_status gpop_ca_create_analytic(gpop_ctx* ctx, int32_t kind, double h, int64
     return st;
 }
 
+gpop_status gpop_ca_create_external(gpop_ctx* ctx, double h, int64_t n, const double* r_in,
+    const double* v_in, const uint32_t* set_ids, gpop_ca** out)
+{
+    if (!ctx || !out)
+        return GPOP_ERR_INVALID_ARG;
+    const gpop_time t0 { 2000, 1, 1, 0, 0, 0.0 };
+    gpop_status st = gpop_ca_create(ctx, &t0, h, n, r_in, v_in, set_ids, out);
+    if (st == GPOP_OK)
+        (*out)->kind = kExternalKind;
+    return st;
+}
+
+gpop_status gpop_ca_append(gpop_ca* ca, int32_t steps, const double* r_dev, const double* v_dev,
+    const double* a_dev)
+{
+    if (!ca)
+        return GPOP_ERR_INVALID_ARG;
+    gpop_ctx* ctx = ca->ctx;
+    if (ca->kind != kExternalKind)
+        return fail(ctx, GPOP_ERR_STATE, "gpop_ca_append needs an object from gpop_ca_create_external");
+    if (steps <= 0 || !r_dev || !v_dev || !a_dev)
+        return fail(ctx, GPOP_ERR_INVALID_ARG, "steps must be positive and the buffers given");
+    cudaError_t e = cudaSetDevice(ctx->cfg.device);
+    if (e != cudaSuccess)
+        return cuda_fail(ctx, e, "cudaSetDevice");
+    cudaStream_t s = nullptr;
+    const int need = ca->total_steps + steps;
+    gpop_status st = grow_store(ca, need);
+    if (st != GPOP_OK)
+        return st;
+    const size_t off = (size_t)ca->total_steps * 3 * ca->n;
+    const int64_t count = (int64_t)steps * ca->n;
+    append_rows_kernel<<<(unsigned)((count + 255) / 256), 256, 0, s>>>(ca->n, count, r_dev, v_dev, a_dev,
+        ca->traj_r.as<double>() + off, ca->traj_v.as<double>() + off, ca->traj_a.as<double>() + off);
+    if ((e = cudaGetLastError()) != cudaSuccess)
+        return cuda_fail(ctx, e, "trajectory rows");
+    ctx->launches++;
+    DeviceTimer timer;
+    timer.mark(s);
+    if ((st = screen_steps(ca, need, s)) != GPOP_OK)
+        return st;
+    timer.mark(s);
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess)
+        return cuda_fail(ctx, e, "screen kernel");
+    ca->t_screen += timer.seconds(0, 1);
+    ca->total_steps = need;
+    ca->refined = false;
+    return GPOP_OK;
+}
+
 int64_t gpop_ca_num_pairs(const gpop_ca* ca) { return ca ? (int64_t)ca->num_pairs : -1; }
 
 gpop_status gpop_ca_propagate(gpop_ca* ca, int32_t steps)
@@ -243,32 +367,12 @@ gpop_status gpop_ca_propagate(gpop_ca* ca, int32_t steps)
     if (e != cudaSuccess)
         return cuda_fail(ctx, e, "cudaSetDevice");
     cudaStream_t s = nullptr;
+    if (ca->kind == kExternalKind)
+        return fail(ctx, GPOP_ERR_STATE, "this closest-approach object takes its trajectory from gpop_ca_append");
     const int need = ca->total_steps + steps;
-    if (need > ca->cap_steps) { // grow the trajectory store, keeping the rows already written
-        const size_t row = (size_t)ca->n * 3 * sizeof(double);
-        DevBuf nr, nv, na;
-        if ((e = nr.ensure(row * need)) != cudaSuccess || (e = nv.ensure(row * need)) != cudaSuccess
-            || (e = na.ensure(row * need)) != cudaSuccess) {
-            nr.release();
-            nv.release();
-            na.release();
-            return fail(ctx, GPOP_ERR_NOMEM, "trajectory store (" + std::to_string(3 * row * need >> 20) + " MiB)");
-        }
-        if (ca->total_steps > 0) {
-            const size_t used = row * ca->total_steps;
-            cudaMemcpy(nr.p, ca->traj_r.p, used, cudaMemcpyDeviceToDevice);
-            cudaMemcpy(nv.p, ca->traj_v.p, used, cudaMemcpyDeviceToDevice);
-            cudaMemcpy(na.p, ca->traj_a.p, used, cudaMemcpyDeviceToDevice);
-        }
-        ca->traj_r.release();
-        ca->traj_v.release();
-        ca->traj_a.release();
-        ca->traj_r = nr;
-        ca->traj_v = nv;
-        ca->traj_a = na;
-        nr.p = nv.p = na.p = nullptr;
-        ca->cap_steps = need;
-    }
+    gpop_status gs = grow_store(ca, need);
+    if (gs != GPOP_OK)
+        return gs;
     // ClosestApproach::Propagate builds a new GpuPropagator from the current state for every
     // phase (closest_approach.cu:134-136): a fresh startup each call. The reference's force model
     // keeps the original start epoch for every phase; GPOP_FIX_PHASE_EPOCH advances it.
@@ -298,21 +402,8 @@ gpop_status gpop_ca_propagate(gpop_ca* ca, int32_t steps)
     if (st != GPOP_OK)
         return st;
     timer.mark(s);
-    ScreenArgs a;
-    a.n = ca->n;
-    a.traj_r = ca->traj_r.as<double>();
-    a.bound = ca->bound.as<int>();
-    a.base = ca->base.as<int64_t>();
-    a.tiles = ca->tiles.as<int2>();
-    a.min_d2 = ca->min_d2.as<double>();
-    a.min_step = ca->min_step.as<uint32_t>();
-    a.step_lo = ca->total_steps;
-    a.step_hi = need;
-    a.step_offset = 0;
-    a.init = ca->total_steps == 0 ? 1 : 0;
-    if ((e = launch_screen(a, ca->num_tiles, s)) != cudaSuccess)
-        return cuda_fail(ctx, e, "screen kernel");
-    ctx->launches++;
+    if ((st = screen_steps(ca, need, s)) != GPOP_OK)
+        return st;
     timer.mark(s);
     if ((e = cudaStreamSynchronize(s)) != cudaSuccess)
         return cuda_fail(ctx, e, "screen kernel");
