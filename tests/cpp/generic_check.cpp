@@ -5,6 +5,7 @@
 //    same gravity as the fused path; its results are printed beside the fused path's.
 //  - Oscillator: a = -w^2 r computed on the host in the hooks (a force with a closed-form
 //    solution); counts the hook calls.
+//  - Poly: a polynomial in time with the reference mock's time rules (exact solution).
 //  - ClosestApproach over the library's ForceModel and over Hooks, two phases.
 #include "gpop.hpp"
 
@@ -64,6 +65,37 @@ struct Oscillator : IForceModel {
     {
         ++prop_calls;
         eval(p, a, 27, col);
+    }
+};
+
+// a = -6 t + 42 t^5 on every axis, with time from the hook arguments by the rules of the reference's
+// mock force model (unit_tests/include/mock_force_model.cuh:65-106): RK8 stage k of startup step s
+// at (s - 1 + c_k) h for s > 0 and (s + 1 - c_k) h for s < 0, propagation epoch index i at (i - 4) h.
+// From r = v = 0 the solution is r = -t^3 + t^7, which GJ8 and RK8 integrate exactly.
+struct Poly : IForceModel {
+    unsigned n;
+    double h;
+    explicit Poly(unsigned count, double step) : n(count), h(step) { }
+    static double f(double t) { return -6 * t + 42 * t * t * t * t * t; }
+    void write(double t, double* devOut, int stride, int slot)
+    {
+        std::vector<double> a(3 * n, f(t));
+        cudaMemcpy2D(devOut + 3 * slot, sizeof(double) * stride, a.data(), sizeof(double) * 3, sizeof(double) * 3, n,
+            cudaMemcpyHostToDevice);
+    }
+    void PreInitialize() override { }
+    void InitializeGeneration(int, int) override { }
+    void ComputeGenerationAcceleration(double*, double*, double* k, int step, int kIndex) override
+    {
+        static const double c[10] = { 0.0, 4.0 / 27.0, 2.0 / 9.0, 1.0 / 3.0, 1.0 / 2.0, 2.0 / 3.0, 1.0 / 6.0, 1.0,
+            5.0 / 6.0, 1.0 };
+        const int dir = step > 0 ? -1 : 1;
+        write((double)(step + dir) * h + (-dir) * c[kIndex] * h, k, 30, kIndex);
+    }
+    void InitializePropagation(int, int) override { }
+    void ComputePropagationAcceleration(double*, double*, double* a, int stepNum, int col) override
+    {
+        write((double)(stepNum - 4) * h, a, 27, col);
     }
 };
 
@@ -144,6 +176,23 @@ int main(int argc, char** argv)
         std::printf("{\"osc_calls\": [%ld, %ld, %ld, %ld, %ld]}\n", osc.pre, osc.init_gen, osc.gen_calls,
             osc.init_prop, osc.prop_calls);
         std::printf("{\"osc_t\": %.17g}\n", hh * osteps);
+    }
+    {
+        // the polynomial mock: 60 steps of 0.1 from rest
+        const unsigned m = 3;
+        const double hh = 0.1;
+        const int psteps = 60;
+        std::vector<double> zero(3 * m, 0.0), ro(3 * m), vo(3 * m);
+        cudaMemcpy(dr, zero.data(), sizeof(double) * 3 * m, cudaMemcpyHostToDevice);
+        cudaMemcpy(dv, zero.data(), sizeof(double) * 3 * m, cudaMemcpyHostToDevice);
+        Poly poly(m, hh);
+        GpuPropagator prop(dr, dv, m, nullptr, hh, &params, poly, psteps);
+        for (int s = 1; s <= psteps; ++s)
+            prop.Step();
+        prop.CopyStateToHost(ro.data(), vo.data());
+        print_vec("poly_r", ro.data(), ro.size());
+        print_vec("poly_v", vo.data(), vo.size());
+        std::printf("{\"poly_t\": %.17g}\n", hh * psteps);
     }
     {
         // ClosestApproach: fused (ForceModel) and per-evaluation (Hooks) over two phases; every

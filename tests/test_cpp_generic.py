@@ -53,6 +53,11 @@ def test_generic_path(tmp_path):
     assert (pre, init_gen, init_prop) == (1, 1, 1)
     assert gen == 80
     assert prop == 9 + 7 * 8 + (200 - 4) * 8
+    # the reference mock's polynomial force, from rest: r = -t^3 + t^7, v = -3 t^2 + 7 t^6 at t = 6
+    t = res["poly_t"]
+    r_ex, v_ex = -t ** 3 + t ** 7, -3 * t ** 2 + 7 * t ** 6
+    assert np.abs(np.array(res["poly_r"]) - r_ex).max() <= 1e-9 * r_ex
+    assert np.abs(np.array(res["poly_v"]) - v_ex).max() <= 1e-9 * v_ex
     # ClosestApproach: the per-evaluation phases screen and refine as the fused ones do
     fused = np.array(res["ca_fused"]).reshape(-1, 4)
     generic = np.array(res["ca_generic"]).reshape(-1, 4)
