@@ -102,6 +102,12 @@ constexpr bool kBatchPairs = GPOP_BATCH_PAIRS != 0;
 #endif
 constexpr bool kBatchStage = GPOP_BATCH_STAGE != 0;
 constexpr int kBatchStageDoubles = 24; // two objects x 12
+// Batches of single-lane items stage the plain table and run gj8_kernel's gravity walk (no lane
+// code in that kernel).
+#ifndef GPOP_BATCH_PLAIN
+#define GPOP_BATCH_PLAIN 1
+#endif
+constexpr bool kBatchPlain = GPOP_BATCH_PLAIN != 0;
 
 // One work item on one warp: K = 2 objects per lane for single-lane items (up to 64 objects),
 // else one object per group of P lanes (up to 32 / P objects).
@@ -193,7 +199,9 @@ __device__ __forceinline__ void run_item(const GravSmem& g0, const BatchArgs& a,
         }
         const double* M = rq.prop_m + (size_t)(step + 4) * 9;
         for (int itc = 0; itc < a.ncorr; ++itc) {
-            if constexpr (K == 2 && PAIRS) {
+            if constexpr (K == 2 && PAIRS && kBatchPlain) {
+                gravity_gcrs<MIXED, 2>(g, M, r, a8); // the plain table: gj8_kernel's walk
+            } else if constexpr (K == 2 && PAIRS) {
                 // two objects per lane: the two-column walk on the lane-layout tables (mixed
                 // needs degree > 8 for it)
                 if (!MIXED || g.L > kMixedSplit)
@@ -244,9 +252,15 @@ template <bool MIXED, bool STAGE, bool PAIRS>
 __global__ void __launch_bounds__(256, 1) batch_gj8_kernel(TableSrc ts, BatchArgs a)
 {
     extern __shared__ __align__(128) uint8_t smem[];
+    constexpr bool kPlain = PAIRS && kBatchPlain;
     GravSmem g0;
-    if (!bind_lane_table(smem, ts, a.err, g0))
-        return;
+    if constexpr (kPlain) {
+        if (!stage_batch_table<MIXED>(smem, ts, a.err, g0))
+            return;
+    } else {
+        if (!bind_lane_table(smem, ts, a.err, g0))
+            return;
+    }
     const int lane = threadIdx.x & 31;
     double* stage = reinterpret_cast<double*>(smem + stage_offset(ts)) + threadIdx.x;
     for (;;) {
@@ -258,10 +272,14 @@ __global__ void __launch_bounds__(256, 1) batch_gj8_kernel(TableSrc ts, BatchArg
             break;
         const BatchItem it = a.items[item];
         const BatchReq rq = a.reqs[it.req];
-        if (rq.lpo == 1)
+        if constexpr (kPlain) { // every item has one lane per object
             run_item<MIXED, 2, STAGE, PAIRS>(g0, a, it, rq, lane, stage);
-        else
-            run_item<MIXED, 1, false, false>(g0, a, it, rq, lane, stage);
+        } else {
+            if (rq.lpo == 1)
+                run_item<MIXED, 2, STAGE, PAIRS>(g0, a, it, rq, lane, stage);
+            else
+                run_item<MIXED, 1, false, false>(g0, a, it, rq, lane, stage);
+        }
     }
 }
 
@@ -301,12 +319,13 @@ static cudaError_t launch_batch_gj8_k(const TableSrc& ts, const BatchArgs& a, in
 }
 
 template <bool MIXED>
-static cudaError_t launch_batch_gj8_m(const TableSrc& ts, const BatchArgs& a, int blocks, int block,
-    cudaStream_t s)
+static cudaError_t launch_batch_gj8_m(const TableSrc& lane_ts, const TableSrc& plain_ts, const BatchArgs& a,
+    int blocks, int block, cudaStream_t s)
 {
+    const bool pairs = kBatchPairs && a.pair_walk;
+    const TableSrc& ts = pairs && kBatchPlain ? plain_ts : lane_ts;
     const size_t staged = stage_offset(ts) + (size_t)kBatchStageDoubles * 8 * block;
     const bool stage = kBatchStage && staged <= max_smem_optin();
-    const bool pairs = kBatchPairs && a.pair_walk;
     const size_t smem = stage ? staged : table_smem_bytes(ts);
     if (stage)
         return pairs ? launch_batch_gj8_k<MIXED, true, true>(ts, a, blocks, block, smem, s)
@@ -315,12 +334,13 @@ static cudaError_t launch_batch_gj8_m(const TableSrc& ts, const BatchArgs& a, in
                  : launch_batch_gj8_k<MIXED, false, false>(ts, a, blocks, block, smem, s);
 }
 
-cudaError_t launch_batch_gj8(const TableSrc& ts, const BatchArgs& a, int blocks, int block, cudaStream_t s)
+cudaError_t launch_batch_gj8(const TableSrc& lane_ts, const TableSrc& plain_ts, const BatchArgs& a,
+    int blocks, int block, cudaStream_t s)
 {
     if (a.n_items <= 0)
         return cudaSuccess;
-    return ts.mixed ? launch_batch_gj8_m<true>(ts, a, blocks, block, s)
-                    : launch_batch_gj8_m<false>(ts, a, blocks, block, s);
+    return lane_ts.mixed ? launch_batch_gj8_m<true>(lane_ts, plain_ts, a, blocks, block, s)
+                         : launch_batch_gj8_m<false>(lane_ts, plain_ts, a, blocks, block, s);
 }
 
 // ---- epoch tables of many requests: epoch e uses calendar cal[5 * epoch_req[e]] ----

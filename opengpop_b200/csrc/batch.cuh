@@ -51,9 +51,10 @@ struct BatchArgs {
 };
 
 cudaError_t launch_batch_startup(const TableSrc& ts, const BatchArgs& a, int num_sms, cudaStream_t s);
-// ts: the lane-layout table. blocks: persistent grid size; block: threads per block.
-cudaError_t launch_batch_gj8(const TableSrc& ts, const BatchArgs& a, int blocks, int block,
-    cudaStream_t s);
+// lane_ts: the lane-layout table; plain_ts: the same model in the plain layout (batches of
+// single-lane items). blocks: persistent grid size; block: threads per block.
+cudaError_t launch_batch_gj8(const TableSrc& lane_ts, const TableSrc& plain_ts, const BatchArgs& a,
+    int blocks, int block, cudaStream_t s);
 cudaError_t launch_frames_batch(const FrameData& fd, const int* cal, const int* epoch_req,
     const double* sec_args, int count, double* m_out, cudaStream_t s);
 

@@ -73,9 +73,9 @@ inline double lpt_makespan(std::vector<std::pair<double, int64_t>>& groups, doub
 // load and the shortest possible item of the longest request -- doubles its lanes while that
 // shortens the item -- except that a batch whose items fit one wave of warps keeps them in one
 // wave (lanes cost efficiency; a second wave of split items costs more). Measured on B200:
-// 4,096 uneven requests 8.8 s; one 65,536-object request at 70x70 keeps one lane per object
-// (115 M object-steps/s with the two-column walk; 75 M with two lanes per object and the
-// one-column walk).
+// 4,096 uneven requests 8.7 s; one 65,536-object request at 70x70 keeps one lane per object
+// (136 M object-steps/s with the two-column walk on the plain table; 75 M with two lanes per
+// object and the one-column walk).
 template <class ItemTime>
 double choose_lanes(const std::vector<int64_t>& n, const std::vector<int>& steps, double warps,
     const ItemTime& item_time, std::vector<int>& lpo, bool fixed)
@@ -458,7 +458,7 @@ gpop_status gpop_propagate_batch(gpop_ctx* ctx, const gpop_request* reqs, int32_
         if (le == cudaSuccess)
             le = cudaMemsetAsync(bc->queue.p, 0, sizeof(int), s);
         if (le == cudaSuccess)
-            le = launch_batch_gj8(ctx->lane_table(mixed), a, ctx->num_sms, 32 * kWarpsPerSm, s);
+            le = launch_batch_gj8(ctx->lane_table(mixed), ctx->table(mixed), a, ctx->num_sms, 32 * kWarpsPerSm, s);
         e = cudaStreamEndCapture(s, &graph);
         if (le != cudaSuccess || e != cudaSuccess) {
             if (graph)
