@@ -48,6 +48,11 @@ double eta(const gpop_ctx* ctx, int L, int P)
     return base70 / cost / (1.0 + 0.12 * lp);
 }
 
+// Speed of single-lane items in a batch of single-lane items (two-column walk on the plain table)
+// over their speed in mixed batches, which is what the tuner measures (65,536 objects at 70x70 on
+// B200: 135.6 / 115.0 M object-steps/s).
+constexpr double kPairWalkGain = 1.15;
+
 // Makespan of the persistent launch: work items taken longest first by the first free warp (the
 // queue order), simulated with a heap of warp loads.
 inline double lpt_makespan(std::vector<std::pair<double, int64_t>>& groups, double warps)
@@ -116,11 +121,35 @@ double choose_lanes(const std::vector<int64_t>& n, const std::vector<int>& steps
                 break;
         }
     }
-    std::vector<std::pair<double, int64_t>> groups;
-    for (size_t r = 0; r < R; ++r)
-        if (steps[r] > 0)
-            groups.push_back({ item_time(r, lpo[r]), items_of(r, lpo[r]) });
-    return lpt_makespan(groups, warps);
+    auto span_of = [&](const std::vector<int>& lp) {
+        std::vector<std::pair<double, int64_t>> groups;
+        for (size_t r = 0; r < R; ++r)
+            if (steps[r] > 0)
+                groups.push_back({ item_time(r, lp[r]), items_of(r, lp[r]) });
+        return lpt_makespan(groups, warps);
+    };
+    const double span = span_of(lpo);
+    if (!fixed) {
+        // A batch of single-lane items runs the two-column walk, faster than the rates measured
+        // for single-lane items in mixed batches: keep one lane per object unless the lanes plan
+        // is shorter even so (64 requests of 1,024 objects at 70x70: lanes on some requests left
+        // the makespan as it was and cost the whole batch the faster kernel, 114 against 136 M
+        // object-steps/s).
+        std::vector<int> ones(R, 1);
+        bool all_one = true;
+        for (size_t r = 0; r < R; ++r)
+            all_one = all_one && (steps[r] <= 0 || lpo[r] == 1);
+        if (!all_one) {
+            const double span1 = span_of(ones) / kPairWalkGain;
+            if (span1 <= span) {
+                lpo = ones;
+                return span1;
+            }
+        } else {
+            return span / kPairWalkGain;
+        }
+    }
+    return span;
 }
 
 struct Plan {
