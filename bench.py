@@ -352,8 +352,9 @@ def run_adjoint(args, torch, G, dev):
     """Differentiation: 10,000 pairs (24 h, 30 s, 70x70, FP64), adjoint gradient of each miss
     distance; and 8,192 state transition matrices by the forward variational equations."""
     from opengpop_b200 import orbits
-    n_pairs, steps, n_stm = args.adjoint_pairs, args.adjoint_steps, args.stm_objects
+    n_pairs, steps = args.adjoint_pairs, args.adjoint_steps
     r, v, pairs = orbits.conjunction_pairs(n_pairs, SEED)
+    n_stm = min(args.stm_objects, r.shape[0])  # the STMs run on the pairs' first objects
     ctx = G.Context(precision=G.FP64)
     sampler = ClockSampler(torch.cuda.current_device())
     t_miss, t_stm = [], []
