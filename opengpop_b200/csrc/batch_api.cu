@@ -50,8 +50,9 @@ double eta(const gpop_ctx* ctx, int L, int P)
 
 // Speed of single-lane items in a batch of single-lane items (two-column walk on the plain table)
 // over their speed in mixed batches, which is what the tuner measures (65,536 objects at 70x70 on
-// B200: 135.6 / 115.0 M object-steps/s).
-constexpr double kPairWalkGain = 1.15;
+// B200: 135.6 / 115.0 M object-steps/s mixed precision, 69.7 / 66.8 M FP64).
+constexpr double kPairWalkGainMixed = 1.15;
+constexpr double kPairWalkGainFp64 = 1.04;
 
 // Makespan of the persistent launch: work items taken longest first by the first free warp (the
 // queue order), simulated with a heap of warp loads.
@@ -83,7 +84,7 @@ inline double lpt_makespan(std::vector<std::pair<double, int64_t>>& groups, doub
 // object and the one-column walk).
 template <class ItemTime>
 double choose_lanes(const std::vector<int64_t>& n, const std::vector<int>& steps, double warps,
-    const ItemTime& item_time, std::vector<int>& lpo, bool fixed)
+    const ItemTime& item_time, std::vector<int>& lpo, bool fixed, double pair_gain)
 {
     const size_t R = n.size();
     auto items_of = [&](size_t r, int P) { return (n[r] + batch_item_objects(P) - 1) / batch_item_objects(P); };
@@ -140,13 +141,13 @@ double choose_lanes(const std::vector<int64_t>& n, const std::vector<int>& steps
         for (size_t r = 0; r < R; ++r)
             all_one = all_one && (steps[r] <= 0 || lpo[r] == 1);
         if (!all_one) {
-            const double span1 = span_of(ones) / kPairWalkGain;
+            const double span1 = span_of(ones) / pair_gain;
             if (span1 <= span) {
                 lpo = ones;
                 return span1;
             }
         } else {
-            return span / kPairWalkGain;
+            return span / pair_gain;
         }
     }
     return span;
@@ -171,7 +172,8 @@ Plan make_plan(const gpop_ctx* ctx, const std::vector<int64_t>& n, const std::ve
     const bool fixed = ctx->force_lpo > 0; // autotuner: fixed lanes per object
     if (fixed)
         p.lpo.assign(R, ctx->force_lpo);
-    p.est = choose_lanes(n, steps, warps, item_time, p.lpo, fixed);
+    p.est = choose_lanes(n, steps, warps, item_time, p.lpo, fixed,
+        ctx->cfg.precision == GPOP_MIXED ? kPairWalkGainMixed : kPairWalkGainFp64);
     std::vector<std::pair<double, BatchItem>> items;
     for (size_t r = 0; r < R; ++r) {
         if (steps[r] <= 0)
