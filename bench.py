@@ -296,8 +296,13 @@ def run_batch(args, torch, G, dev):
 
 def run_screen(args, torch, G, dev):
     """Closest approach: 20,000 LEO objects, 2,000 seed-chosen objects against all (2,000
-    singleton sets plus one set of 18,000: 37,999,000 pairs), 70x70, 30 s, 3 days, 5 km."""
-    from opengpop_b200 import orbits
+    singleton sets plus one set of 18,000: 37,999,000 pairs), 70x70, 30 s, 3 days, 5 km.
+    Under torchrun each rank propagates its share of the objects, the ranks all-gather the
+    trajectory in windows and each screens and refines its block of pair rows; every time is the
+    max over ranks."""
+    import torch.distributed as dist
+    from opengpop_b200 import orbits, sharding
+    rank, world = env_int("RANK", 0), env_int("WORLD_SIZE", 1)
     n, steps, thr = args.screen_objects, args.screen_steps, 5000.0
     n_sel = n // 10
     r, v = orbits.leo(n, SEED)
@@ -305,26 +310,42 @@ def run_screen(args, torch, G, dev):
     order = np.concatenate([sel, np.setdiff1d(np.arange(n), sel)])
     r, v = r[order], v[order]
     set_ids = np.concatenate([np.arange(n_sel), np.full(n - n_sel, n_sel)]).astype(np.uint32)
-    ctx = G.Context(precision=G.FP64)
+    ctx = G.Context(device=dev.index, precision=G.FP64)
     sampler = ClockSampler(torch.cuda.current_device())
     res = []
     for i in range(args.warmup + args.steps):
         if i == args.warmup:
             sampler.start()
+        if world > 1:
+            dist.barrier()
         t0 = time.perf_counter()
-        ca = ctx.closest_approach(START, H, r, v, set_ids)
-        ca.propagate(steps)
-        recs = ca.find(thr)
-        wall = time.perf_counter() - t0
-        dt = ca.device_seconds()
-        pairs = ca.num_pairs
-        ca.close()
+        if world == 1:
+            ca = ctx.closest_approach(START, H, r, v, set_ids)
+            ca.propagate(steps)
+            recs = ca.find(thr)
+            wall = time.perf_counter() - t0
+            dt = list(ca.device_seconds())
+            dt.insert(1, 0.0)
+            pairs = ca.num_pairs
+            ca.close()
+        else:
+            recs, sec = sharding.closest_approach_sharded(ctx, START, H, r, v, set_ids, [steps], thr)
+            wall = time.perf_counter() - t0
+            dt = [sec["propagation"], sec["exchange"], sec["screen"], sec["refinement"]]
+            pairs = int(sharding.pairs_per_row(set_ids).sum())
         if i >= args.warmup:
             res.append((wall, dt))
     clocks = sampler.stop()
     ctx.close()
-    wall = float(np.mean([x[0] for x in res]))
-    t_prop, t_screen, t_refine = (float(np.mean([x[1][k] for x in res])) for k in range(3))
+    wall = sharding.max_over_ranks(float(np.mean([x[0] for x in res])), dev)
+    t_prop, t_exch, t_screen, t_refine = (sharding.max_over_ranks(float(np.mean([x[1][k] for x in res])), dev)
+                                          for k in range(4))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    args.gpus = world
     pair_steps = pairs * steps
     peak64 = probe_peak(torch, True, dev)
     achieved = 9.0 * pair_steps / t_screen / 1e12
@@ -333,14 +354,19 @@ def run_screen(args, torch, G, dev):
             {"workload": "%d LEO objects (seed %d), %d vs all = %d pairs, 70x70, 30 s, "
                          "%d steps, threshold 5 km" % (n, SEED, n_sel, pairs, steps),
              "pairs": pairs, "steps": steps,
-             "l2": "trajectory store %.1f GB" % (n * steps * 72 / 1e9)},
-            {"ms_per_step": 1e3 * wall,
-             "device_seconds": {"propagation": t_prop, "screen": t_screen, "refinement": t_refine},
+             "l2": "trajectory store %.1f GB" % (n * steps * 72 / 1e9),
+             "parallelism": "one GPU" if world == 1 else
+             "object shards x%d, trajectory all-gather per 240 steps, pair rows x%d" % (world, world)},
+            {"n_gpus": world, "scaling": "strong", "ms_per_step": 1e3 * wall,
+             "device_seconds": {"propagation": t_prop, "exchange": t_exch, "screen": t_screen,
+                                "refinement": t_refine},
              "pairs_per_s_whole_job": pairs / wall,
              "found_below_threshold": len(recs),
              "e2e": {"value": pair_steps / wall, "unit": "pair-steps/s",
                      "h2d_bytes_per_step": n * 6 * 8 + n * 4, "d2h_bytes_per_step": len(recs) * 64,
-                     "call": "gpop_ca_create + gpop_ca_propagate + gpop_ca_find"},
+                     "call": "gpop_ca_create + gpop_ca_propagate + gpop_ca_find" if world == 1 else
+                     "sharding.closest_approach_sharded (gpop_propagator_step, NCCL all-gather, "
+                     "gpop_ca_append, gpop_ca_find)"},
              "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak64, "unit": "TFLOP/s",
                           "frac": achieved / peak64 if peak64 else None, "traffic": None,
                           "per_unit": "9 FP64 flops per pair-step"},
@@ -453,15 +479,15 @@ def main():
         import opengpop_b200 as G
         dev = torch.device("cuda", env_int("LOCAL_RANK", 0))
         torch.cuda.set_device(dev)
-        if args.workload == "batch":
+        if args.workload in ("batch", "screen"):
             if env_int("WORLD_SIZE", 1) > 1:
                 import datetime
                 import torch.distributed as dist
                 dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
-            return run_batch(args, torch, G, dev)
+            return (run_batch if args.workload == "batch" else run_screen)(args, torch, G, dev)
         if env_int("RANK", 0) != 0:
             return 0
-        return {"screen": run_screen, "adjoint": run_adjoint}[args.workload](args, torch, G, dev)
+        return run_adjoint(args, torch, G, dev)
 
     import torch
     import torch.distributed as dist

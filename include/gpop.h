@@ -293,6 +293,10 @@ gpop_status gpop_ca_create_external(gpop_ctx* ctx, double h, int64_t n, const do
  * runs the screen over them (UpdateClosestApproachKernel, closest_approach.cu:138-146). */
 gpop_status gpop_ca_append(gpop_ca* ca, int32_t steps, const double* r_dev, const double* v_dev,
     const double* a_dev);
+/* No counterpart in the reference. Sizes the trajectory store for total_steps steps in all, so
+ * that later gpop_ca_propagate / gpop_ca_append calls up to that many steps neither reallocate
+ * nor copy it (without it, appends grow the store by doubling). */
+gpop_status gpop_ca_reserve(gpop_ca* ca, int32_t total_steps);
 /* ClosestApproach::Propagate (closest_approach.cu:129-157): steps more steps; running minima
  * persist across calls. */
 gpop_status gpop_ca_propagate(gpop_ca* ca, int32_t steps);
@@ -306,6 +310,14 @@ gpop_status gpop_ca_find(gpop_ca* ca, double threshold_m, gpop_ca_record* out, i
 gpop_status gpop_ca_pairs(gpop_ca* ca, double* dist, double* time, double* pos_a, double* pos_b,
     uint32_t* closest_step);
 int64_t gpop_ca_num_pairs(const gpop_ca* ca);
+/* No counterpart in the reference (one process per GPU for the screen). Narrows this object to
+ * the pairs whose first object lies in rows [row_begin, row_end): the screen, the refinement,
+ * gpop_ca_find and gpop_ca_pairs then cover only those pairs, a contiguous range of the pair
+ * order, and gpop_ca_pairs fills only that range of its num_pairs-long arrays. begin and end are
+ * multiples of 64 (the screen's tile) or n. Only before the first propagate or append. */
+gpop_status gpop_ca_set_rows(gpop_ca* ca, int64_t row_begin, int64_t row_end);
+/* [pair_begin, pair_end): the pair indices this object screens (all pairs by default). */
+gpop_status gpop_ca_pair_range(const gpop_ca* ca, int64_t* pair_begin, int64_t* pair_end);
 /* Device trajectory of the propagated phases ([steps][3][n] SoA), for inspection and tests. */
 gpop_status gpop_ca_trajectory(gpop_ca* ca, double* r_host, double* v_host, double* a_host,
     int32_t* steps_out);

@@ -561,6 +561,7 @@ public:
         if (_ca)
             gpop_ca_destroy(_ca);
         _ca = nullptr;
+        _steps = 0;
         const int64_t n = (int64_t)positions.size();
         if (_model) {
             _ctx = _model->context(7);
@@ -608,9 +609,11 @@ public:
         }
         if (numSteps <= 0)
             throw std::invalid_argument("ClosestApproach: number of steps must be positive");
-        // a new propagator from the current state for every phase
+        // a new propagator from the current state for every phase; the store is sized once for
+        // the phase's steps, which are screened one at a time
+        gpop_cpp::check(_ctx, gpop_ca_reserve(_ca, _steps + numSteps), "ClosestApproach::Propagate");
         GpuPropagator prop(_dr.p, _dv.p, (unsigned)_set.size(), nullptr, _h, _params, *_any, numSteps);
-        for (int step = 0; step < numSteps; ++step) {
+        for (int step = 0; step < numSteps; ++step, ++_steps) {
             prop.Step(nullptr, nullptr, _da.p);
             gpop_cpp::check(_ctx, gpop_ca_append(_ca, 1, _dr.p, _dv.p, _da.p), "ClosestApproach::Propagate");
         }
@@ -649,6 +652,7 @@ private:
     gpop_ctx* _own = nullptr; // the context of the per-evaluation path
     gpop_ca* _ca = nullptr;
     std::vector<uint32_t> _set;
+    int _steps = 0; // steps screened so far (per-evaluation path)
     gpop_cpp::DevArray _dr, _dv, _da;
 };
 

@@ -36,7 +36,7 @@ EXPORTS = (
     "gpop_startup_init", "gpop_startup_correct", "gpop_gj8_predict", "gpop_gj8_correct",
     "gpop_matrix_column", "gpop_gj8_coefficients", "gpop_gravity", "gpop_frame_matrices",
     "gpop_ca_create", "gpop_ca_create_analytic", "gpop_ca_create_external", "gpop_ca_append", "gpop_ca_propagate", "gpop_ca_find", "gpop_ca_pairs", "gpop_ca_num_pairs",
-    "gpop_ca_trajectory", "gpop_ca_device_seconds", "gpop_ca_destroy",
+    "gpop_ca_set_rows", "gpop_ca_pair_range", "gpop_ca_reserve", "gpop_ca_trajectory", "gpop_ca_device_seconds", "gpop_ca_destroy",
 )
 
 
@@ -120,10 +120,15 @@ def load_library(path=LIB_PATH):
         "gpop_frame_matrices": (i32, [_VP, C.POINTER(Time), f64, i32, i32, i32, _VP, _VP, _VP]),
         "gpop_ca_create": (i32, [_VP, C.POINTER(Time), f64, i64, _VP, _VP, _VP, C.POINTER(_VP)]),
         "gpop_ca_create_analytic": (i32, [_VP, i32, f64, i64, _VP, _VP, _VP, C.POINTER(_VP)]),
+        "gpop_ca_create_external": (i32, [_VP, f64, i64, _VP, _VP, _VP, C.POINTER(_VP)]),
+        "gpop_ca_append": (i32, [_VP, i32, _VP, _VP, _VP]),
         "gpop_ca_propagate": (i32, [_VP, i32]),
         "gpop_ca_find": (i32, [_VP, f64, _VP, i64, C.POINTER(i64)]),
         "gpop_ca_pairs": (i32, [_VP] * 6),
         "gpop_ca_num_pairs": (i64, [_VP]),
+        "gpop_ca_set_rows": (i32, [_VP, i64, i64]),
+        "gpop_ca_reserve": (i32, [_VP, i32]),
+        "gpop_ca_pair_range": (i32, [_VP, C.POINTER(i64), C.POINTER(i64)]),
         "gpop_ca_trajectory": (i32, [_VP] * 4 + [C.POINTER(i32)]),
         "gpop_ca_device_seconds": (i32, [_VP, _VP]),
         "gpop_ca_destroy": (None, [_VP]),
@@ -190,6 +195,7 @@ class Context:
             raise GpopError(st, msg)
         self.device = device
         self.precision = precision
+        self.flags = flags
 
     def close(self):
         if getattr(self, "_h", None):
@@ -438,8 +444,13 @@ class ClosestApproach:
         if ids.shape[0] != r.shape[0]:
             raise GpopError(1, "set_ids size mismatch")
         out = _VP()
-        k = FORCE[kind] if isinstance(kind, str) else kind
-        if k == 0:
+        k = -1 if kind == "external" else FORCE[kind] if isinstance(kind, str) else kind
+        if k == -1:
+            # trajectory supplied by append() (per-evaluation path, sharded screen)
+            ctx._check(lib.gpop_ca_create_external(ctx._h, float(h), r.shape[0],
+                                                   r.ctypes.data_as(_VP), v.ctypes.data_as(_VP),
+                                                   ids.ctypes.data_as(_VP), C.byref(out)))
+        elif k == 0:
             ctx._check(lib.gpop_ca_create(ctx._h, C.byref(as_time(start)), float(h), r.shape[0],
                                           r.ctypes.data_as(_VP), v.ctypes.data_as(_VP),
                                           ids.ctypes.data_as(_VP), C.byref(out)))
@@ -467,6 +478,28 @@ class ClosestApproach:
 
     def propagate(self, steps):
         self.ctx._check(load_library().gpop_ca_propagate(self._h, int(steps)))
+
+    def append(self, steps, r, v, a):
+        """Screens `steps` more steps of an external object: device tensors [steps][n][3]."""
+        for t in (r, v, a):
+            if tuple(t.shape) != (int(steps), self.n, 3) or not t.is_contiguous():
+                raise GpopError(1, "append wants contiguous [steps][n][3] device arrays")
+        self.ctx._check(load_library().gpop_ca_append(self._h, int(steps), _dptr(r), _dptr(v),
+                                                      _dptr(a)))
+
+    def reserve(self, total_steps):
+        """Sizes the trajectory store for total_steps steps in all (no regrowth up to there)."""
+        self.ctx._check(load_library().gpop_ca_reserve(self._h, int(total_steps)))
+
+    def set_rows(self, begin, end):
+        """Screen and refine only the pairs whose first object is in rows [begin, end)."""
+        self.ctx._check(load_library().gpop_ca_set_rows(self._h, int(begin), int(end)))
+
+    @property
+    def pair_range(self):
+        lo, hi = C.c_int64(), C.c_int64()
+        self.ctx._check(load_library().gpop_ca_pair_range(self._h, C.byref(lo), C.byref(hi)))
+        return lo.value, hi.value
 
     def find(self, threshold=-1.0):
         lib = load_library()

@@ -23,6 +23,10 @@ struct gpop_ca {
     std::vector<uint32_t> set_offsets, num_higher;
     std::vector<uint64_t> map_offsets;
     int num_tiles = 0;
+    // rows (first objects) whose pairs this object screens and refines, and their pair range;
+    // all of them unless gpop_ca_set_rows narrowed it
+    int64_t row_lo = 0, row_hi = 0;
+    int64_t pair_lo = 0, pair_hi = 0;
     DevBuf r, v, bound, base, tiles, min_d2, min_step, so, nh, mo;
     // trajectory store [step][3][n] for r, v and the exported acceleration
     DevBuf traj_r, traj_v, traj_a;
@@ -45,6 +49,8 @@ struct gpop_ca {
 };
 
 namespace {
+
+constexpr int kTile = 64; // rows and columns of a screen tile (screen_kernel's block)
 
 __global__ void gather_kernel(const int64_t* idx, int64_t count, const double* dist, const double* time,
     const double* pa, const double* pb, double* out)
@@ -72,6 +78,36 @@ void pair_objects(const gpop_ca* ca, uint64_t idx, uint32_t& a, uint32_t& b)
     b = (uint32_t)(rel % ca->num_higher[s]) + ca->set_offsets[s + 1];
 }
 
+// Number of pairs whose first object precedes object a (GetPartitionMapIdx of (a, first b)).
+int64_t pairs_before(const gpop_ca* ca, int64_t a)
+{
+    if (a >= ca->n)
+        return (int64_t)ca->num_pairs;
+    auto it = std::upper_bound(ca->set_offsets.begin(), ca->set_offsets.end(), (uint32_t)a);
+    const size_t s = (size_t)(it - ca->set_offsets.begin()) - 1;
+    if (s + 1 >= ca->num_sets)
+        return (int64_t)ca->num_pairs;
+    return (int64_t)(ca->map_offsets[s] + (uint64_t)(a - ca->set_offsets[s]) * ca->num_higher[s]);
+}
+
+// Tiles of the (a, b) staircase with a0 in [row_lo, row_hi), b-major (the screen's work list).
+std::vector<int2> staircase_tiles(const gpop_ca* ca, int64_t row_lo, int64_t row_hi)
+{
+    const int64_t n = ca->n;
+    std::vector<int> bound;
+    for (int64_t a0 = row_lo; a0 < row_hi; a0 += kTile) {
+        auto it = std::upper_bound(ca->set_offsets.begin(), ca->set_offsets.end(), (uint32_t)a0);
+        const size_t s = (size_t)(it - ca->set_offsets.begin()) - 1;
+        bound.push_back(s + 1 >= ca->num_sets ? (int)n : (int)ca->set_offsets[s + 1]);
+    }
+    std::vector<int2> tiles;
+    for (int64_t b0 = 0; b0 < n; b0 += kTile)
+        for (size_t t = 0; t < bound.size(); ++t)
+            if (bound[t] < n && b0 + kTile > bound[t])
+                tiles.push_back(make_int2((int)(row_lo + (int64_t)t * kTile), (int)b0));
+    return tiles;
+}
+
 gpop_status refine(gpop_ca* ca, cudaStream_t s)
 {
     gpop_ctx* ctx = ca->ctx;
@@ -85,6 +121,8 @@ gpop_status refine(gpop_ca* ca, cudaStream_t s)
     RefineArgs a;
     a.n = ca->n;
     a.num_pairs = (int64_t)P;
+    a.pair_lo = ca->pair_lo;
+    a.pair_hi = ca->pair_hi;
     a.num_sets = (int)ca->num_sets;
     a.set_offsets = ca->so.as<uint32_t>();
     a.num_higher = ca->nh.as<uint32_t>();
@@ -132,27 +170,24 @@ __global__ void append_rows_kernel(int64_t n, int64_t count, const double* __res
     }
 }
 
-// Grows the trajectory store to `need` steps, keeping the rows already written.
-gpop_status grow_store(gpop_ca* ca, int need)
+// Replaces the trajectory store by one of `cap` steps, keeping the rows already written.
+cudaError_t resize_store(gpop_ca* ca, int cap)
 {
-    gpop_ctx* ctx = ca->ctx;
-    if (need <= ca->cap_steps)
-        return GPOP_OK;
     const size_t row = (size_t)ca->n * 3 * sizeof(double);
     DevBuf nr, nv, na;
     cudaError_t e;
-    if ((e = nr.ensure(row * need)) != cudaSuccess || (e = nv.ensure(row * need)) != cudaSuccess
-        || (e = na.ensure(row * need)) != cudaSuccess) {
+    if ((e = nr.ensure(row * cap)) == cudaSuccess && (e = nv.ensure(row * cap)) == cudaSuccess
+        && (e = na.ensure(row * cap)) == cudaSuccess && ca->total_steps > 0) {
+        const size_t used = row * ca->total_steps;
+        if ((e = cudaMemcpy(nr.p, ca->traj_r.p, used, cudaMemcpyDeviceToDevice)) == cudaSuccess
+            && (e = cudaMemcpy(nv.p, ca->traj_v.p, used, cudaMemcpyDeviceToDevice)) == cudaSuccess)
+            e = cudaMemcpy(na.p, ca->traj_a.p, used, cudaMemcpyDeviceToDevice);
+    }
+    if (e != cudaSuccess) {
         nr.release();
         nv.release();
         na.release();
-        return fail(ctx, GPOP_ERR_NOMEM, "trajectory store (" + std::to_string(3 * row * need >> 20) + " MiB)");
-    }
-    if (ca->total_steps > 0) {
-        const size_t used = row * ca->total_steps;
-        cudaMemcpy(nr.p, ca->traj_r.p, used, cudaMemcpyDeviceToDevice);
-        cudaMemcpy(nv.p, ca->traj_v.p, used, cudaMemcpyDeviceToDevice);
-        cudaMemcpy(na.p, ca->traj_a.p, used, cudaMemcpyDeviceToDevice);
+        return e;
     }
     ca->traj_r.release();
     ca->traj_v.release();
@@ -161,8 +196,27 @@ gpop_status grow_store(gpop_ca* ca, int need)
     ca->traj_v = nv;
     ca->traj_a = na;
     nr.p = nv.p = na.p = nullptr;
-    ca->cap_steps = need;
-    return GPOP_OK;
+    ca->cap_steps = cap;
+    return cudaSuccess;
+}
+
+// Grows the trajectory store to hold `need` steps. With `amortized` (steps appended a few at a
+// time by a caller that reserved nothing) it first tries twice the present capacity, so that
+// appends copy the store O(log steps) times instead of once per call.
+gpop_status grow_store(gpop_ca* ca, int need, bool amortized = false)
+{
+    if (need <= ca->cap_steps)
+        return GPOP_OK;
+    if (amortized && ca->cap_steps > 0 && 2LL * ca->cap_steps > need && 2LL * ca->cap_steps <= INT32_MAX) {
+        if (resize_store(ca, 2 * ca->cap_steps) == cudaSuccess)
+            return GPOP_OK;
+        cudaGetLastError(); // out of memory for the doubled store: try the exact size
+    }
+    const cudaError_t e = resize_store(ca, need);
+    if (e == cudaErrorMemoryAllocation)
+        return fail(ca->ctx, GPOP_ERR_NOMEM,
+            "trajectory store (" + std::to_string((size_t)ca->n * 72 * need >> 20) + " MiB)");
+    return e == cudaSuccess ? GPOP_OK : cuda_fail(ca->ctx, e, "growing the trajectory store");
 }
 
 // UpdateClosestApproachKernel over steps [total_steps, need) of the store (running minima).
@@ -253,13 +307,10 @@ gpop_status gpop_ca_create(gpop_ctx* ctx, const gpop_time* start, double h, int6
                 - (int64_t)ca->set_offsets[s + 1];
         }
     }
-    std::vector<int2> tiles;
-    const int T = 64;
-    for (int64_t b0 = 0; b0 < n; b0 += T)
-        for (int64_t a0 = 0; a0 < n; a0 += T)
-            if (bound[a0] < n && b0 + T > bound[a0])
-                tiles.push_back(make_int2((int)a0, (int)b0));
+    const std::vector<int2> tiles = staircase_tiles(ca, 0, n);
     ca->num_tiles = (int)tiles.size();
+    ca->row_hi = n;
+    ca->pair_hi = (int64_t)ca->num_pairs;
     cudaError_t e = cudaSetDevice(ctx->cfg.device);
     const size_t P = ca->num_pairs;
     if (e != cudaSuccess || (e = ca->r.ensure(n * 24)) != cudaSuccess || (e = ca->v.ensure(n * 24)) != cudaSuccess
@@ -331,7 +382,7 @@ gpop_status gpop_ca_append(gpop_ca* ca, int32_t steps, const double* r_dev, cons
         return cuda_fail(ctx, e, "cudaSetDevice");
     cudaStream_t s = nullptr;
     const int need = ca->total_steps + steps;
-    gpop_status st = grow_store(ca, need);
+    gpop_status st = grow_store(ca, need, true);
     if (st != GPOP_OK)
         return st;
     const size_t off = (size_t)ca->total_steps * 3 * ca->n;
@@ -355,6 +406,53 @@ gpop_status gpop_ca_append(gpop_ca* ca, int32_t steps, const double* r_dev, cons
 }
 
 int64_t gpop_ca_num_pairs(const gpop_ca* ca) { return ca ? (int64_t)ca->num_pairs : -1; }
+
+gpop_status gpop_ca_reserve(gpop_ca* ca, int32_t total_steps)
+{
+    if (!ca)
+        return GPOP_ERR_INVALID_ARG;
+    if (total_steps < 0)
+        return fail(ca->ctx, GPOP_ERR_INVALID_ARG, "negative step count");
+    cudaError_t e = cudaSetDevice(ca->ctx->cfg.device);
+    if (e != cudaSuccess)
+        return cuda_fail(ca->ctx, e, "cudaSetDevice");
+    return grow_store(ca, total_steps);
+}
+
+gpop_status gpop_ca_set_rows(gpop_ca* ca, int64_t row_begin, int64_t row_end)
+{
+    if (!ca)
+        return GPOP_ERR_INVALID_ARG;
+    gpop_ctx* ctx = ca->ctx;
+    if (ca->total_steps != 0)
+        return fail(ctx, GPOP_ERR_STATE, "gpop_ca_set_rows after the first propagation");
+    if (row_begin < 0 || row_end > ca->n || row_end < row_begin
+        || (row_begin % kTile != 0 && row_begin != ca->n) || (row_end % kTile != 0 && row_end != ca->n))
+        return fail(ctx, GPOP_ERR_INVALID_ARG,
+            "rows must satisfy 0 <= begin <= end <= n with begin and end multiples of 64 or n");
+    const std::vector<int2> tiles = staircase_tiles(ca, row_begin, row_end);
+    cudaError_t e = cudaSetDevice(ctx->cfg.device);
+    if (e == cudaSuccess && (e = ca->tiles.ensure(std::max<size_t>(1, tiles.size()) * sizeof(int2))) == cudaSuccess
+        && !tiles.empty())
+        e = cudaMemcpy(ca->tiles.p, tiles.data(), tiles.size() * sizeof(int2), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess)
+        return cuda_fail(ctx, e, "screen tiles");
+    ca->num_tiles = (int)tiles.size();
+    ca->row_lo = row_begin;
+    ca->row_hi = row_end;
+    ca->pair_lo = pairs_before(ca, row_begin);
+    ca->pair_hi = std::max(ca->pair_lo, pairs_before(ca, row_end));
+    return GPOP_OK;
+}
+
+gpop_status gpop_ca_pair_range(const gpop_ca* ca, int64_t* pair_begin, int64_t* pair_end)
+{
+    if (!ca || !pair_begin || !pair_end)
+        return GPOP_ERR_INVALID_ARG;
+    *pair_begin = ca->pair_lo;
+    *pair_end = ca->pair_hi;
+    return GPOP_OK;
+}
 
 gpop_status gpop_ca_propagate(gpop_ca* ca, int32_t steps)
 {
@@ -427,7 +525,8 @@ gpop_status gpop_ca_find(gpop_ca* ca, double threshold, gpop_ca_record* out, int
     gpop_status st = refine(ca, s);
     if (st != GPOP_OK)
         return st;
-    const int64_t P = (int64_t)ca->num_pairs;
+    // the pairs of this object's rows (all pairs unless gpop_ca_set_rows narrowed them)
+    const int64_t lo = ca->pair_lo, P = ca->pair_hi - ca->pair_lo;
     std::vector<int64_t> idx;
     cudaError_t e;
     if (threshold < 0.0) {
@@ -437,12 +536,12 @@ gpop_status gpop_ca_find(gpop_ca* ca, double threshold, gpop_ca_record* out, int
         const int64_t k = std::min(P, capacity);
         idx.resize(k);
         for (int64_t i = 0; i < k; ++i)
-            idx[i] = i;
+            idx[i] = lo + i;
     } else {
         if ((e = ca->count.ensure(8)) != cudaSuccess || (e = ca->cand.ensure(std::max<int64_t>(1, P) * 8)) != cudaSuccess)
             return fail(ctx, GPOP_ERR_NOMEM, "candidate list");
         cudaMemsetAsync(ca->count.p, 0, 8, s);
-        if ((e = launch_select(ca->dist.as<double>(), P, threshold, ca->count.as<unsigned long long>(),
+        if ((e = launch_select(ca->dist.as<double>() + lo, P, threshold, ca->count.as<unsigned long long>(),
                  ca->cand.as<int64_t>(), P, s))
             != cudaSuccess)
             return cuda_fail(ctx, e, "select kernel");
@@ -456,6 +555,8 @@ gpop_status gpop_ca_find(gpop_ca* ca, double threshold, gpop_ca_record* out, int
         idx.resize(cnt);
         if (cnt && (e = cudaMemcpy(idx.data(), ca->cand.p, cnt * 8, cudaMemcpyDeviceToHost)) != cudaSuccess)
             return cuda_fail(ctx, e, "candidate list");
+        for (int64_t& i : idx)
+            i += lo;
         std::sort(idx.begin(), idx.end()); // pair order = (object_index1, object_index2) order
         if ((int64_t)idx.size() > capacity)
             idx.resize(capacity);
@@ -508,18 +609,21 @@ gpop_status gpop_ca_pairs(gpop_ca* ca, double* dist, double* time, double* pos_a
     gpop_status st = refine(ca, nullptr);
     if (st != GPOP_OK)
         return st;
-    const size_t P = ca->num_pairs;
+    // entries [pair_lo, pair_hi) of the full-length arrays; the others are left as they are
+    const size_t lo = (size_t)ca->pair_lo, P = (size_t)(ca->pair_hi - ca->pair_lo);
     cudaError_t e = cudaSuccess;
+    if (P == 0)
+        return GPOP_OK;
     if (dist && e == cudaSuccess)
-        e = cudaMemcpy(dist, ca->dist.p, P * 8, cudaMemcpyDeviceToHost);
+        e = cudaMemcpy(dist + lo, ca->dist.as<double>() + lo, P * 8, cudaMemcpyDeviceToHost);
     if (time && e == cudaSuccess)
-        e = cudaMemcpy(time, ca->time.p, P * 8, cudaMemcpyDeviceToHost);
+        e = cudaMemcpy(time + lo, ca->time.as<double>() + lo, P * 8, cudaMemcpyDeviceToHost);
     if (pos_a && e == cudaSuccess)
-        e = cudaMemcpy(pos_a, ca->pos_a.p, P * 24, cudaMemcpyDeviceToHost);
+        e = cudaMemcpy(pos_a + 3 * lo, ca->pos_a.as<double>() + 3 * lo, P * 24, cudaMemcpyDeviceToHost);
     if (pos_b && e == cudaSuccess)
-        e = cudaMemcpy(pos_b, ca->pos_b.p, P * 24, cudaMemcpyDeviceToHost);
+        e = cudaMemcpy(pos_b + 3 * lo, ca->pos_b.as<double>() + 3 * lo, P * 24, cudaMemcpyDeviceToHost);
     if (closest_step && e == cudaSuccess)
-        e = cudaMemcpy(closest_step, ca->min_step.p, P * 4, cudaMemcpyDeviceToHost);
+        e = cudaMemcpy(closest_step + lo, ca->min_step.as<uint32_t>() + lo, P * 4, cudaMemcpyDeviceToHost);
     return e == cudaSuccess ? GPOP_OK : cuda_fail(ctx, e, "copying pair results");
 }
 

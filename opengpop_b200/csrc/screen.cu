@@ -106,8 +106,8 @@ __global__ void __launch_bounds__(256) screen_kernel(ScreenArgs a)
 
 __global__ void __launch_bounds__(128) refine_kernel(RefineArgs a)
 {
-    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= a.num_pairs)
+    const int64_t idx = a.pair_lo + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= a.pair_hi)
         return;
     // pair index -> (a, b): binary search of the set whose map range holds idx
     // (inverse of PartitionParameters::GetPartitionMapIdx, partition_parameters.cuh:50-91)
@@ -200,9 +200,9 @@ cudaError_t launch_screen(const ScreenArgs& a, int num_tiles, cudaStream_t s)
 
 cudaError_t launch_refine(const RefineArgs& a, cudaStream_t s)
 {
-    if (a.num_pairs <= 0)
+    if (a.pair_lo < 0 || a.pair_hi > a.num_pairs || a.pair_hi <= a.pair_lo)
         return cudaSuccess;
-    const int64_t blocks = (a.num_pairs + 127) / 128;
+    const int64_t blocks = (a.pair_hi - a.pair_lo + 127) / 128;
     refine_kernel<<<(unsigned)blocks, 128, 0, s>>>(a);
     return cudaGetLastError();
 }

@@ -21,6 +21,7 @@ struct ScreenArgs {
 struct RefineArgs {
     int64_t n = 0;
     int64_t num_pairs = 0;
+    int64_t pair_lo = 0, pair_hi = 0; // pairs refined by this launch: [pair_lo, pair_hi)
     int num_sets = 0;
     const uint32_t* set_offsets = nullptr;
     const uint32_t* num_higher = nullptr;
