@@ -510,6 +510,8 @@ class ClosestApproach:
         return [recs[i] for i in range(cnt.value)]
 
     def pairs(self):
+        """Per-pair results in the reference's pair order (num_pairs entries); after set_rows only
+        the entries of pair_range are filled, the others stay zero."""
         P = self.num_pairs
         d = np.zeros(P)
         t = np.zeros(P)

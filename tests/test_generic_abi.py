@@ -77,3 +77,20 @@ def test_coefficients_without_buffers(lib):
     f.restype = C.c_int32
     f.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     assert f(None, None, None, None) == OK
+
+
+def test_closest_approach_row_calls_without_object(lib):
+    # the sharded screen's entry points reject a missing object before any CUDA call
+    rows = lib.gpop_ca_set_rows
+    rows.restype = C.c_int32
+    rows.argtypes = [C.c_void_p, C.c_int64, C.c_int64]
+    assert rows(None, 0, 64) == INVALID
+    rng = lib.gpop_ca_pair_range
+    rng.restype = C.c_int32
+    rng.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+    lo, hi = C.c_int64(), C.c_int64()
+    assert rng(None, C.byref(lo), C.byref(hi)) == INVALID
+    res = lib.gpop_ca_reserve
+    res.restype = C.c_int32
+    res.argtypes = [C.c_void_p, C.c_int32]
+    assert res(None, 100) == INVALID
