@@ -178,6 +178,11 @@ def closest_approach_sharded(ctx, start, h, r, v, set_ids, phases, threshold=-1.
     r = np.ascontiguousarray(r, dtype=np.float64).reshape(-1, 3)
     v = np.ascontiguousarray(v, dtype=np.float64).reshape(-1, 3)
     n = r.shape[0]
+    phases = [int(p) for p in phases]
+    if not phases or min(phases) <= 0:
+        raise ValueError("every phase needs a positive number of steps")
+    if v.shape[0] != n or len(set_ids) != n:
+        raise ValueError("positions, velocities and set ids differ in length")
     shards = object_shards(n, world)
     o0, o1 = shards[rank]
     m, m_max = o1 - o0, max(e - s for s, e in shards)

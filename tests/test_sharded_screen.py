@@ -119,6 +119,16 @@ def test_fake_job_checksums_the_trajectory():
         assert d == pytest.approx(want, rel=1e-12)
 
 
+def test_sharded_job_rejects_bad_phases():
+    import sharded_screen_worker as W
+    ids = _dense(np.array([0, 0, 1, 1]))
+    for phases in ([], [3, 0], [-1]):
+        with pytest.raises(ValueError):
+            W.fake_job(4, ids, phases, 2)
+    with pytest.raises(ValueError):
+        W.fake_job(4, ids[:3], [2], 2)
+
+
 # ---- GPU ----
 
 def _fused(n, seed, phases, threshold):
