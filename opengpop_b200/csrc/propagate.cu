@@ -360,9 +360,10 @@ __global__ void __launch_bounds__(K == 1 ? kOneObjectBlock : 256, 1) gj8_kernel(
 // Same step as gj8_kernel; the P lanes of a group split the gravity columns of its K objects
 // (lanes.cuh, lane-layout table) and hold identical state; lane 0 of the group stores. Object k
 // of group g is g + k * (groups in the grid). Used when the objects alone leave most warp slots of
-// the GPU empty.
-template <bool MIXED, int K>
-__global__ void __launch_bounds__(K == 1 ? 512 : 256, 1) gj8_lanes_kernel(TableSrc ts, PropArgs a, int P)
+// the GPU empty. MAXT bounds the block (and so the registers a thread may hold): 512 for the many
+// lanes of few objects, 384 for two lanes per object, which then keeps its table loads in flight.
+template <bool MIXED, int K, int MAXT = (K == 1 ? 512 : 256)>
+__global__ void __launch_bounds__(MAXT, 1) gj8_lanes_kernel(TableSrc ts, PropArgs a, int P)
 {
     extern __shared__ __align__(128) uint8_t smem[];
     GravSmem g;
@@ -690,6 +691,11 @@ static cudaError_t launch_gj8_f(F f, const TableSrc& ts, const PropArgs& a, int 
     return launch_gj8_k<F, 1>(f, ts, a, num_sms, s, block_override);
 }
 
+#ifndef GPOP_LANES_BLOCK_MID
+#define GPOP_LANES_BLOCK_MID 384
+#endif
+constexpr int kLanesBlockMid = GPOP_LANES_BLOCK_MID; // blocks up to this size take the MAXT = 384 kernel
+
 int lanes_per_object(int64_t n, int num_sms)
 {
     int P = 1; // the most lanes that keep every object in one wave of 512-thread blocks
@@ -708,15 +714,21 @@ cudaError_t launch_gj8(const TableSrc& ts, const PropArgs& a, int num_sms, cudaS
     // 35.3 against 57.2 / 34.3 with two lanes per pair; 37,000: 120 / 64 against 104 / 62), except
     // that FP64 takes one object per thread up to 256 objects per SM, where two objects per thread
     // leave at most one warp per scheduler (20,000 objects: 40.0 against 35.3; 30,000: 57.2 against
-    // 52.7; 37,000: 65.1 against 64.5); two lanes per pair of objects from 112 to 128 per SM, where
+    // 52.7; 37,000: 65.1 against 64.5), and up to 192 per SM two lanes per object in blocks of at
+    // most 384 threads (20,000: 42.0 against 39.1 with one object per thread; 24,000: 50.0 against
+    // 46.4; 28,000: 57.7 against 54.1); two lanes per pair of objects from 112 to 128 per SM, where
     // they fill the four schedulers with one warp each (18,944 objects: 67.7 / 41.2 against 63.3 /
     // 33.6 with two objects per thread); below, 2 or more lanes per object (9,472 objects: 48.2 /
     // 31.0 against 34.0 / 20.8). One or two objects per thread when no lane-layout table is at hand.
     if (walk <= 0) {
         const bool lanes = lane_ts && a.kind == 0;
         const bool fp64_gravity = a.kind == 0 && !ts.mixed;
-        if (a.n > (int64_t)num_sms * 128 || (!lanes && a.n >= (int64_t)num_sms * 128))
-            walk = fp64_gravity && a.n <= (int64_t)num_sms * 256 ? kWalkOneObject : kWalkTwoObjects;
+        if (a.n > (int64_t)num_sms * 128 || (!lanes && a.n >= (int64_t)num_sms * 128)) {
+            if (fp64_gravity && lanes && 2 * a.n <= (int64_t)num_sms * kLanesBlockMid)
+                walk = kWalkLanes; // lanes_per_object gives 2 here: one block of <= 384 per SM
+            else
+                walk = fp64_gravity && a.n <= (int64_t)num_sms * 256 ? kWalkOneObject : kWalkTwoObjects;
+        }
         else if (a.n >= (int64_t)num_sms * 112)
             walk = kWalkLanesTwo;
         else
@@ -735,7 +747,11 @@ cudaError_t launch_gj8(const TableSrc& ts, const PropArgs& a, int num_sms, cudaS
         const size_t smem = table_smem_bytes(lt);
         cudaError_t e;
         if (lt.mixed) {
-            if (K == 1) {
+            if (K == 1 && block <= kLanesBlockMid) {
+                if ((e = set_smem(gj8_lanes_kernel<true, 1, kLanesBlockMid>, smem)) != cudaSuccess)
+                    return e;
+                gj8_lanes_kernel<true, 1, kLanesBlockMid><<<grid, block, smem, s>>>(lt, a, P);
+            } else if (K == 1) {
                 if ((e = set_smem(gj8_lanes_kernel<true, 1>, smem)) != cudaSuccess)
                     return e;
                 gj8_lanes_kernel<true, 1><<<grid, block, smem, s>>>(lt, a, P);
@@ -745,7 +761,11 @@ cudaError_t launch_gj8(const TableSrc& ts, const PropArgs& a, int num_sms, cudaS
                 gj8_lanes_kernel<true, 2><<<grid, block, smem, s>>>(lt, a, P);
             }
         } else {
-            if (K == 1) {
+            if (K == 1 && block <= kLanesBlockMid) {
+                if ((e = set_smem(gj8_lanes_kernel<false, 1, kLanesBlockMid>, smem)) != cudaSuccess)
+                    return e;
+                gj8_lanes_kernel<false, 1, kLanesBlockMid><<<grid, block, smem, s>>>(lt, a, P);
+            } else if (K == 1) {
                 if ((e = set_smem(gj8_lanes_kernel<false, 1>, smem)) != cudaSuccess)
                     return e;
                 gj8_lanes_kernel<false, 1><<<grid, block, smem, s>>>(lt, a, P);
