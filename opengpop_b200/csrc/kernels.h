@@ -66,10 +66,11 @@ size_t max_smem_optin();
 cudaError_t launch_startup(const TableSrc& ts, const PropArgs& a, int num_sms, cudaStream_t s);
 // How many objects a GJ8 thread carries through the gravity triangle walk (0 = by problem size).
 // kWalkLanes: P lanes per object split the gravity columns (few objects; P from lanes_per_object).
-// kWalkLanesTwo: two lanes per group of two objects.
+// kWalkLanesTwo: two lanes per group of two objects (only when forced; the default walks take
+// kWalkLanes where they would have taken it).
 enum WalkMode : int { kWalkOneObject = 1, kWalkTwoObjects = 2, kWalkLanes = 3, kWalkLanesTwo = 4 };
-// Lanes per object (1..32, a power of 2): the most that keep n objects in one wave of 512-thread
-// blocks, one per SM.
+// Lanes per object (1..32, a power of 2): the most that keep n objects in one wave of blocks of at
+// most 384 threads, one per SM.
 int lanes_per_object(int64_t n, int num_sms);
 // lane_ts: the lane-layout table of the same precision (NULL: no lane-split walk).
 cudaError_t launch_gj8(const TableSrc& ts, const PropArgs& a, int num_sms, cudaStream_t s,

@@ -696,10 +696,15 @@ static cudaError_t launch_gj8_f(F f, const TableSrc& ts, const PropArgs& a, int 
 #endif
 constexpr int kLanesBlockMid = GPOP_LANES_BLOCK_MID; // blocks up to this size take the MAXT = 384 kernel
 
+// The most lanes that keep every object in one wave of blocks of at most kLanesBlockMid threads,
+// so that the lane kernel runs with the registers of its 384-thread variant: fewer lanes with
+// more registers beat more lanes with 128 (B200, 70x70, FP64 / mixed M object-steps/s: 2,048
+// objects 19.0 / 26.1 against 16.2 / 21.2 with 512-thread blocks; 4,096: 25.6 / 36.1 against
+// 21.8 / 33.6; 9,472: 31.6 / 49.4 against 29.6 / 46.5; 16,000: 42.2 / 63.7 against 30.2 / 53.1).
 int lanes_per_object(int64_t n, int num_sms)
 {
-    int P = 1; // the most lanes that keep every object in one wave of 512-thread blocks
-    while (P < 32 && n * 2 * P <= (int64_t)num_sms * 512)
+    int P = 1;
+    while (P < 32 && n * 2 * P <= (int64_t)num_sms * kLanesBlockMid)
         P *= 2;
     return P;
 }
@@ -709,30 +714,27 @@ cudaError_t launch_gj8(const TableSrc& ts, const PropArgs& a, int num_sms, cudaS
 {
     if (a.n <= 0 || a.step_end <= a.step_begin)
         return cudaSuccess;
-    // Default walk (measured on B200 at 70x70, LEO objects, mixed / FP64 M object-steps/s with the
-    // two-column walk): two objects per thread above 128 objects per SM (20,000 objects: 66.5 /
-    // 35.3 against 57.2 / 34.3 with two lanes per pair; 37,000: 120 / 64 against 104 / 62), except
-    // that FP64 takes one object per thread up to 256 objects per SM, where two objects per thread
-    // leave at most one warp per scheduler (20,000 objects: 40.0 against 35.3; 30,000: 57.2 against
-    // 52.7; 37,000: 65.1 against 64.5), and up to 192 per SM two lanes per object in blocks of at
-    // most 384 threads (20,000: 42.0 against 39.1 with one object per thread; 24,000: 50.0 against
-    // 46.4; 28,000: 57.7 against 54.1); two lanes per pair of objects from 112 to 128 per SM, where
-    // they fill the four schedulers with one warp each (18,944 objects: 67.7 / 41.2 against 63.3 /
-    // 33.6 with two objects per thread); below, 2 or more lanes per object (9,472 objects: 48.2 /
-    // 31.0 against 34.0 / 20.8). One or two objects per thread when no lane-layout table is at hand.
+    // Default walk (measured on B200 at 70x70, LEO objects, mixed / FP64 M object-steps/s):
+    // - up to 128 objects per SM, lanes (P from lanes_per_object, blocks of at most 384 threads):
+    //   18,900 objects 74.7 / 49.4 against 65.0 / 47.0 with two lanes per pair of objects; 9,472:
+    //   49.4 / 31.6 against 34.0 / 20.8 with two objects per thread;
+    // - FP64 up to 192 per SM keeps two lanes per object (20,000: 42.0 against 39.1 with one object
+    //   per thread; 24,000: 50.0 against 46.4; 28,000: 57.7 against 54.1);
+    // - above, two objects per thread (20,000 mixed: 64.5 against 63.7 with two lanes per object;
+    //   37,000: 120 / 64 against 104 / 62 with two lanes per pair), except that FP64 takes one
+    //   object per thread up to 256 per SM, where two objects per thread leave at most one warp
+    //   per scheduler (30,000: 57.2 against 52.7; 37,000: 65.1 against 64.5).
+    // One or two objects per thread when no lane-layout table is at hand.
     if (walk <= 0) {
         const bool lanes = lane_ts && a.kind == 0;
         const bool fp64_gravity = a.kind == 0 && !ts.mixed;
-        if (a.n > (int64_t)num_sms * 128 || (!lanes && a.n >= (int64_t)num_sms * 128)) {
-            if (fp64_gravity && lanes && 2 * a.n <= (int64_t)num_sms * kLanesBlockMid)
-                walk = kWalkLanes; // lanes_per_object gives 2 here: one block of <= 384 per SM
-            else
-                walk = fp64_gravity && a.n <= (int64_t)num_sms * 256 ? kWalkOneObject : kWalkTwoObjects;
-        }
-        else if (a.n >= (int64_t)num_sms * 112)
-            walk = kWalkLanesTwo;
+        if (lanes
+            && (a.n <= (int64_t)num_sms * 128 || (fp64_gravity && 2 * a.n <= (int64_t)num_sms * kLanesBlockMid)))
+            walk = kWalkLanes;
+        else if (a.n >= (int64_t)num_sms * 128)
+            walk = fp64_gravity && a.n <= (int64_t)num_sms * 256 ? kWalkOneObject : kWalkTwoObjects;
         else
-            walk = lanes ? kWalkLanes : kWalkOneObject;
+            walk = kWalkOneObject;
     }
     if ((walk == kWalkLanes || walk == kWalkLanesTwo) && a.kind == 0 && lane_ts) {
         const TableSrc& lt = *lane_ts;
