@@ -189,48 +189,52 @@ def closest_approach_sharded(ctx, start, h, r, v, set_ids, phases, threshold=-1.
     make_propagator = make_propagator or G.Propagator
     make_ca = make_ca or (lambda *a: G.ClosestApproach(*a, kind="external"))
     ca = make_ca(ctx, start, h, r, v, set_ids)
-    ca.set_rows(*screen_rows(set_ids, world)[rank])
-    ca.reserve(sum(phases))
-    dev = torch.device("cuda", ctx.device) if torch.cuda.is_available() else torch.device("cpu")
-    r_loc = torch.tensor(r[o0:o1], device=dev)
-    v_loc = torch.tensor(v[o0:o1], device=dev)
-    win = max(1, min(int(window), max(phases)))
-    buf = torch.zeros(3 * win * 3 * m_max, dtype=torch.float64, device=dev)
-    timed = dev.type == "cuda"
-    t_prop = t_gather = 0.0
-    done = 0
-    for steps in phases:
-        p = make_propagator(ctx, _phase_start(start, h, done, ctx.flags), h, steps, r_loc, v_loc) if m else None
-        left = steps
-        while left > 0:
-            k = min(win, left)
-            seg = k * 3 * m_max
-            if timed:
-                ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
-                ev[0].record()
-            if p is not None:
-                p.step(k, buf[0: k * 3 * m], buf[seg: seg + k * 3 * m], buf[2 * seg: 2 * seg + k * 3 * m])
-            if timed:
-                ev[1].record()
-            rows = gather_window(buf, k, n)
-            if timed:
-                ev[2].record()
-                ev[2].synchronize()
-                t_prop += ev[0].elapsed_time(ev[1]) / 1e3
-                t_gather += ev[1].elapsed_time(ev[2]) / 1e3
-            ca.append(k, *rows)
-            left -= k
-        if p is not None:
-            p.close()
-        done += steps
-    recs = [(int(x.object_index1), int(x.object_index2), float(x.distance), float(x.time),
-             tuple(x.position_a), tuple(x.position_b)) for x in ca.find(threshold)]
+    try:
+        ca.set_rows(*screen_rows(set_ids, world)[rank])
+        ca.reserve(sum(phases))
+        dev = torch.device("cuda", ctx.device) if torch.cuda.is_available() else torch.device("cpu")
+        r_loc = torch.tensor(r[o0:o1], device=dev)
+        v_loc = torch.tensor(v[o0:o1], device=dev)
+        win = max(1, min(int(window), max(phases)))
+        buf = torch.zeros(3 * win * 3 * m_max, dtype=torch.float64, device=dev)
+        timed = dev.type == "cuda"
+        t_prop = t_gather = 0.0
+        done = 0
+        for steps in phases:
+            p = make_propagator(ctx, _phase_start(start, h, done, ctx.flags), h, steps, r_loc, v_loc) if m else None
+            try:
+                left = steps
+                while left > 0:
+                    k = min(win, left)
+                    seg = k * 3 * m_max
+                    if timed:
+                        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+                        ev[0].record()
+                    if p is not None:
+                        p.step(k, buf[0: k * 3 * m], buf[seg: seg + k * 3 * m], buf[2 * seg: 2 * seg + k * 3 * m])
+                    if timed:
+                        ev[1].record()
+                    rows = gather_window(buf, k, n)
+                    if timed:
+                        ev[2].record()
+                        ev[2].synchronize()
+                        t_prop += ev[0].elapsed_time(ev[1]) / 1e3
+                        t_gather += ev[1].elapsed_time(ev[2]) / 1e3
+                    ca.append(k, *rows)
+                    left -= k
+            finally:
+                if p is not None:
+                    p.close()
+            done += steps
+        recs = [(int(x.object_index1), int(x.object_index2), float(x.distance), float(x.time),
+                 tuple(x.position_a), tuple(x.position_b)) for x in ca.find(threshold)]
+        ds = ca.device_seconds()
+    finally:
+        ca.close()
     if world > 1:
         everyone = [None] * world
         dist.all_gather_object(everyone, recs)
         recs = [x for part in everyone for x in part]
     recs.sort(key=lambda x: (x[0], x[1]))
-    ds = ca.device_seconds()
-    ca.close()
     return recs, {"propagation": t_prop, "exchange": t_gather, "screen": float(ds[1]),
                   "refinement": float(ds[2])}
