@@ -42,6 +42,22 @@ def test_pairs_per_row_brute_force():
         assert np.array_equal(sharding.pairs_per_row(ids), brute)
 
 
+def test_row_pair_ranges_follow_the_partition_map():
+    # the first pair index of every row (the start of a row block's pair range) is the oracle's
+    # PartitionParameters map of (a, first b of a later set)
+    import oracle_api as O
+    from opengpop_b200 import sharding
+    for ids in _set_layouts():
+        ids = _dense(ids)
+        p = O.partition(ids)
+        cum = np.concatenate([[0], np.cumsum(sharding.pairs_per_row(ids))])
+        assert cum[-1] == p["num_pairs"]
+        for s in range(p["num_sets"] - 1):
+            a0, a1 = int(p["set_offsets"][s]), int(p["set_offsets"][s + 1])
+            for a in range(a0, a1):
+                assert cum[a] == int(p["map_offsets"][s]) + (a - a0) * int(p["num_higher"][s])
+
+
 def test_screen_rows_cover_tiles_and_balance():
     from opengpop_b200 import sharding
     for ids in _set_layouts():
