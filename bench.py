@@ -313,9 +313,11 @@ def run_screen(args, torch, G, dev):
     ctx = G.Context(device=dev.index, precision=G.FP64)
     sampler = ClockSampler(torch.cuda.current_device())
     res = []
+    launches0 = 0
     for i in range(args.warmup + args.steps):
         if i == args.warmup:
             sampler.start()
+            launches0 = ctx.kernel_launches
         if world > 1:
             dist.barrier()
         t0 = time.perf_counter()
@@ -336,6 +338,7 @@ def run_screen(args, torch, G, dev):
         if i >= args.warmup:
             res.append((wall, dt))
     clocks = sampler.stop()
+    launches = int(sharding.max_over_ranks(ctx.kernel_launches - launches0, dev))
     ctx.close()
     wall = sharding.max_over_ranks(float(np.mean([x[0] for x in res])), dev)
     t_prop, t_exch, t_screen, t_refine = (sharding.max_over_ranks(float(np.mean([x[1][k] for x in res])), dev)
@@ -370,7 +373,7 @@ def run_screen(args, torch, G, dev):
              "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak64, "unit": "TFLOP/s",
                           "frac": achieved / peak64 if peak64 else None, "traffic": None,
                           "per_unit": "9 FP64 flops per pair-step"},
-             "cpu_baseline": None, "clocks": clocks})
+             "cpu_baseline": None, "clocks": clocks, "gpu_launches": launches})
     return 0
 
 
@@ -384,9 +387,11 @@ def run_adjoint(args, torch, G, dev):
     ctx = G.Context(precision=G.FP64)
     sampler = ClockSampler(torch.cuda.current_device())
     t_miss, t_stm = [], []
+    launches0 = 0
     for i in range(args.warmup + args.steps):
         if i == args.warmup:
             sampler.start()
+            launches0 = ctx.kernel_launches
         t0 = time.perf_counter()
         ctx.miss_gradient(START, H, steps, r, v, pairs)
         t1 = time.perf_counter()
@@ -396,6 +401,7 @@ def run_adjoint(args, torch, G, dev):
             t_miss.append(t1 - t0)
             t_stm.append(t2 - t1)
     clocks = sampler.stop()
+    launches = ctx.kernel_launches - launches0
     ctx.close()
     tm, ts = float(np.mean(t_miss)), float(np.mean(t_stm))
     # work of the miss-gradient call: forward propagation of 2 n_pairs objects, then per unit
@@ -420,7 +426,7 @@ def run_adjoint(args, torch, G, dev):
                           "frac": ach / peak64 if peak64 else None, "traffic": None,
                           "per_unit": "per unit-step 2 (7 W + 500) + W_J, W(70) = %d, "
                                       "W_J(70) = %d flops" % (W, w_jac(DEGREE))},
-             "cpu_baseline": None, "clocks": clocks})
+             "cpu_baseline": None, "clocks": clocks, "gpu_launches": launches})
     return 0
 
 
