@@ -119,6 +119,28 @@ def test_fake_job_two_ranks_equals_one(tmp_path, n, phases, window):
         assert [tuple(x) for x in log] == want
 
 
+def test_fake_job_three_ranks_uneven_shards(tmp_path):
+    # 5 objects over 3 ranks: shards of 2, 2 and 1 objects; every pair once, the same checksums
+    import sharded_screen_worker as W
+    n, phases = 5, [3, 4]
+    ids = _dense(np.array([0, 0, 1, 2, 2]))
+    recs1, _ = W.fake_job(n, ids, phases, 2)
+    recs3, logs = _spawn_fake(tmp_path, n, ids, phases, 2, world=3)
+    assert np.array_equal(np.array([(a, b, d, t) for a, b, d, t, _, _ in recs1]), recs3)
+    assert [len(log) for log in logs] == [2, 2, 2]
+
+
+def test_fake_job_rank_without_objects(tmp_path):
+    # more ranks than objects: the empty rank still takes part in every exchange
+    import sharded_screen_worker as W
+    n, phases = 2, [3]
+    ids = _dense(np.array([0, 1]))
+    recs1, _ = W.fake_job(n, ids, phases, 2)
+    recs3, logs = _spawn_fake(tmp_path, n, ids, phases, 2, world=3)
+    assert np.array_equal(np.array([(a, b, d, t) for a, b, d, t, _, _ in recs1]), recs3)
+    assert [len(log) for log in logs] == [1, 1, 0]
+
+
 def test_fake_job_checksums_the_trajectory():
     import sharded_screen_worker as W
     n, phases = 6, [3, 2]
