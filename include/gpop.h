@@ -108,6 +108,11 @@ gpop_status gpop_propagator_step(gpop_propagator* p, int32_t steps, double* traj
     double* traj_a, void* stream);
 /* Steps taken so far. */
 int32_t gpop_propagator_steps_done(const gpop_propagator* p);
+/* No counterpart in the reference. The gravity walk the propagation calls take for n objects on a
+ * GPU of num_sms SMs at the given precision: 1 = one object per thread, 2 = two objects per
+ * thread, 3 = lanes (*lanes_out = lanes per object, else 1); -1 for invalid arguments. Host
+ * arithmetic only, no CUDA call. */
+int32_t gpop_walk_policy(int64_t n, int32_t num_sms, int32_t precision, int32_t* lanes_out);
 void gpop_propagator_destroy(gpop_propagator* p);
 /* No counterpart in the reference. gpop_propagate_device for callers that may not allocate device
  * memory while running (services that reserve their memory budget at start-up and forbid later

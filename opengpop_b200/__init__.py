@@ -36,7 +36,7 @@ EXPORTS = (
     "gpop_startup_init", "gpop_startup_correct", "gpop_gj8_predict", "gpop_gj8_correct",
     "gpop_matrix_column", "gpop_gj8_coefficients", "gpop_gravity", "gpop_frame_matrices",
     "gpop_ca_create", "gpop_ca_create_analytic", "gpop_ca_create_external", "gpop_ca_append", "gpop_ca_propagate", "gpop_ca_find", "gpop_ca_pairs", "gpop_ca_num_pairs",
-    "gpop_ca_set_rows", "gpop_ca_pair_range", "gpop_ca_reserve", "gpop_ca_trajectory", "gpop_ca_device_seconds", "gpop_ca_destroy",
+    "gpop_ca_set_rows", "gpop_ca_pair_range", "gpop_ca_reserve", "gpop_walk_policy", "gpop_ca_trajectory", "gpop_ca_device_seconds", "gpop_ca_destroy",
 )
 
 
@@ -128,6 +128,7 @@ def load_library(path=LIB_PATH):
         "gpop_ca_num_pairs": (i64, [_VP]),
         "gpop_ca_set_rows": (i32, [_VP, i64, i64]),
         "gpop_ca_reserve": (i32, [_VP, i32]),
+        "gpop_walk_policy": (i32, [i64, i32, i32, C.POINTER(i32)]),
         "gpop_ca_pair_range": (i32, [_VP, C.POINTER(i64), C.POINTER(i64)]),
         "gpop_ca_trajectory": (i32, [_VP] * 4 + [C.POINTER(i32)]),
         "gpop_ca_device_seconds": (i32, [_VP, _VP]),
@@ -139,6 +140,18 @@ def load_library(path=LIB_PATH):
         fn.argtypes = args
     _lib = lib
     return lib
+
+
+WALKS = {1: "one object per thread", 2: "two objects per thread", 3: "lanes"}
+
+
+def walk_policy(n, num_sms=148, precision=FP64):
+    """(walk, lanes per object) the propagation takes for n objects (gpop_walk_policy)."""
+    lanes = C.c_int32()
+    w = load_library().gpop_walk_policy(int(n), int(num_sms), int(precision), C.byref(lanes))
+    if w < 0:
+        raise GpopError(1, "invalid arguments to gpop_walk_policy")
+    return w, lanes.value
 
 
 def as_time(t):

@@ -423,6 +423,16 @@ gpop_status gpop_propagator_step(gpop_propagator* p, int32_t steps, double* traj
 
 int32_t gpop_propagator_steps_done(const gpop_propagator* p) { return p ? p->done : -1; }
 
+int32_t gpop_walk_policy(int64_t n, int32_t num_sms, int32_t precision, int32_t* lanes_out)
+{
+    if (n <= 0 || num_sms <= 0 || (precision != GPOP_FP64 && precision != GPOP_MIXED))
+        return -1;
+    const int walk = default_walk(n, num_sms, true, precision == GPOP_FP64);
+    if (lanes_out)
+        *lanes_out = walk == kWalkLanes ? lanes_per_object(n, num_sms) : 1;
+    return walk;
+}
+
 void gpop_propagator_destroy(gpop_propagator* p) { delete p; }
 
 gpop_status gpop_propagate_analytic(gpop_ctx* ctx, int32_t kind, double h, int32_t steps,

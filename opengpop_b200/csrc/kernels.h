@@ -72,6 +72,9 @@ enum WalkMode : int { kWalkOneObject = 1, kWalkTwoObjects = 2, kWalkLanes = 3, k
 // Lanes per object (1..32, a power of 2): the most that keep n objects in one wave of blocks of at
 // most 384 threads, one per SM.
 int lanes_per_object(int64_t n, int num_sms);
+// The walk launch_gj8 takes for n objects when none is forced (lanes: a lane-layout table is at
+// hand and the force is the gravity model; fp64_gravity: the FP64 build of it).
+int default_walk(int64_t n, int num_sms, bool lanes, bool fp64_gravity);
 // lane_ts: the lane-layout table of the same precision (NULL: no lane-split walk).
 cudaError_t launch_gj8(const TableSrc& ts, const PropArgs& a, int num_sms, cudaStream_t s,
     int block_override = 0, int walk = 0, const TableSrc* lane_ts = nullptr);

@@ -709,33 +709,33 @@ int lanes_per_object(int64_t n, int num_sms)
     return P;
 }
 
+// Default walk (measured on B200 at 70x70, LEO objects, mixed / FP64 M object-steps/s):
+// - up to 128 objects per SM, lanes (P from lanes_per_object, blocks of at most 384 threads):
+//   18,900 objects 74.7 / 49.4 against 65.0 / 47.0 with two lanes per pair of objects; 9,472:
+//   49.4 / 31.6 against 34.0 / 20.8 with two objects per thread;
+// - FP64 up to 192 per SM keeps two lanes per object (20,000: 42.0 against 39.1 with one object
+//   per thread; 24,000: 50.0 against 46.4; 28,000: 57.7 against 54.1);
+// - above, two objects per thread (20,000 mixed: 64.5 against 63.7 with two lanes per object;
+//   37,000: 120 / 64 against 104 / 62 with two lanes per pair), except that FP64 takes one
+//   object per thread up to 256 per SM, where two objects per thread leave at most one warp
+//   per scheduler (30,000: 57.2 against 52.7; 37,000: 65.1 against 64.5).
+// One or two objects per thread when no lane-layout table is at hand.
+int default_walk(int64_t n, int num_sms, bool lanes, bool fp64_gravity)
+{
+    if (lanes && (n <= (int64_t)num_sms * 128 || (fp64_gravity && 2 * n <= (int64_t)num_sms * kLanesBlockMid)))
+        return kWalkLanes;
+    if (n >= (int64_t)num_sms * 128)
+        return fp64_gravity && n <= (int64_t)num_sms * 256 ? kWalkOneObject : kWalkTwoObjects;
+    return kWalkOneObject;
+}
+
 cudaError_t launch_gj8(const TableSrc& ts, const PropArgs& a, int num_sms, cudaStream_t s,
     int block_override, int walk, const TableSrc* lane_ts)
 {
     if (a.n <= 0 || a.step_end <= a.step_begin)
         return cudaSuccess;
-    // Default walk (measured on B200 at 70x70, LEO objects, mixed / FP64 M object-steps/s):
-    // - up to 128 objects per SM, lanes (P from lanes_per_object, blocks of at most 384 threads):
-    //   18,900 objects 74.7 / 49.4 against 65.0 / 47.0 with two lanes per pair of objects; 9,472:
-    //   49.4 / 31.6 against 34.0 / 20.8 with two objects per thread;
-    // - FP64 up to 192 per SM keeps two lanes per object (20,000: 42.0 against 39.1 with one object
-    //   per thread; 24,000: 50.0 against 46.4; 28,000: 57.7 against 54.1);
-    // - above, two objects per thread (20,000 mixed: 64.5 against 63.7 with two lanes per object;
-    //   37,000: 120 / 64 against 104 / 62 with two lanes per pair), except that FP64 takes one
-    //   object per thread up to 256 per SM, where two objects per thread leave at most one warp
-    //   per scheduler (30,000: 57.2 against 52.7; 37,000: 65.1 against 64.5).
-    // One or two objects per thread when no lane-layout table is at hand.
-    if (walk <= 0) {
-        const bool lanes = lane_ts && a.kind == 0;
-        const bool fp64_gravity = a.kind == 0 && !ts.mixed;
-        if (lanes
-            && (a.n <= (int64_t)num_sms * 128 || (fp64_gravity && 2 * a.n <= (int64_t)num_sms * kLanesBlockMid)))
-            walk = kWalkLanes;
-        else if (a.n >= (int64_t)num_sms * 128)
-            walk = fp64_gravity && a.n <= (int64_t)num_sms * 256 ? kWalkOneObject : kWalkTwoObjects;
-        else
-            walk = kWalkOneObject;
-    }
+    if (walk <= 0)
+        walk = default_walk(a.n, num_sms, lane_ts && a.kind == 0, a.kind == 0 && !ts.mixed);
     if ((walk == kWalkLanes || walk == kWalkLanesTwo) && a.kind == 0 && lane_ts) {
         const TableSrc& lt = *lane_ts;
         const int K = walk == kWalkLanesTwo ? 2 : 1;
