@@ -110,3 +110,50 @@ def test_streaming_json_writer_matches_whole_document(tmp_path):
                     os.path.join(ROOT, "tests", "cpp", "json_stream_check.cpp"), "-o", exe],
                    check=True, capture_output=True, text=True)
     assert subprocess.run([exe]).returncode == 0
+
+
+def _nlohmann_include():
+    """Directory holding nlohmann/json.hpp 3.11.3 in this Python environment (a vendored copy in
+    cudnn_frontend's package), or None."""
+    import glob
+    import site
+    import sysconfig
+    roots = set(site.getsitepackages() + [sysconfig.get_paths()["purelib"]])
+    for root in sorted(roots):
+        for hdr in glob.glob(os.path.join(root, "**", "nlohmann", "json.hpp"), recursive=True):
+            with open(hdr, errors="replace") as f:
+                head = f.read(4000)
+            if "NLOHMANN_JSON_VERSION_MINOR 11" in head and "NLOHMANN_JSON_VERSION_PATCH 3" in head:
+                return os.path.dirname(os.path.dirname(hdr))
+    return None
+
+
+def test_json_writer_bytes_equal_nlohmann(tmp_path):
+    # The reference writes its output with nlohmann::json's dump(4) (exec/main.cpp:87-88,100-101).
+    # The CLI's writer must give the same bytes: numbers (edge values and ~1.4 million random
+    # doubles), string escapes, and whole propagate / closest-approach documents, streamed or not.
+    import subprocess
+    inc = _nlohmann_include()
+    if inc is None:
+        pytest.skip("nlohmann/json 3.11.3 header not found in this environment")
+    exe = str(tmp_path / "json_nlohmann_check")
+    subprocess.run(["g++", "-std=c++17", "-O2", "-I", os.path.join(ROOT, "opengpop_b200", "csrc"),
+                    "-I", inc, os.path.join(ROOT, "tests", "cpp", "json_nlohmann_check.cpp"), "-o",
+                    exe], check=True, capture_output=True, text=True)
+    p = subprocess.run([exe], capture_output=True, text=True, timeout=300)
+    assert p.returncode == 0 and p.stdout.strip().endswith("ok"), p.stdout[-3000:]
+
+
+def test_json_writer_power_table():
+    # the writer's cached powers of ten: 10^k (k = -300, -292, ..., 324) rounded to nearest as a
+    # 64-bit significand with its top bit set, times 2^e; recomputed here with exact rationals
+    import re
+    from fractions import Fraction
+    text = open(os.path.join(ROOT, "opengpop_b200", "csrc", "json.h")).read()
+    rows = re.findall(r"\{ 0x([0-9A-F]{16})ULL, (-?\d+), (-?\d+) \}", text)
+    assert [int(k) for _, _, k in rows] == list(range(-300, 325, 8))
+    for f_hex, e, k in rows:
+        f, e, k = int(f_hex, 16), int(e), int(k)
+        assert 2 ** 63 <= f < 2 ** 64
+        exact = Fraction(10) ** k / Fraction(2) ** e
+        assert abs(exact - f) <= Fraction(1, 2), k
