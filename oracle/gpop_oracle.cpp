@@ -581,13 +581,16 @@ double table_sec(const or_time& st, double h, int idx, bool midpoints, int befor
 }
 
 // ---------------- gravity (gravity_source.cu:168-262 + gravity_source_device.cu:63-239) ----------------
-void gravity_itrs(const Data& d, const double* p, double* a, std::vector<double>& P,
-    std::vector<double>& Cm, std::vector<double>& Sm, std::vector<double>& sums)
+// R = double is the oracle; R = long double (x87 extended) serves the finite differences of the
+// adjoint checks, which need less rounding noise than double gives.
+template <typename R>
+void gravity_itrs(const Data& d, const R* p, R* a, std::vector<R>& P, std::vector<R>& Cm,
+    std::vector<R>& Sm, std::vector<R>& sums)
 {
     const unsigned N = d.N;
-    double x = p[0], y = p[1], z = p[2];
-    double r = std::sqrt(x * x + y * y + z * z);
-    double eps = z / r;
+    R x = p[0], y = p[1], z = p[2];
+    R r = std::sqrt(x * x + y * y + z * z);
+    R eps = z / r;
     // ComputePbarKernel: per column m, subdiagonal then column recursion (eq. 7-12, 7-16)
     for (unsigned m = 0; m < N; ++m)
         P[tri(m, m)] = d.pdiag[m];
@@ -612,33 +615,33 @@ void gravity_itrs(const Data& d, const double* p, double* a, std::vector<double>
         Sm[i] = Sm[1] * Cm[i - 1] + Cm[1] * Sm[i - 1];
     }
     // PrepareMSumKernel + SumM (eq. 4-11), per-n sums over m
-    double* Gn = sums.data();
-    double* Hn = Gn + N;
-    double* Jn = Hn + N;
-    double* Kn = Jn + N;
+    R* Gn = sums.data();
+    R* Hn = Gn + N;
+    R* Jn = Hn + N;
+    R* Kn = Jn + N;
     for (unsigned n = 0; n < N; ++n) {
-        double g = 0, h = 0, j = 0, k = 0;
+        R g = 0, h = 0, j = 0, k = 0;
         for (unsigned m = 0; m <= n; ++m) {
-            double tg, th, tj, tk;
+            R tg, th, tj, tk;
             size_t nm = tri(n, m);
-            double Pnm = P[nm];
-            double Pnm1 = (n > m) ? P[tri(n, m + 1)] : 0.0;
-            double Cnm = d.C[nm], Snm = d.S[nm];
+            R Pnm = P[nm];
+            R Pnm1 = (n > m) ? P[tri(n, m + 1)] : R(0);
+            R Cnm = d.C[nm], Snm = d.S[nm];
             if (n < 2) {
                 tg = th = tj = tk = 0;
             } else if (m == 0) {
-                double Pn0 = P[tri(n, 0)];
-                double Pn1 = P[tri(n, 1)];
-                double Cn0 = d.C[tri(n, 0)];
+                R Pn0 = P[tri(n, 0)];
+                R Pn1 = P[tri(n, 1)];
+                R Cn0 = d.C[tri(n, 0)];
                 tj = 0;
                 tk = 0;
-                tg = Cn0 * (n + 1) * Pn0;
+                tg = Cn0 * R(n + 1) * Pn0;
                 th = d.zeta[tri(n, 0)] * Cn0 * Pn1;
             } else {
-                double c = Cm[m], s = Sm[m], c1 = Cm[m - 1], s1 = Sm[m - 1];
-                tj = (double)m * Pnm * (Cnm * c1 + Snm * s1);
-                tk = -(double)m * Pnm * (Cnm * s1 - Snm * c1);
-                tg = (double)(1 + n + m) * Pnm * (Cnm * c + Snm * s);
+                R c = Cm[m], s = Sm[m], c1 = Cm[m - 1], s1 = Sm[m - 1];
+                tj = (R)m * Pnm * (Cnm * c1 + Snm * s1);
+                tk = -(R)m * Pnm * (Cnm * s1 - Snm * c1);
+                tg = (R)(1 + n + m) * Pnm * (Cnm * c + Snm * s);
                 th = d.zeta[nm] * Pnm1 * (Cnm * c + Snm * s);
             }
             g += tg;
@@ -652,8 +655,8 @@ void gravity_itrs(const Data& d, const double* p, double* a, std::vector<double>
         Kn[n] = k;
     }
     // PrepareNSumKernel + SumN (eq. 4-12)
-    double base = d.R / r;
-    double coeff = base * base;
+    R base = d.R / r;
+    R coeff = base * base;
     for (unsigned n = 2; n < N; ++n) {
         Gn[n] *= coeff;
         Hn[n] *= coeff;
@@ -661,7 +664,7 @@ void gravity_itrs(const Data& d, const double* p, double* a, std::vector<double>
         Jn[n] *= coeff;
         coeff *= base;
     }
-    double G = 0, H = 0, J = 0, K = 0;
+    R G = 0, H = 0, J = 0, K = 0;
     for (unsigned n = 0; n < N; ++n) {
         G += Gn[n];
         H += Hn[n];
@@ -670,19 +673,19 @@ void gravity_itrs(const Data& d, const double* p, double* a, std::vector<double>
     }
     // CalculateAcceleration (eq. 4-13)
     G = G + 1;
-    double Lambda = G + z * H / r;
-    double ax = Lambda * x / r - J;
-    double ay = Lambda * y / r - K;
-    double az = Lambda * z / r - H;
-    double c = -d.GM / (r * r);
+    R Lambda = G + z * H / r;
+    R ax = Lambda * x / r - J;
+    R ay = Lambda * y / r - K;
+    R az = Lambda * z / r - H;
+    R c = -d.GM / (r * r);
     a[0] = c * ax;
     a[1] = c * ay;
     a[2] = c * az;
 }
 
-struct GravScratch {
-    std::vector<double> P, Cm, Sm, sums;
-    explicit GravScratch(const Data& d)
+template <typename R> struct GravScratchT {
+    std::vector<R> P, Cm, Sm, sums;
+    explicit GravScratchT(const Data& d)
         : P(tri_size(d.N))
         , Cm(d.N)
         , Sm(d.N)
@@ -690,14 +693,16 @@ struct GravScratch {
     {
     }
 };
+using GravScratch = GravScratchT<double>;
 
 // GravitySource::ComputeAcceleration frame handling: r_itrs = M^T r_gcrs, a_gcrs = M a_itrs
-void gravity_gcrs(const Data& d, const double* M, const double* r, double* a, GravScratch& s)
+template <typename R>
+void gravity_gcrs(const Data& d, const double* M, const R* r, R* a, GravScratchT<R>& s)
 {
-    double p[3], ai[3];
+    R p[3], ai[3];
     if (M) {
         for (int j = 0; j < 3; ++j) {
-            double v = 0.0;
+            R v = 0.0;
             for (int i = 0; i < 3; ++i)
                 v += M[sq(i, j)] * r[i];
             p[j] = v;
@@ -710,7 +715,7 @@ void gravity_gcrs(const Data& d, const double* M, const double* r, double* a, Gr
     gravity_itrs(d, p, ai, s.P, s.Cm, s.Sm, s.sums);
     if (M) {
         for (int i = 0; i < 3; ++i) {
-            double v = 0.0;
+            R v = 0.0;
             for (int j = 0; j < 3; ++j)
                 v += M[sq(i, j)] * ai[j];
             a[i] = v;
@@ -723,7 +728,7 @@ void gravity_gcrs(const Data& d, const double* M, const double* r, double* a, Gr
 }
 
 // ---------------- analytic force models (unit_tests/include/gpu_test_helpers.cuh:19-145) ----------------
-void analytic(int kind, const double* pos, const double* vel, double t, double* out)
+template <typename R> void analytic(int kind, const R* pos, const R* vel, R t, R* out)
 {
     switch (kind) {
     case OR_FORCE_ZERO:
@@ -735,24 +740,24 @@ void analytic(int kind, const double* pos, const double* vel, double t, double* 
         out[2] = 3;
         return;
     case OR_FORCE_POLY7: {
-        double v = -3 * 2 * t + 7 * 6 * t * t * t * t * t;
+        R v = -3 * 2 * t + 7 * 6 * t * t * t * t * t;
         out[0] = out[1] = out[2] = v;
         return;
     }
     case OR_FORCE_POLY8: {
-        double v = 56 * std::pow(t, 6) - 42 * std::pow(t, 5) + 60 * std::pow(t, 4)
+        R v = 56 * std::pow(t, 6) - 42 * std::pow(t, 5) + 60 * std::pow(t, 4)
             - 100 * std::pow(t, 3) - 120 * std::pow(t, 2) + 6 * t - 2;
         out[0] = out[1] = out[2] = v;
         return;
     }
     case OR_FORCE_POLY9: {
-        double v = 72 * std::pow(t, 7) + 56 * std::pow(t, 6) - 42 * std::pow(t, 5)
+        R v = 72 * std::pow(t, 7) + 56 * std::pow(t, 6) - 42 * std::pow(t, 5)
             + 60 * std::pow(t, 4) - 100 * std::pow(t, 3) - 120 * std::pow(t, 2) + 6 * t - 2;
         out[0] = out[1] = out[2] = v;
         return;
     }
     case OR_FORCE_EXP: {
-        double v = std::exp(-t);
+        R v = std::exp(-t);
         out[0] = out[1] = out[2] = v;
         return;
     }
@@ -776,7 +781,8 @@ struct Force {
     std::vector<double> prop_m; // (steps + 5) x 9 (propagation epochs, index i <-> (i-4) h)
 
     // ForceModel::ComputeGenerationAcceleration (force_model.cu:59-89) / mock (mock_force_model.cuh:65-82)
-    void gen(const double* r, const double* v, int step, int k, double* a, GravScratch* gs) const
+    template <typename R>
+    void gen(const R* r, const R* v, int step, int k, R* a, GravScratchT<R>* gs) const
     {
         if (kind == OR_FORCE_GRAVITY) {
             int s = step > 0 ? step - 1 : step;
@@ -784,17 +790,18 @@ struct Force {
         } else {
             int dir = step > 0 ? -1 : 1;
             double t = static_cast<double>(step + dir) * h + (-dir) * kRkNodes[k] * h;
-            analytic(kind, r, v, t, a);
+            analytic<R>(kind, r, v, (R)t, a);
         }
     }
     // ForceModel::ComputePropagationAcceleration (force_model.cu:91-109) / mock (:94-106)
-    void prop(const double* r, const double* v, int idx, double* a, GravScratch* gs) const
+    template <typename R>
+    void prop(const R* r, const R* v, int idx, R* a, GravScratchT<R>* gs) const
     {
         if (kind == OR_FORCE_GRAVITY) {
             gravity_gcrs(*d, &prop_m[idx * 9], r, a, *gs);
         } else {
             double t = (double)(idx - 4) * h;
-            analytic(kind, r, v, t, a);
+            analytic<R>(kind, r, v, (R)t, a);
         }
     }
 };
@@ -823,18 +830,19 @@ void build_tables(Force& f, const or_time& st, int steps)
         frame_matrix(*f.d, st, table_sec(st, f.h, idx, false, 4), &f.prop_m[idx * 9], nullptr);
 }
 
-struct Startup {
-    double r[9][3], v[9][3], a[9][3], s[9][3], S[9][3];
+template <typename R> struct StartupT {
+    R r[9][3], v[9][3], a[9][3], s[9][3], S[9][3];
 };
+using Startup = StartupT<double>;
 
 // RK8::step (lib/gpu_startup/src/gpu_startup.cu:108-144) for one object
-void rk8_step(const Force& f, int step, Startup& sd, GravScratch* gs)
+template <typename R> void rk8_step(const Force& f, int step, StartupT<R>& sd, GravScratchT<R>* gs)
 {
-    double hh = step > 0 ? f.h : -f.h;
+    R hh = step > 0 ? (R)f.h : -(R)f.h;
     int dir = step > 0 ? -1 : 1;
     int base = 4 + step + dir;
-    double Kx[10][3] = {}, Kv[10][3] = {};
-    double tx[3], tv[3];
+    R Kx[10][3] = {}, Kv[10][3] = {};
+    R tx[3], tv[3];
     for (int j = 0; j < 3; ++j) {
         tx[j] = sd.r[base][j];
         tv[j] = sd.v[base][j];
@@ -843,7 +851,7 @@ void rk8_step(const Force& f, int step, Startup& sd, GravScratch* gs)
     f.gen(tx, tv, step, 0, Kv[0], gs);
     for (int k = 1; k <= 9; ++k) {
         for (int j = 0; j < 3; ++j) {
-            double sx = 0, sv = 0;
+            R sx = 0, sv = 0;
             for (int i = 0; i < 9; ++i) {
                 sx += kRkA[k - 1][i] * Kx[i][j];
                 sv += kRkA[k - 1][i] * Kv[i][j];
@@ -857,7 +865,7 @@ void rk8_step(const Force& f, int step, Startup& sd, GravScratch* gs)
     }
     int col = 4 + step;
     for (int j = 0; j < 3; ++j) {
-        double sx = 0, sv = 0;
+        R sx = 0, sv = 0;
         for (int k = 0; k < 10; ++k) {
             sx += Kx[k][j] * kRkB[k];
             sv += Kv[k][j] * kRkB[k];
@@ -868,7 +876,7 @@ void rk8_step(const Force& f, int step, Startup& sd, GravScratch* gs)
 }
 
 // StartupPredictor::Predict (gpu_startup.cu:146-168)
-void rk8_all(const Force& f, const double* r0, const double* v0, Startup& sd, GravScratch* gs)
+template <typename R> void rk8_all(const Force& f, const R* r0, const R* v0, StartupT<R>& sd, GravScratchT<R>* gs)
 {
     std::memset(&sd, 0, sizeof(sd));
     for (int j = 0; j < 3; ++j) {
@@ -882,7 +890,7 @@ void rk8_all(const Force& f, const double* r0, const double* v0, Startup& sd, Gr
 }
 
 // StartupCorrector::CalculateAccelerationMatrix (gpu_startup.cu:196-224)
-void corr_accel(const Force& f, Startup& sd, bool epoch, GravScratch* gs)
+template <typename R> void corr_accel(const Force& f, StartupT<R>& sd, bool epoch, GravScratchT<R>* gs)
 {
     for (int i = 0; i < 9; ++i) {
         if (i == 4 && !epoch)
@@ -892,12 +900,12 @@ void corr_accel(const Force& f, Startup& sd, bool epoch, GravScratch* gs)
 }
 
 // StartupCorrector::CalculateS0 (gpu_startup.cu:170-195): column 4 of s and S
-void corr_s0(const Force& f, Startup& sd)
+template <typename R> void corr_s0(const Force& f, StartupT<R>& sd)
 {
-    double hinv = 1 / f.h;
-    double h2inv = 1 / (f.h * f.h);
+    R hinv = 1 / (R)f.h;
+    R h2inv = 1 / ((R)f.h * (R)f.h);
     for (int j = 0; j < 3; ++j) {
-        double sb = 0, sa = 0;
+        R sb = 0, sa = 0;
         for (int k = 0; k < 9; ++k) {
             sb += kSA[4][k] * sd.a[k][j];
             sa += kGJ[4][k] * sd.a[k][j];
@@ -908,7 +916,7 @@ void corr_s0(const Force& f, Startup& sd)
 }
 
 // CalculateAllSKernel (lib/gpu_startup/src/device/calculate_all_s.cu:19-47)
-void corr_all_s(Startup& sd)
+template <typename R> void corr_all_s(StartupT<R>& sd)
 {
     for (int i = 1; i <= 4; ++i)
         for (int j = 0; j < 3; ++j) {
@@ -920,28 +928,29 @@ void corr_all_s(Startup& sd)
 }
 
 // StartupCorrector::Correct (gpu_startup.cu:247-294)
-void corr_correct(const Force& f, Startup& sd, GravScratch* gs)
+template <typename R> void corr_correct(const Force& f, StartupT<R>& sd, GravScratchT<R>* gs)
 {
     corr_s0(f, sd);
     corr_all_s(sd);
-    double h2 = f.h * f.h;
+    R h2 = (R)f.h * (R)f.h;
     for (int c = 0; c < 9; ++c) {
         if (c == 4)
             continue; // epoch column restored (MoveStateToTemp / MoveStateToMatrix)
         for (int j = 0; j < 3; ++j) {
-            double sv = 0, sr = 0;
+            R sv = 0, sr = 0;
             for (int k = 0; k < 9; ++k) {
                 sv += sd.a[k][j] * kSA[c][k];
                 sr += sd.a[k][j] * kGJ[c][k];
             }
-            sd.v[c][j] = f.h * (sv + sd.s[c][j]);
+            sd.v[c][j] = (R)f.h * (sv + sd.s[c][j]);
             sd.r[c][j] = h2 * (sr + sd.S[c][j]);
         }
     }
     corr_accel(f, sd, false, gs);
 }
 
-void startup_all(const Force& f, int ncorr, const double* r0, const double* v0, Startup& sd, GravScratch* gs)
+template <typename R>
+void startup_all(const Force& f, int ncorr, const R* r0, const R* v0, StartupT<R>& sd, GravScratchT<R>* gs)
 {
     rk8_all(f, r0, v0, sd, gs); // GpuStartup::Startup (gpu_startup.cu:55-68)
     corr_accel(f, sd, true, gs);
@@ -951,11 +960,12 @@ void startup_all(const Force& f, int ncorr, const double* r0, const double* v0, 
 
 // Predictor::Predict (lib/gpu_integrator/src/prediction.cu:49-74) +
 // FinalizePredictionKernel / MoveAccelerationsKernel (gpu_integrator/src/device/dev_functions.cu:20-50)
-void predict(const Force& f, int step, double* r, double* v, double (*acc)[3], double* s, double* S, GravScratch* gs)
+template <typename R>
+void predict(const Force& f, int step, R* r, R* v, R (*acc)[3], R* s, R* S, GravScratchT<R>* gs)
 {
-    double vt[3], rt[3];
+    R vt[3], rt[3];
     for (int j = 0; j < 3; ++j) {
-        double sv = 0, sr = 0;
+        R sv = 0, sr = 0;
         for (int k = 0; k < 9; ++k) {
             sv += acc[k][j] * kSA[9][k];
             sr += acc[k][j] * kGJ[9][k];
@@ -965,8 +975,8 @@ void predict(const Force& f, int step, double* r, double* v, double (*acc)[3], d
     }
     for (int j = 0; j < 3; ++j) {
         S[j] += s[j] + acc[8][j] / 2;
-        v[j] = (vt[j] + s[j] + acc[8][j] / 2) * f.h;
-        r[j] = (rt[j] + S[j]) * f.h * f.h;
+        v[j] = (vt[j] + s[j] + acc[8][j] / 2) * (R)f.h;
+        r[j] = (rt[j] + S[j]) * (R)f.h * (R)f.h;
     }
     for (int k = 0; k < 8; ++k)
         for (int j = 0; j < 3; ++j)
@@ -976,13 +986,14 @@ void predict(const Force& f, int step, double* r, double* v, double (*acc)[3], d
 
 // GpuPropagator::Correct (lib/gpu_propagator/src/gpu_propagator.cu:86-119) + UpdateSmallSKernel and
 // FinalizeCorrectionKernel (gpu_propagator/src/device/dev_functions.cu:36-69)
-void correct(const Force& f, int step, int ncorr, double* r, double* v, double (*acc)[3], double* s,
-    const double* S, GravScratch* gs)
+template <typename R>
+void correct(const Force& f, int step, int ncorr, R* r, R* v, R (*acc)[3], R* s, const R* S,
+    GravScratchT<R>* gs)
 {
-    double prev[3], s1[3], s2[3];
+    R prev[3], s1[3], s2[3];
     for (int j = 0; j < 3; ++j) {
         prev[j] = s[j];
-        double a1 = 0, a2 = 0;
+        R a1 = 0, a2 = 0;
         for (int k = 0; k < 8; ++k) {
             a1 += acc[k][j] * kSA[8][k];
             a2 += acc[k][j] * kGJ[8][k];
@@ -995,19 +1006,20 @@ void correct(const Force& f, int step, int ncorr, double* r, double* v, double (
         for (int j = 0; j < 3; ++j)
             s[j] = prev[j] + (acc[8][j] + acc[7][j]) / 2;
         for (int j = 0; j < 3; ++j) {
-            v[j] = f.h * (s1[j] + acc[8][j] * kSA[8][8] + s[j]);
-            r[j] = f.h * f.h * (s2[j] + acc[8][j] * kGJ[8][8] + S[j]);
+            v[j] = (R)f.h * (s1[j] + acc[8][j] * kSA[8][8] + s[j]);
+            r[j] = (R)f.h * (R)f.h * (s2[j] + acc[8][j] * kGJ[8][8] + S[j]);
         }
     }
 }
 
-void propagate_one(const Force& f, int steps, int ncorr, const double* r0, const double* v0,
-    int64_t n, int64_t obj, double* r_steps, double* v_steps, double* a_steps, double* rf, double* vf)
+template <typename R>
+void propagate_one(const Force& f, int steps, int ncorr, const R* r0, const R* v0, int64_t n, int64_t obj,
+    R* r_steps, R* v_steps, R* a_steps, R* rf, R* vf)
 {
-    GravScratch gs(*f.d);
-    Startup sd;
+    GravScratchT<R> gs(*f.d);
+    StartupT<R> sd;
     startup_all(f, ncorr, r0, v0, sd, &gs);
-    double s[3], S[3], acc[9][3], r[3], v[3];
+    R s[3], S[3], acc[9][3], r[3], v[3];
     for (int j = 0; j < 3; ++j) {
         s[j] = sd.s[8][j];
         S[j] = sd.S[8][j];
@@ -1028,7 +1040,7 @@ void propagate_one(const Force& f, int steps, int ncorr, const double* r0, const
         size_t o = ((size_t)(step - 1) * n + obj) * 3;
         // Exported acceleration (MoveColumnToVectorKernel, column 8). Quirk Q3: for steps 1..4 the
         // reference exports the startup column 8 (t = 4h); OR_FLAG_FIX_Q3 exports column step+4.
-        const double* ea = acc[8];
+        const R* ea = acc[8];
         if (step <= 4 && (f.flags & OR_FLAG_FIX_Q3))
             ea = sd.a[step + 4];
         for (int j = 0; j < 3; ++j) {
@@ -1091,15 +1103,14 @@ bool part_pair(const Part& p, uint64_t idx, uint32_t& a, uint32_t& b)
 }
 
 // HermitePolynomial (lib/closest_approach/include/closest_approach/utility/interpolation.cuh:27-98)
-struct Hermite {
-    double c[9];
-    double dt;
-    Hermite() { }
-    Hermite(double p0, double v0, double a0, double p1, double v1, double a1, double p2, double v2,
-        double a2, double dt_)
+template <typename R> struct HermiteT {
+    R c[9];
+    R dt;
+    HermiteT() { }
+    HermiteT(R p0, R v0, R a0, R p1, R v1, R a1, R p2, R v2, R a2, R dt_)
         : dt(dt_)
     {
-        double t[9] = { 0.0, 0.0, 0.0, dt, dt, dt, 2.0 * dt, 2.0 * dt, 2.0 * dt };
+        R t[9] = { 0.0, 0.0, 0.0, dt, dt, dt, 2.0 * dt, 2.0 * dt, 2.0 * dt };
         c[0] = c[1] = c[2] = p0;
         c[3] = c[4] = c[5] = p1;
         c[6] = c[7] = c[8] = p2;
@@ -1115,20 +1126,20 @@ struct Hermite {
                 }
             }
     }
-    double operator()(double t) const
+    R operator()(R t) const
     {
-        double z[9] = { 0.0, 0.0, 0.0, dt, dt, dt, 2.0 * dt, 2.0 * dt, 2.0 * dt };
-        double res = c[0], term = 1.0;
+        R z[9] = { 0.0, 0.0, 0.0, dt, dt, dt, 2.0 * dt, 2.0 * dt, 2.0 * dt };
+        R res = c[0], term = 1.0;
         for (int i = 1; i < 9; ++i) {
             term *= (t - z[i - 1]);
             res += c[i] * term;
         }
         return res;
     }
-    double deriv(double te) const
+    R deriv(R te) const
     {
-        double z[9] = { 0.0, 0.0, 0.0, dt, dt, dt, 2.0 * dt, 2.0 * dt, 2.0 * dt };
-        double res = 0.0, Nn = 1.0, dN = 0.0;
+        R z[9] = { 0.0, 0.0, 0.0, dt, dt, dt, 2.0 * dt, 2.0 * dt, 2.0 * dt };
+        R res = 0.0, Nn = 1.0, dN = 0.0;
         for (int i = 0; i < 9; ++i) {
             res += c[i] * dN;
             if (i < 8) {
@@ -1139,33 +1150,35 @@ struct Hermite {
         return res;
     }
 };
+using Hermite = HermiteT<double>;
 
-struct Interp {
-    Hermite x, y, z;
+template <typename R> struct InterpT {
+    HermiteT<R> x, y, z;
 };
+using Interp = InterpT<double>;
 
 // ApproachFunc (interpolation.cuh:106-123)
-double approach(const Interp& A, const Interp& B, double t)
+template <typename R> R approach(const InterpT<R>& A, const InterpT<R>& B, R t)
 {
-    double dx = A.x(t) - B.x(t);
-    double dy = A.y(t) - B.y(t);
-    double dz = A.z(t) - B.z(t);
-    double ddx = A.x.deriv(t) - B.x.deriv(t);
-    double ddy = A.y.deriv(t) - B.y.deriv(t);
-    double ddz = A.z.deriv(t) - B.z.deriv(t);
+    R dx = A.x(t) - B.x(t);
+    R dy = A.y(t) - B.y(t);
+    R dz = A.z(t) - B.z(t);
+    R ddx = A.x.deriv(t) - B.x.deriv(t);
+    R ddy = A.y.deriv(t) - B.y.deriv(t);
+    R ddz = A.z.deriv(t) - B.z.deriv(t);
     return (dx * ddx) + (dy * ddy) + (dz * ddz);
 }
 
 // FindRoot (interpolation.cuh:126-152), secant
-template <typename F> double find_root(F f, double x0, double x1, double tol = 1e-7, int max_iter = 100)
+template <typename R, typename F> R find_root(F f, R x0, R x1, R tol = 1e-7, int max_iter = 100)
 {
-    double f0 = f(x0);
-    double f1 = f(x1);
+    R f0 = f(x0);
+    R f1 = f(x1);
     for (int i = 0; i < max_iter; ++i) {
-        if (std::fabs(f1 - f0) < 1e-14)
+        if (std::fabs(f1 - f0) < R(1e-14))
             return x1;
-        double xn = x1 - f1 * (x1 - x0) / (f1 - f0);
-        double fn = f(xn);
+        R xn = x1 - f1 * (x1 - x0) / (f1 - f0);
+        R fn = f(xn);
         if (std::fabs(xn - x1) < tol || std::fabs(fn) < tol)
             return xn;
         x0 = x1;
@@ -1177,15 +1190,74 @@ template <typename F> double find_root(F f, double x0, double x1, double tol = 1
 }
 
 // nodes27 layout: axis (x,y,z) x [before p,v,a; closest p,v,a; after p,v,a]
-Interp make_interp(const double* n27, double dt)
+template <typename R> InterpT<R> make_interp(const R* n27, R dt)
 {
-    Interp I;
-    Hermite* hs[3] = { &I.x, &I.y, &I.z };
+    InterpT<R> I;
+    HermiteT<R>* hs[3] = { &I.x, &I.y, &I.z };
     for (int ax = 0; ax < 3; ++ax) {
-        const double* q = n27 + ax * 9;
-        *hs[ax] = Hermite(q[0], q[1], q[2], q[3], q[4], q[5], q[6], q[7], q[8], dt);
+        const R* q = n27 + ax * 9;
+        *hs[ax] = HermiteT<R>(q[0], q[1], q[2], q[3], q[4], q[5], q[6], q[7], q[8], dt);
     }
     return I;
+}
+
+// One pair's closest approach over stored trajectories [steps][3] of A and B (positions, velocities,
+// exported accelerations): the running minimum and node capture of or_ca_screen for a single pair,
+// then or_ca_refine's refinement. Templated so that the long double finite differences use it.
+template <typename R>
+void pair_closest(const R* rA, const R* vA, const R* aA, const R* rB, const R* vB, const R* aB, int steps,
+    R h, R& miss, R& tca)
+{
+    R mind = std::numeric_limits<R>::max();
+    uint32_t cs = 0xFFFFFFFFu;
+    R nodes[54] = {};
+    R last[18] = {}; // A then B: p, v, a (zero before the first step)
+    auto put = [&](int o, int node, const R* p, const R* v, const R* a) {
+        for (int ax = 0; ax < 3; ++ax) {
+            nodes[o * 27 + ax * 9 + node * 3 + 0] = p[ax];
+            nodes[o * 27 + ax * 9 + node * 3 + 1] = v[ax];
+            nodes[o * 27 + ax * 9 + node * 3 + 2] = a[ax];
+        }
+    };
+    for (int k = 0; k < steps; ++k) {
+        const R *pa = rA + 3 * k, *va = vA + 3 * k, *xa = aA + 3 * k;
+        const R *pb = rB + 3 * k, *vb = vB + 3 * k, *xb = aB + 3 * k;
+        R dx = pa[0] - pb[0], dy = pa[1] - pb[1], dz = pa[2] - pb[2];
+        R dist = std::sqrt(dx * dx + dy * dy + dz * dz);
+        if (dist < mind) {
+            mind = dist;
+            cs = (uint32_t)k;
+            put(0, 1, pa, va, xa);
+            put(1, 1, pb, vb, xb);
+            put(0, 0, last, last + 3, last + 6);
+            put(1, 0, last + 9, last + 12, last + 15);
+        } else if (cs == (uint32_t)k - 1) {
+            put(0, 2, pa, va, xa);
+            put(1, 2, pb, vb, xb);
+        }
+        for (int j = 0; j < 3; ++j) {
+            last[j] = pa[j];
+            last[3 + j] = va[j];
+            last[6 + j] = xa[j];
+            last[9 + j] = pb[j];
+            last[12 + j] = vb[j];
+            last[15 + j] = xb[j];
+        }
+    }
+    miss = mind;
+    if (cs == 0) {
+        tca = 0;
+        return;
+    }
+    if (cs == (uint32_t)steps - 1) {
+        tca = (R)steps * h;
+        return;
+    }
+    InterpT<R> A = make_interp<R>(nodes, h), B = make_interp<R>(nodes + 27, h);
+    R t = find_root<R>([&](R tt) { return approach<R>(A, B, tt); }, R(0), h);
+    tca = t + (R)cs * h;
+    R dx = A.x(t) - B.x(t), dy = A.y(t) - B.y(t), dz = A.z(t) - B.z(t);
+    miss = std::sqrt(dx * dx + dy * dy + dz * dz);
 }
 
 int nthreads(int t)
@@ -1354,11 +1426,11 @@ void or_corrector_unit(int32_t kind, double h, int32_t op, double* r27, double* 
     std::memset(&sd, 0, sizeof(sd));
     std::memcpy(sd.r, r27, sizeof(sd.r));
     std::memcpy(sd.v, v27, sizeof(sd.v));
-    corr_accel(f, sd, true, nullptr);
+    corr_accel<double>(f, sd, true, nullptr);
     if (op == 1) {
         corr_s0(f, sd);
     } else if (op == 2) {
-        corr_correct(f, sd, nullptr);
+        corr_correct<double>(f, sd, nullptr);
     }
     unpack27(sd, r27, v27, a27, s27, S27);
 }
@@ -1369,7 +1441,7 @@ void or_predict_unit(int32_t kind, double h, int32_t step, double* r, double* v,
     Force f;
     f.kind = kind;
     f.h = h;
-    predict(f, step, r, v, reinterpret_cast<double(*)[3]>(a27), s, S, nullptr);
+    predict<double>(f, step, r, v, reinterpret_cast<double(*)[3]>(a27), s, S, nullptr);
 }
 
 void or_finalize_correction_unit(double h, double* r, double* v, const double* a27, const double* s,
@@ -1600,6 +1672,60 @@ void or_ca_refine(int64_t n, const uint32_t* ids, double h, uint32_t total_steps
         pb[pi * 3 + 1] = B.y(t);
         pb[pi * 3 + 2] = B.z(t);
     }
+}
+
+int32_t or_miss_fd_ld(const void* dv, const or_time* st, double h, int32_t steps, int32_t ncorr,
+    int64_t n_pairs, const double* rA, const double* vA, const double* rB, const double* vB, double dr,
+    double dvel, double* miss, double* tca, double* grad, int32_t threads)
+{
+    typedef long double LD;
+    if (!dv || n_pairs <= 0 || steps < 1 || h == 0.0)
+        return 1;
+    Force f = make_force(dv, OR_FORCE_GRAVITY, st, h, steps, 0);
+    // run 0: the pair as given; run 1 + 2 c + s: component c (0..11: r_A, v_A, r_B, v_B) moved by
+    // +step (s = 0) or -step (s = 1)
+    const int runs = 25;
+    std::vector<LD> out((size_t)n_pairs * runs * 2, 0.0L);
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads(threads))
+    for (int64_t job = 0; job < n_pairs * runs; ++job) {
+        const int64_t p = job / runs;
+        const int run = (int)(job % runs);
+        LD x0[2][6];
+        for (int j = 0; j < 3; ++j) {
+            x0[0][j] = rA[3 * p + j];
+            x0[0][3 + j] = vA[3 * p + j];
+            x0[1][j] = rB[3 * p + j];
+            x0[1][3 + j] = vB[3 * p + j];
+        }
+        if (run > 0) {
+            const int c = (run - 1) / 2;
+            const LD stepv = c % 6 < 3 ? (LD)dr : (LD)dvel;
+            x0[c / 6][c % 6] += (run - 1) % 2 == 0 ? stepv : -stepv;
+        }
+        std::vector<LD> tr[2][3];
+        LD rf[3], vf[3];
+        for (int o = 0; o < 2; ++o) {
+            for (int k = 0; k < 3; ++k)
+                tr[o][k].assign((size_t)steps * 3, 0.0L);
+            propagate_one<LD>(f, steps, ncorr, x0[o], x0[o] + 3, 1, 0, tr[o][0].data(), tr[o][1].data(),
+                tr[o][2].data(), rf, vf);
+        }
+        LD m, t;
+        pair_closest<LD>(tr[0][0].data(), tr[0][1].data(), tr[0][2].data(), tr[1][0].data(), tr[1][1].data(),
+            tr[1][2].data(), steps, (LD)h, m, t);
+        out[(size_t)job * 2] = m;
+        out[(size_t)job * 2 + 1] = t;
+    }
+    for (int64_t p = 0; p < n_pairs; ++p) {
+        const LD* o = out.data() + (size_t)p * runs * 2;
+        miss[p] = (double)o[0];
+        tca[p] = (double)o[1];
+        for (int c = 0; c < 12; ++c) {
+            const LD stepv = c % 6 < 3 ? (LD)dr : (LD)dvel;
+            grad[p * 12 + c] = (double)((o[(1 + 2 * c) * 2] - o[(2 + 2 * c) * 2]) / (2 * stepv));
+        }
+    }
+    return 0;
 }
 
 } // extern "C"

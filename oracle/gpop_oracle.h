@@ -134,6 +134,18 @@ void or_ca_refine(int64_t n, const uint32_t* set_ids, double h, uint32_t total_s
     const or_ca_state* st, double* dist_out, double* time_out, double* posA_out, double* posB_out,
     int32_t threads);
 
+/* Finite-difference side of the adjoint checks, in x87 extended precision (long double) so that the
+ * difference quotient is not swamped by rounding noise at small steps. For each pair (objects A and
+ * B with initial states rA, vA, rB, vB [n_pairs][3]) propagates both objects with gravity over
+ * `steps` steps, screens the pair (running minimum of the sampled distance, or_ca_screen's rules)
+ * and refines the miss distance and TCA (or_ca_refine's Hermite and secant); then does the same
+ * with each of the 12 initial-state components moved by +-dr (positions, m) or +-dv (velocities,
+ * m/s), the moves applied in long double. Outputs per pair: miss, tca, and grad[12] = central
+ * differences d miss / d(r0_A, v0_A, r0_B, v0_B). Returns 0 on success. */
+int32_t or_miss_fd_ld(const void* data, const or_time* start, double h, int32_t steps, int32_t ncorr,
+    int64_t n_pairs, const double* rA, const double* vA, const double* rB, const double* vB, double dr,
+    double dv, double* miss, double* tca, double* grad, int32_t threads);
+
 #ifdef __cplusplus
 }
 #endif

@@ -475,3 +475,20 @@ def test_ca_multi_object_sets():
     i02 = _map_idx(p, 0, 2)
     assert abs(res["distance"][i01] - 5.0) < 1e-14 and abs(res["time"][i01] - 10.0) < 1e-14
     assert abs(res["distance"][i02] - 3.0) < 1e-14 and abs(res["time"][i02] - 4.0) < 1e-14
+
+
+def test_long_double_miss_matches_double_oracle(oracle_data):
+    # the extended-precision copy of the oracle's propagation, screen and refinement (used only for
+    # finite differences) agrees with the double oracle on the miss distance and TCA of a pair
+    from opengpop_b200 import orbits
+    r, v, pairs = orbits.conjunction_pairs(2, 20240101)
+    a, b = pairs[0]
+    start, h, steps = (2024, 1, 1, 0, 0, 0.0), 30.0, 60
+    m_ld, t_ld, grad = O.miss_fd_ld(oracle_data, start, h, steps, r[a], v[a], r[b], v[b], 1.0, 1e-3)
+    _, _, rs, vs, as_ = O.propagate(oracle_data, "gravity", start, h, steps, r[[a, b]], v[[a, b]],
+                                    per_step=True)
+    o = O.closest_approach(rs, vs, as_, np.array([0, 1], np.uint32), h)
+    assert abs(m_ld[0] - o["distance"][0]) <= 1e-9 * o["distance"][0]
+    assert abs(t_ld[0] - o["time"][0]) <= 1e-6
+    # d miss / d r0_A along the line of sight is close to the unit vector early on: bounded, finite
+    assert np.all(np.isfinite(grad)) and np.linalg.norm(grad[0, :3]) < 10.0
