@@ -120,8 +120,10 @@ void gpop_propagator_destroy(gpop_propagator* p);
  * one fixed device array of the library (about 4.1 MB on every GPU that loads it, until exit), so
  * calls are limited to GPOP_NOALLOC_MAX_OBJECTS objects and GPOP_NOALLOC_MAX_STEPS steps; larger
  * requests return GPOP_ERR_INVALID_ARG. All calls share that array: calls that overlap on the GPU
- * race. The first call on a device looks the array up (cudaGetSymbolAddress) and should come
- * before any stream capture. */
+ * race. Every call looks the array's device address up (cudaGetSymbolAddress, which allocates
+ * nothing), so calls stay correct across a cudaDeviceReset; the first call on a device also loads
+ * the library's device code and should come before any stream capture. The call waits for its
+ * own work to finish before it returns. Same walk, tables and results as gpop_propagate_device. */
 #define GPOP_NOALLOC_MAX_OBJECTS 4096
 #define GPOP_NOALLOC_MAX_STEPS 20160
 gpop_status gpop_propagate_device_noalloc(gpop_ctx* ctx, const gpop_time* start, double h,

@@ -13,15 +13,18 @@
 // exits). Every call shares the one array and finds the previous call's contents in it; calls that
 // overlap on the GPU (several streams, threads or contexts at once) race on it.
 //
-// Set-up: the array's device address is looked up with cudaGetSymbolAddress the first time the
-// entry point runs on a device (with that device current) and cached; that first call on each
-// device should therefore come before any stream capture.
+// Set-up: every call looks the array's device address up with cudaGetSymbolAddress, with the
+// context's device current. The address belongs to the CUDA context that loaded the library's
+// device code; a cudaDeviceReset (which test harnesses written for the reference call between
+// cases) makes a new context whose array may lie elsewhere, so a cached address could go stale.
+// The lookup is a host-side query that allocates nothing. The first call on a device also loads
+// the device code, so that first call should come before any stream capture. Each call waits for
+// its own work (it reads the device error word back) before it returns.
 #include "common.cuh"
 #include "context.h"
 
 #include <algorithm>
 #include <cmath>
-#include <mutex>
 #include <string>
 
 using namespace gpop;
@@ -42,9 +45,6 @@ constexpr size_t kOffErr = kOffPropSec + kMaxEpochs;
 constexpr size_t kScratchDoubles = kOffErr + 1;
 
 static __device__ __align__(256) double g_noalloc_scratch[kScratchDoubles];
-
-std::mutex g_setup_mutex;
-void* g_scratch_addr[64] = {};
 
 __device__ const double kNodesDev[10]
     = { 0.0, 4.0 / 27.0, 2.0 / 9.0, 1.0 / 3.0, 1.0 / 2.0, 2.0 / 3.0, 1.0 / 6.0, 1.0, 5.0 / 6.0, 1.0 };
@@ -68,20 +68,16 @@ __global__ void epoch_args_kernel(double sec, double h, int count, bool fix_q1, 
         prop_sec[i] = __dadd_rn(base, __dmul_rn((double)i, h));
 }
 
+// The scratch array's device address in the current CUDA context (the caller has made the
+// context's device current). Host code must not use g_noalloc_scratch itself: there it names a
+// host-side stand-in, not device memory.
 gpop_status scratch_address(gpop_ctx* ctx, double** out)
 {
-    const int dev = ctx->cfg.device;
-    if (dev < 0 || dev >= 64)
-        return fail(ctx, GPOP_ERR_INVALID_ARG, "device ordinal out of range for the no-alloc path");
-    std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_addr[dev]) {
-        void* p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || !p)
-            return cuda_fail(ctx, e, "cudaGetSymbolAddress(no-alloc scratch)");
-        g_scratch_addr[dev] = p;
-    }
-    *out = static_cast<double*>(g_scratch_addr[dev]);
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+        return cuda_fail(ctx, e, "cudaGetSymbolAddress(no-alloc scratch)");
+    *out = static_cast<double*>(p);
     return GPOP_OK;
 }
 
@@ -126,7 +122,9 @@ extern "C" gpop_status gpop_propagate_device_noalloc(gpop_ctx* ctx, const gpop_t
             != cudaSuccess)
         return cuda_fail(ctx, e, "epoch tables");
     const bool mixed = ctx->cfg.precision == GPOP_MIXED;
-    TableSrc ts = ctx->table(mixed);
+    // the same walk and tables as gpop_propagate_device (both built when the context was made)
+    const TableSrc ts = ctx->table(mixed);
+    const TableSrc lane_ts = ctx->lane_table(mixed);
     PropArgs a;
     a.n = n;
     a.h = h;
@@ -148,7 +146,8 @@ extern "C" gpop_status gpop_propagate_device_noalloc(gpop_ctx* ctx, const gpop_t
         const bool last = a.step_end == steps + 1;
         a.out_r = last ? r_dev : nullptr;
         a.out_v = last ? v_dev : nullptr;
-        if ((e = launch_gj8(ts, a, ctx->num_sms, s, ctx->block_override)) != cudaSuccess)
+        if ((e = launch_gj8(ts, a, ctx->num_sms, s, ctx->block_override, ctx->walk_mode, &lane_ts))
+            != cudaSuccess)
             return cuda_fail(ctx, e, "GJ8 kernel");
     }
     ctx->launches += 4 + (steps + chunk - 1) / chunk;
