@@ -6,6 +6,7 @@
 // chdir()s into a directory two levels below a data/ copy before calling in.
 #include "closest_approach/closest_approach.cuh"
 #include "force_model/force_model.cuh"
+#include "force_model/time_points/time_points.cuh"
 #include "gpu_propagator/gpu_propagator.cuh"
 
 #include <cstring>
@@ -100,6 +101,31 @@ int ref_closest_approach(int year, int month, int day, int hour, int min, double
     *num_out = k;
     cublasDestroy(handle);
     return cudaGetLastError() == cudaSuccess ? 0 : 2;
+}
+
+// FMTimePoints::Initialize + CalculateParameters (time_points.cu:26-71,126-201: the per-epoch
+// TimePointParamsKernel and the seven batched DGEMMs of ComputeITRStoGCRS): count ITRS->GCRS
+// matrices (column-major, 9 each) and UTC MJDs into host buffers.
+int ref_frame_matrices(int year, int month, int day, int hour, int min, double sec, double h,
+    int count, int use_midpoints, int before_epoch, double* m_out, double* mjd_out)
+{
+    cublasHandle_t handle;
+    if (cublasCreate(&handle) != CUBLAS_STATUS_SUCCESS)
+        return 1;
+    int rc = 0;
+    {
+        FMTimePoints tp(&handle, h, TimeData { year, month, day, hour, min, sec });
+        tp.Initialize();
+        tp.CalculateParameters(count, use_midpoints != 0, before_epoch);
+        TimePointParameters p = tp.GetParametersDev(0);
+        if (cudaMemcpy(m_out, p.ITRS_to_GCRS, (size_t)count * 9 * sizeof(double), cudaMemcpyDeviceToHost)
+                != cudaSuccess
+            || cudaMemcpy(mjd_out, p.mjd, (size_t)count * sizeof(double), cudaMemcpyDeviceToHost)
+                != cudaSuccess)
+            rc = 2;
+    }
+    cublasDestroy(handle);
+    return rc == 0 && cudaGetLastError() == cudaSuccess ? 0 : 2;
 }
 
 } // extern "C"

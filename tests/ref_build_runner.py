@@ -25,6 +25,13 @@ def available():
     return os.path.exists(LIB)
 
 
+def frames(start, h, count, midpoints=False, before=4):
+    """The reference's own per-epoch ITRS->GCRS matrices [count, 9] (column-major) and UTC MJDs."""
+    out = run("frames", start, h, 0, np.zeros((1, 3)), np.zeros((1, 3)), count=count,
+              midpoints=int(midpoints), before=before)
+    return out["m"], out["mjd"]
+
+
 def _stage_data(tmp, degree):
     d = os.path.join(tmp, "data")
     os.makedirs(d)
@@ -56,7 +63,15 @@ def child(inp, outp):
         n = r.shape[0]
         ms = C.c_double()
         vp = C.c_void_p
-        if str(z["mode"]) == "propagate":
+        if str(z["mode"]) == "frames":
+            cnt = int(z["count"])
+            m = np.zeros((cnt, 9))
+            mjd = np.zeros(cnt)
+            lib.ref_frame_matrices.argtypes = [C.c_int] * 5 + [C.c_double, C.c_double] + [C.c_int] * 3 + [vp, vp]
+            rc = lib.ref_frame_matrices(*st, float(z["h"]), cnt, int(z["midpoints"]),
+                                        int(z["before"]), m.ctypes.data_as(vp), mjd.ctypes.data_as(vp))
+            np.savez(outp, rc=rc, m=m, mjd=mjd, ms=0.0)
+        elif str(z["mode"]) == "propagate":
             ro = np.zeros_like(r)
             vo = np.zeros_like(v)
             lib.ref_propagate.argtypes = [C.c_int] * 5 + [C.c_double, C.c_double, C.c_int, C.c_int,
@@ -92,7 +107,7 @@ def child(inp, outp):
         shutil.rmtree(tmp, ignore_errors=True)
 
 
-def run(mode, start, h, steps, r, v, set_ids=None, degree=70, timeout=1800):
+def run(mode, start, h, steps, r, v, set_ids=None, degree=70, timeout=1800, **extra):
     """Runs the reference build in a child process; returns the result arrays."""
     tmp = tempfile.mkdtemp(prefix="gpop_refio_")
     try:
@@ -102,6 +117,7 @@ def run(mode, start, h, steps, r, v, set_ids=None, degree=70, timeout=1800):
                   r=np.asarray(r, float), v=np.asarray(v, float), degree=degree)
         if set_ids is not None:
             kw["set_ids"] = np.asarray(set_ids, np.uint32)
+        kw.update(extra)
         np.savez(inp, **kw)
         p = subprocess.run([sys.executable, os.path.abspath(__file__), inp, outp],
                            capture_output=True, text=True, timeout=timeout)

@@ -269,3 +269,33 @@ def test_invalid_pairs_rejected(ctx):
     for bad in ([[0, 0]], [[0, 99]], [[-1, 2]]):
         with pytest.raises(G.GpopError):
             ctx.miss_gradient(START, 30.0, 10, r, v, np.array(bad, np.int32))
+
+
+def test_miss_gradient_at_configuration_steps_long_double_fd(ctx, oracle_data):
+    """The differentiation configuration (24 h, 30 s steps, 70x70, FP64) on three of its seeded
+    pairs: the adjoint gradient of each miss distance against central differences at the
+    configuration's steps (1e-3 m, 1e-6 m/s), taken in long double by the oracle so that the
+    difference quotient is not limited by double rounding noise. Bound 1e-5 relative per
+    (object, position | velocity) block."""
+    from opengpop_b200 import orbits
+    r, v, pairs = orbits.conjunction_pairs(10000, 20240101)
+    pairs = pairs[:3]
+    objs = np.unique(pairs)
+    remap = {int(o): i for i, o in enumerate(objs)}
+    sub = np.array([[remap[int(a)], remap[int(b)]] for a, b in pairs], np.int32)
+    steps = 2880
+    tca, miss, grad = ctx.miss_gradient(START, 30.0, steps, r[objs], v[objs], sub)
+    a, b = pairs[:, 0], pairs[:, 1]
+    m_ld, t_ld, fd = O.miss_fd_ld(oracle_data, START, 30.0, steps, r[a], v[a], r[b], v[b],
+                                  H_R_CFG, H_V_CFG)
+    assert np.allclose(miss, m_ld, rtol=1e-9, atol=1e-4) and np.allclose(tca, t_ld, rtol=0, atol=1e-4)
+    worst = 0.0
+    for p in range(len(pairs)):
+        for blk in range(4):
+            g = grad[p, 3 * blk:3 * blk + 3]
+            f = fd[p, 3 * blk:3 * blk + 3]
+            err = np.linalg.norm(g - f) / np.linalg.norm(f)
+            worst = max(worst, err)
+            assert err <= 1e-5, (p, blk, g, f)
+    print("\nadjoint vs long double central differences (1e-3 m, 1e-6 m/s), 24 h: max relative "
+          "error %.2e" % worst)
