@@ -83,6 +83,10 @@ int32_t gpop_gravity_degree(const gpop_ctx* ctx);
 int64_t gpop_kernel_launches(const gpop_ctx* ctx);
 
 /* ---- propagation ---- */
+/* Input states: where the reference exits (gpu_utils.cuh:28-48) or propagates bad values into
+ * NaNs, these calls return GPOP_ERR_INVALID_ARG for a state with a non-finite component or a
+ * position at the origin. Host inputs are checked before any work; device inputs by the startup
+ * kernel, which still propagates the other objects and writes their results. */
 /* exec propagate (exec/runner.cu:11-70) / GpuPropagator::Step x steps + CopyStateToHost
  * (gpu_propagator.cu:28-84): host AoS buffers [n][3] in metres and m/s (GCRS). */
 gpop_status gpop_propagate(gpop_ctx* ctx, const gpop_time* start, double h, int32_t steps, int64_t n,
@@ -153,8 +157,17 @@ typedef struct {
  * one persistent launch: the reference runs one GpuPropagator per request (gpu_propagator.cu:
  * 121-136), i.e. one exec propagate call each. Results equal those of gpop_propagate per request
  * to rounding. The launch sequence is captured in a CUDA graph and replayed when the next batch
- * has the same shape. */
+ * has the same shape. A request that cannot run (invalid arguments; an object whose position or
+ * velocity is not finite, or whose position is the origin) is refused alone: the others are
+ * propagated and written, its outputs are left untouched, and the call returns
+ * GPOP_ERR_INVALID_ARG naming the first refused request. */
 gpop_status gpop_propagate_batch(gpop_ctx* ctx, const gpop_request* reqs, int32_t n_req);
+/* No counterpart in the reference (which exits on bad input, gpu_utils.cuh:28-48).
+ * gpop_propagate_batch with one status per request in status[n_req] (NULL: none): GPOP_OK for
+ * the propagated requests, GPOP_ERR_INVALID_ARG for the refused ones; when the batch itself fails,
+ * its status for every request that was to run. */
+gpop_status gpop_propagate_batch_status(gpop_ctx* ctx, const gpop_request* reqs, int32_t n_req,
+    int32_t* status);
 /* The batch plan: lanes per object chosen for each request and the estimated makespan (s). */
 gpop_status gpop_batch_plan(gpop_ctx* ctx, const gpop_request* reqs, int32_t n_req,
     int32_t* lanes_per_object, double* est_seconds);

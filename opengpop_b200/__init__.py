@@ -30,7 +30,7 @@ EXPORTS = (
     "gpop_gravity_degree", "gpop_kernel_launches", "gpop_propagate", "gpop_propagate_device",
     "gpop_propagate_device_noalloc", "gpop_propagate_trajectory", "gpop_propagator_create", "gpop_propagator_step",
     "gpop_propagator_steps_done", "gpop_propagator_destroy", "gpop_propagate_analytic",
-    "gpop_propagate_batch", "gpop_batch_plan", "gpop_tune", "gpop_batch_device_seconds", "gpop_gravity_jacobian", "gpop_stm", "gpop_propagate_vjp",
+    "gpop_propagate_batch", "gpop_propagate_batch_status", "gpop_batch_plan", "gpop_tune", "gpop_batch_device_seconds", "gpop_gravity_jacobian", "gpop_stm", "gpop_propagate_vjp",
     "gpop_miss_gradient", "gpop_sample_states", "gpop_startup", "gpop_corrector_unit",
     "gpop_predict_unit", "gpop_finalize_correction_unit", "gpop_rk8_stage", "gpop_rk8_finish",
     "gpop_startup_init", "gpop_startup_correct", "gpop_gj8_predict", "gpop_gj8_correct",
@@ -103,6 +103,7 @@ def load_library(path=LIB_PATH):
         "gpop_propagator_destroy": (None, [_VP]),
         "gpop_propagate_analytic": (i32, [_VP, i32, f64, i32, i32, i64] + [_VP] * 6),
         "gpop_propagate_batch": (i32, [_VP, _VP, i32]),
+        "gpop_propagate_batch_status": (i32, [_VP, _VP, i32, _VP]),
         "gpop_batch_plan": (i32, [_VP, _VP, i32, _VP, C.POINTER(f64)]),
         "gpop_tune": (i32, [_VP, C.c_char_p]),
         "gpop_batch_device_seconds": (f64, [_VP]),
@@ -322,6 +323,17 @@ class Context:
         arr, keep = self._requests(reqs)
         self._check(load_library().gpop_propagate_batch(self._h, arr, len(reqs)))
         return [(k[2], k[3]) for k in keep]
+
+    def propagate_batch_status(self, reqs):
+        """Requests that cannot run are refused alone. Returns ([(r_end, v_end) or None per
+        request], per-request status array, the call's status, its error message or None)."""
+        arr, keep = self._requests(reqs)
+        status = np.zeros(len(reqs), np.int32)
+        st = load_library().gpop_propagate_batch_status(self._h, arr, len(reqs),
+                                                        status.ctypes.data_as(_VP))
+        msg = None if st == OK else load_library().gpop_last_error(self._h).decode()
+        out = [(k[2], k[3]) if status[i] == OK else None for i, k in enumerate(keep)]
+        return out, status, st, msg
 
     def batch_plan(self, reqs):
         arr, keep = self._requests(reqs)

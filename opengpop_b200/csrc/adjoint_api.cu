@@ -34,6 +34,9 @@ gpop_status check_common(gpop_ctx* ctx, const gpop_time* start, double h, int32_
         return fail(ctx, GPOP_ERR_INVALID_ARG, "invalid propagation arguments");
     if (n > (int64_t)1 << 24)
         return fail(ctx, GPOP_ERR_INVALID_ARG, "too many objects");
+    const int64_t bad = first_bad_state(static_cast<const double*>(r_in), static_cast<const double*>(v_in), n, true);
+    if (bad >= 0)
+        return bad_state(ctx, bad, "object");
     if (ctx->cfg.n_corrections < 1)
         return fail(ctx, GPOP_ERR_UNSUPPORTED, "the adjoint needs at least one corrector pass");
     cudaError_t e = cudaSetDevice(ctx->cfg.device);

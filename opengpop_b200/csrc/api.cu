@@ -89,10 +89,37 @@ gpop_status check_device_errors(gpop_ctx* ctx, cudaStream_t s)
         cudaMemsetAsync(ctx->err_word.p, 0, sizeof(unsigned), s);
         cudaStreamSynchronize(s);
         if (word & kErrTmaTimeout)
-            return fail(ctx, GPOP_ERR_TIMEOUT, "gravity table staging timed out on the device");
+            return fail(ctx, GPOP_ERR_TIMEOUT,
+                (word & kErrTmaUnfinished)
+                    ? "gravity table staging timed out on the device; a copy was still in flight when its block left"
+                    : "gravity table staging timed out on the device; every copy had landed when its block left");
+        if (word & kErrBadInput)
+            return fail(ctx, GPOP_ERR_INVALID_ARG,
+                "an initial state on the device is not finite or lies at the origin (the other "
+                "objects were propagated)");
         return fail(ctx, GPOP_ERR_CUDA, "device error word " + std::to_string(word));
     }
     return GPOP_OK;
+}
+
+int64_t first_bad_state(const double* r, const double* v, int64_t n, bool radius)
+{
+    for (int64_t i = 0; i < n; ++i) {
+        const double* p = r + 3 * i;
+        const double* q = v + 3 * i;
+        if (!std::isfinite(p[0]) || !std::isfinite(p[1]) || !std::isfinite(p[2]) || !std::isfinite(q[0])
+            || !std::isfinite(q[1]) || !std::isfinite(q[2]))
+            return i;
+        if (radius && p[0] == 0.0 && p[1] == 0.0 && p[2] == 0.0)
+            return i;
+    }
+    return -1;
+}
+
+gpop_status bad_state(gpop_ctx* ctx, int64_t i, const char* what)
+{
+    return fail(ctx, GPOP_ERR_INVALID_ARG,
+        std::string(what) + " " + std::to_string(i) + ": position or velocity not finite, or position at the origin");
 }
 
 static bool valid_time(const gpop_time* t)
@@ -244,6 +271,8 @@ gpop_status gpop_create(const gpop_config* cfg_in, gpop_ctx** out)
         ctx->steps_per_launch = std::max(1, atoi(spl));
     if (const char* wm = std::getenv("GPOP_WALK_MODE"))
         ctx->walk_mode = std::min(4, std::max(0, atoi(wm)));
+    if (const char* ws = std::getenv("GPOP_TEST_FIRST_WAIT_SPINS"))
+        ctx->first_wait_spins = (uint32_t)std::min(1L << 22, std::max(0L, atol(ws)));
     cudaError_t e = cudaSetDevice(cfg.device);
     if (e != cudaSuccess)
         return cuda_fail(ctx, e, "cudaSetDevice");
@@ -452,6 +481,9 @@ gpop_status gpop_propagate(gpop_ctx* ctx, const gpop_time* start, double h, int3
         return GPOP_ERR_INVALID_ARG;
     if (n <= 0 || !r_in || !v_in || !r_out || !v_out)
         return fail(ctx, GPOP_ERR_INVALID_ARG, "invalid buffers");
+    const int64_t bad = first_bad_state(r_in, v_in, n, true);
+    if (bad >= 0)
+        return bad_state(ctx, bad, "object");
     cudaError_t e = cudaSetDevice(ctx->cfg.device);
     if (e != cudaSuccess)
         return cuda_fail(ctx, e, "cudaSetDevice");

@@ -38,7 +38,7 @@ __device__ __forceinline__ bool stage_batch_table(uint8_t* smem, const TableSrc&
 {
     uint64_t* mbar = reinterpret_cast<uint64_t*>(smem);
     uint8_t* tab = smem + 128;
-    const bool ok = stage_to_smem(tab, ts.src, ts.bytes, mbar, err);
+    const bool ok = stage_to_smem(tab, ts.src, ts.bytes, mbar, err, ts.wait_spins);
     g.L = ts.L;
     g.Lt = ts.L;
     g.radius = ts.radius;

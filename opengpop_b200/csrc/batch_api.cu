@@ -200,18 +200,30 @@ struct TableKey {
     }
 };
 
+// Why request q cannot run (empty when it can): bad arguments, or an object whose position or
+// velocity is not finite or whose position is the origin.
+std::string request_problem(const gpop_request& q)
+{
+    const gpop_time& t = q.start;
+    if (q.n <= 0 || !q.r_in || !q.v_in || !q.r_out || !q.v_out || q.steps < 0 || !(q.h > 0.0)
+        || !std::isfinite(q.h) || t.month < 1 || t.month > 12 || t.day < 1 || t.day > 31 || !std::isfinite(t.sec))
+        return "invalid arguments";
+    if (q.n > (int64_t)1 << 24)
+        return "too many objects";
+    const int64_t bad = first_bad_state(q.r_in, q.v_in, q.n, true);
+    if (bad >= 0)
+        return "object " + std::to_string(bad) + " has a position or velocity that is not finite, or a position at the origin";
+    return std::string();
+}
+
 gpop_status validate(gpop_ctx* ctx, const gpop_request* reqs, int32_t n_req)
 {
     if (!reqs || n_req <= 0)
         return fail(ctx, GPOP_ERR_INVALID_ARG, "empty batch");
     for (int32_t i = 0; i < n_req; ++i) {
-        const gpop_request& q = reqs[i];
-        const gpop_time& t = q.start;
-        if (q.n <= 0 || !q.r_in || !q.v_in || !q.r_out || !q.v_out || q.steps < 0 || !(q.h > 0.0)
-            || !std::isfinite(q.h) || t.month < 1 || t.month > 12 || t.day < 1 || t.day > 31 || !std::isfinite(t.sec))
-            return fail(ctx, GPOP_ERR_INVALID_ARG, "invalid request " + std::to_string(i));
-        if (q.n > (int64_t)1 << 24)
-            return fail(ctx, GPOP_ERR_INVALID_ARG, "request " + std::to_string(i) + " has too many objects");
+        const std::string why = request_problem(reqs[i]);
+        if (!why.empty())
+            return fail(ctx, GPOP_ERR_INVALID_ARG, "request " + std::to_string(i) + ": " + why);
     }
     return GPOP_OK;
 }
@@ -273,13 +285,11 @@ gpop_status gpop_batch_plan(gpop_ctx* ctx, const gpop_request* reqs, int32_t n_r
     return GPOP_OK;
 }
 
-gpop_status gpop_propagate_batch(gpop_ctx* ctx, const gpop_request* reqs, int32_t n_req)
+} // extern "C"
+
+// The batch proper, over requests that have passed request_problem.
+static gpop_status run_batch(gpop_ctx* ctx, const gpop_request* reqs, int32_t n_req)
 {
-    if (!ctx)
-        return GPOP_ERR_INVALID_ARG;
-    gpop_status st = validate(ctx, reqs, n_req);
-    if (st != GPOP_OK)
-        return st;
     cudaError_t e = cudaSetDevice(ctx->cfg.device);
     if (e != cudaSuccess)
         return cuda_fail(ctx, e, "cudaSetDevice");
@@ -513,7 +523,7 @@ gpop_status gpop_propagate_batch(gpop_ctx* ctx, const gpop_request* reqs, int32_
     if ((e = cudaMemcpyAsync(host + 6 * N, dio + 6 * N, (size_t)N * 6 * sizeof(double), cudaMemcpyDeviceToHost, s))
         != cudaSuccess)
         return cuda_fail(ctx, e, "batch download");
-    st = check_device_errors(ctx, s);
+    const gpop_status st = check_device_errors(ctx, s);
     if (st != GPOP_OK)
         return st;
     ctx->batch_seconds = timer.seconds(0, 1);
@@ -524,6 +534,57 @@ gpop_status gpop_propagate_batch(gpop_ctx* ctx, const gpop_request* reqs, int32_
         std::copy(host + 9 * N + 3 * obj0[i], host + 9 * N + 3 * (obj0[i] + n[i]), reqs[i].v_out);
     }
     return GPOP_OK;
+}
+
+extern "C" {
+
+gpop_status gpop_propagate_batch_status(gpop_ctx* ctx, const gpop_request* reqs, int32_t n_req,
+    int32_t* status)
+{
+    if (!ctx)
+        return GPOP_ERR_INVALID_ARG;
+    if (!reqs || n_req <= 0)
+        return fail(ctx, GPOP_ERR_INVALID_ARG, "empty batch");
+    // a request that cannot run is refused alone; the others run as one batch
+    std::vector<gpop_request> good;
+    std::vector<int32_t> good_idx;
+    good.reserve(n_req);
+    int32_t first_bad = -1, refused = 0;
+    std::string why_first;
+    for (int32_t i = 0; i < n_req; ++i) {
+        const std::string why = request_problem(reqs[i]);
+        if (why.empty()) {
+            good.push_back(reqs[i]);
+            good_idx.push_back(i);
+        } else {
+            ++refused;
+            if (first_bad < 0) {
+                first_bad = i;
+                why_first = why;
+            }
+        }
+        if (status)
+            status[i] = why.empty() ? GPOP_OK : GPOP_ERR_INVALID_ARG;
+    }
+    if (!good.empty()) {
+        const gpop_status st = run_batch(ctx, good.data(), (int32_t)good.size());
+        if (st != GPOP_OK) {
+            if (status)
+                for (int32_t i : good_idx)
+                    status[i] = st;
+            return st;
+        }
+    }
+    if (first_bad >= 0)
+        return fail(ctx, GPOP_ERR_INVALID_ARG,
+            "request " + std::to_string(first_bad) + ": " + why_first + " (" + std::to_string(refused) + " of "
+                + std::to_string(n_req) + " requests refused; the others were propagated)");
+    return GPOP_OK;
+}
+
+gpop_status gpop_propagate_batch(gpop_ctx* ctx, const gpop_request* reqs, int32_t n_req)
+{
+    return gpop_propagate_batch_status(ctx, reqs, n_req, nullptr);
 }
 
 double gpop_batch_device_seconds(const gpop_ctx* ctx) { return ctx ? ctx->batch_seconds : -1.0; }

@@ -262,6 +262,11 @@ gpop_status gpop_ca_create(gpop_ctx* ctx, const gpop_time* start, double h, int6
         return fail(ctx, GPOP_ERR_INVALID_ARG, "invalid setIndices: at least 2 sets are required");
     if (set_ids[0] != 0)
         return fail(ctx, GPOP_ERR_INVALID_ARG, "invalid setIndices: they must start at 0");
+    // non-finite states are refused here; a position at the origin only where gravity is evaluated
+    // (the startup kernel flags it, and gpop_ca_propagate fails)
+    const int64_t bad = first_bad_state(r_in, v_in, n, false);
+    if (bad >= 0)
+        return bad_state(ctx, bad, "object");
     gpop_ca* ca = new (std::nothrow) gpop_ca();
     if (!ca)
         return fail(ctx, GPOP_ERR_NOMEM, "closest approach");

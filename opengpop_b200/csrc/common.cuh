@@ -8,7 +8,8 @@ namespace gpop {
 // Error bits a kernel may raise in the context's device error word.
 enum : unsigned {
     kErrTmaTimeout = 1u, // the bounded wait on the gravity-table bulk copy gave up
-    kErrBadInput = 2u, // non-finite or zero-radius position met by the force model
+    kErrBadInput = 2u, // a state with a non-finite component, or a position at the origin
+    kErrTmaUnfinished = 4u, // a staging copy had still not landed when its block gave up and left
 };
 
 // ---- bulk-copy (TMA, cp.async.bulk) staging of a read-only table into shared memory ----
@@ -19,9 +20,11 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p)
 
 // Copies `bytes` (multiple of 16, both addresses 16-byte aligned) from global to shared memory with
 // one elected thread issuing cp.async.bulk chunks that complete on an mbarrier. Every thread of the
-// block waits with a bounded spin; on timeout the block's error bit is raised and false returned.
+// block waits with a bounded spin of first_spins polls; when that runs out the block raises
+// kErrTmaTimeout and returns false after a second bounded wait for the copies still in flight
+// (kErrTmaUnfinished if they have not landed by then either: the caller's results are void).
 __device__ __forceinline__ bool stage_to_smem(void* smem_dst, const void* gsrc, uint32_t bytes,
-    uint64_t* mbar, unsigned* err_word)
+    uint64_t* mbar, unsigned* err_word, uint32_t first_spins)
 {
     const uint32_t bar = smem_u32(mbar);
     if (threadIdx.x == 0) {
@@ -46,7 +49,7 @@ __device__ __forceinline__ bool stage_to_smem(void* smem_dst, const void* gsrc, 
     }
     // bounded wait on phase 0 (about a second at the sleep below before giving up)
     uint32_t done = 0;
-    for (int it = 0; it < (1 << 22) && !done; ++it) {
+    for (uint32_t it = 0; it < first_spins && !done; ++it) {
         asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n"
                      " selp.u32 %0, 1, 0, p;\n}"
                      : "=r"(done)
@@ -68,6 +71,8 @@ __device__ __forceinline__ bool stage_to_smem(void* smem_dst, const void* gsrc, 
             if (!done)
                 __nanosleep(64);
         }
+        if (!done && threadIdx.x == 0)
+            atomicOr(err_word, kErrTmaUnfinished);
         return false;
     }
     return true;

@@ -79,6 +79,9 @@ struct gpop_ctx {
     int steps_per_launch = 64;
     int block_override = 0; // GJ8 block size chosen by the tuner (0 = default policy)
     int walk_mode = 0; // GJ8 triangle walk (WalkMode; 0 = default)
+    // first staging wait of every kernel (TableSrc::wait_spins); GPOP_TEST_FIRST_WAIT_SPINS, a
+    // test setting, lowers it so that a test can watch the wait give up
+    uint32_t first_wait_spins = 1u << 22;
     // device-resident model data
     gpop::DevBuf t64, mixed, nut, eop, leap, err_word;
     uint32_t t64_bytes = 0, mixed_bytes = 0, mixed_off32 = 0;
@@ -111,6 +114,7 @@ struct gpop_ctx {
         ts.src = mixed_mode ? lane_mixed.p : lane64.p;
         ts.bytes = mixed_mode ? lane_mixed_bytes : lane64_bytes;
         ts.off32 = mixed_mode ? lane_mixed_off32 : lane64_off32;
+        ts.wait_spins = first_wait_spins;
         return ts;
     }
 
@@ -130,6 +134,7 @@ struct gpop_ctx {
             ts.bytes = t64_bytes;
             ts.off32 = 0;
         }
+        ts.wait_spins = first_wait_spins;
         return ts;
     }
 };
@@ -172,6 +177,12 @@ gpop_status propagator_step(gpop_propagator* p, int steps, double* traj_r, doubl
     double* traj_a, cudaStream_t s);
 // Reads and clears the device error word (synchronises the stream).
 gpop_status check_device_errors(gpop_ctx* ctx, cudaStream_t s);
+// Index of the first object of n (host [n][3] arrays) whose position or velocity has a component
+// that is not finite, or, when `radius` is set, whose position is the origin (where gravity is
+// undefined); -1 when every object is usable. The reference takes such states without a check.
+int64_t first_bad_state(const double* r, const double* v, int64_t n, bool radius);
+// GPOP_ERR_INVALID_ARG naming object i of `what`.
+gpop_status bad_state(gpop_ctx* ctx, int64_t i, const char* what);
 // Frees the batch cache, stream and staging buffer of a context.
 void destroy_batch_cache(gpop_ctx* ctx);
 } // namespace gpop

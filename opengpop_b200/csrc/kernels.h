@@ -15,6 +15,9 @@ struct TableSrc {
     double radius = 0, gm = 0;
     bool mixed = false;
     bool lanes = false; // lane layout (build_lane_blob): column bases, FP64 at kLaneOff64, FP32 at off32
+    // spins of the first bounded wait on the staging copy (2^22, about a second; a test setting
+    // lowers it to make the wait give up on purpose)
+    uint32_t wait_spins = 1u << 22;
 };
 
 // Byte offset, in a kernel's dynamic shared memory, of what follows a staged table (the 128-byte

@@ -156,7 +156,13 @@ extern "C" gpop_status gpop_propagate_device_noalloc(gpop_ctx* ctx, const gpop_t
         || (e = cudaStreamSynchronize(s)) != cudaSuccess)
         return cuda_fail(ctx, e, "no-alloc propagation");
     if (word & kErrTmaTimeout)
-        return fail(ctx, GPOP_ERR_TIMEOUT, "gravity table staging timed out on the device");
+        return fail(ctx, GPOP_ERR_TIMEOUT,
+            (word & kErrTmaUnfinished)
+                ? "gravity table staging timed out on the device; a copy was still in flight when its block left"
+                : "gravity table staging timed out on the device; every copy had landed when its block left");
+    if (word & kErrBadInput)
+        return fail(ctx, GPOP_ERR_INVALID_ARG,
+            "an initial state is not finite or lies at the origin (the other objects were propagated)");
     if (word)
         return fail(ctx, GPOP_ERR_CUDA, "device error word " + std::to_string(word));
     return GPOP_OK;

@@ -106,7 +106,7 @@ __device__ __forceinline__ bool bind_table(uint8_t* smem, const TableSrc& ts, un
 {
     uint64_t* mbar = reinterpret_cast<uint64_t*>(smem);
     uint8_t* tab = smem + 128;
-    bool ok = stage_to_smem(tab, ts.src, ts.bytes, mbar, err);
+    bool ok = stage_to_smem(tab, ts.src, ts.bytes, mbar, err, ts.wait_spins);
     g.L = ts.L;
     g.Lt = ts.L;
     g.radius = ts.radius;
@@ -132,6 +132,15 @@ __global__ void __launch_bounds__(256) startup_kernel(F f, TableSrc ts, PropArgs
         r0[j] = a.r0[i * 3 + j];
         v0[j] = a.v0[i * 3 + j];
     }
+    // a state the force model cannot take (the reference propagates it into NaNs) fails the call;
+    // the object still runs, so every other object's result is written as usual
+    bool usable = true;
+    for (int j = 0; j < 3; ++j)
+        usable = usable && isfinite(r0[j]) && isfinite(v0[j]);
+    if (F::kTable && r0[0] == 0.0 && r0[1] == 0.0 && r0[2] == 0.0)
+        usable = false;
+    if (!usable && a.err)
+        atomicOr(a.err, kErrBadInput);
     StartupMats m;
     run_startup(f, a.h, a.ncorr, r0, v0, m);
     if (a.out27[0]) {
@@ -517,6 +526,8 @@ __global__ void __launch_bounds__(512, 1) gravity_kernel(TableSrc ts, int64_t n,
     if (i >= n)
         return;
     double p[3] = { r[i * 3], r[i * 3 + 1], r[i * 3 + 2] };
+    if (!isfinite(p[0]) || !isfinite(p[1]) || !isfinite(p[2]) || (p[0] == 0.0 && p[1] == 0.0 && p[2] == 0.0))
+        atomicOr(err, kErrBadInput);
     double acc[3];
     if (m9) {
         gravity_gcrs1<MIXED>(g, m9, p, acc);
