@@ -48,6 +48,10 @@ enum {
     GPOP_FIX_STARTUP_EXPORT_ACC = 1u << 1, /* Q3: gpu_propagator.cu:48-53,68-72 exports column 8 */
     GPOP_FIX_PHASE_EPOCH = 1u << 2, /* closest_approach.cu:134: each phase restarts the epoch */
 };
+/* No counterpart in the reference. Mixed precision only: the FP32 sums of the degree > 8 terms are
+ * compensated (TwoSum per added term) instead of summed in two levels; the propagation then walks
+ * one or two objects per thread (no lane split). Slower; for error studies. */
+enum { GPOP_MIXED_COMPENSATED = 1u << 3 };
 
 /* Analytic force models of the reference's test suite (unit_tests/include/gpu_test_helpers.cuh) */
 typedef enum {

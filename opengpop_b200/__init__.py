@@ -21,6 +21,7 @@ FP64, MIXED = 0, 1
 FIX_BACKWARD_RK8_EPOCH = 1
 FIX_STARTUP_EXPORT_ACC = 2
 FIX_PHASE_EPOCH = 4
+MIXED_COMPENSATED = 8
 FORCE = {"gravity": 0, "zero": 1, "const": 2, "poly7": 3, "poly8": 4, "poly9": 5, "exp": 6,
          "damped": 7}
 

@@ -5,6 +5,9 @@
 
 namespace gpop {
 
+// gpop_config.flags bit (GPOP_MIXED_COMPENSATED in gpop.h): compensated FP32 sums in mixed mode.
+constexpr unsigned kFlagMixedCompensated = 1u << 3;
+
 // Error bits a kernel may raise in the context's device error word.
 enum : unsigned {
     kErrTmaTimeout = 1u, // the bounded wait on the gravity-table bulk copy gave up

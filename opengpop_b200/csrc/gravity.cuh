@@ -887,12 +887,158 @@ __device__ __forceinline__ void gravity_itrs(const GravSmem& gs, const double (&
     }
 }
 
+// ---- mixed precision with compensated FP32 sums (GPOP_MIXED_COMPENSATED) ----
+// The same split as the mixed walk (terms of degree <= 8 in FP64, every term of degree > 8 in
+// FP32), with each FP32 column sum carried as a value and a compensation term: every product
+// Q(n) x coefficient is added by Knuth's TwoSum, whose rounding error goes into the compensation
+// (compensated summation). Each column's sum and compensation are then added to the FP64 column
+// sums and combined in FP64. The walk is plain (one column at a time); it exists to measure the
+// error and the cost of compensation against the two-level sums of the default mixed walk.
+
+// s + c <- s + c + p, with the rounding error of s + p kept in c (TwoSum; no contraction).
+__device__ __forceinline__ void two_sum_add(float& s, float& c, float p)
+{
+    const float t = __fadd_rn(s, p);
+    const float z = __fsub_rn(t, s);
+    const float e = __fadd_rn(__fsub_rn(s, __fsub_rn(t, z)), __fsub_rn(p, z));
+    s = t;
+    c = __fadd_rn(c, e);
+}
+
+// FP32 terms first..last of a column (entries e[first..last]) for K objects, continuing the
+// recursion from Q1 = Q(n-1), Q2 = Q(n-2), compensated sums into sum/cmp [k][g1 g2 j1 j2 h1 h2].
+template <int K>
+__device__ __forceinline__ void column32_comp(const GravEntry32* __restrict__ e, int first, int last,
+    const float (&u)[K], const float (&w)[K], float (&Q1)[K], float (&Q2)[K], float (&sum)[K][6],
+    float (&cmp)[K][6])
+{
+    for (int i = first; i <= last; ++i) {
+        const float4* p = reinterpret_cast<const float4*>(e + i);
+        const float4 a = p[0], b = p[1]; // (-c, -c, g1, g2 | j1, j2, h1, h2)
+        const float coef[6] = { a.z, a.w, b.x, b.y, b.z, b.w };
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const float t2 = (a.x * w[k]) * Q2[k];
+            const float Q = fmaf(u[k], Q1[k], t2);
+#pragma unroll
+            for (int c = 0; c < 6; ++c)
+                two_sum_add(sum[k][c], cmp[k][c], __fmul_rn(Q, coef[c]));
+            Q2[k] = Q1[k];
+            Q1[k] = Q;
+        }
+    }
+}
+
+template <int K>
+__device__ __forceinline__ void gravity_itrs_comp(const GravSmem& gs, const double (&x)[K],
+    const double (&y)[K], const double (&z)[K], double (&ax)[K], double (&ay)[K], double (&az)[K])
+{
+    const int L = gs.L;
+    double r[K], q[K], u[K], w[K], C1[K], S1[K], Cm[K], Sm[K], Cp[K], Sp[K], qm[K];
+    double G[K], H[K], J[K], KK[K];
+    float uf[K], wf[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        r[k] = sqrt(x[k] * x[k] + y[k] * y[k] + z[k] * z[k]);
+        const double eps = z[k] / r[k];
+        q[k] = gs.radius / r[k];
+        u[k] = q[k] * eps;
+        w[k] = q[k] * q[k];
+        C1[k] = x[k] / r[k];
+        S1[k] = y[k] / r[k];
+        Cm[k] = 1.0;
+        Sm[k] = 0.0;
+        Cp[k] = 0.0;
+        Sp[k] = 0.0;
+        qm[k] = 1.0;
+        G[k] = H[k] = J[k] = KK[k] = 0.0;
+        uf[k] = (float)u[k];
+        wf[k] = (float)w[k];
+    }
+    for (int m = 0; m <= L; ++m) {
+        ColSums64<K> s;
+        s.zero();
+        float sum[K][6], cmp[K][6], Q1f[K], Q2f[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+#pragma unroll
+            for (int c = 0; c < 6; ++c)
+                sum[k][c] = cmp[k][c] = 0.f;
+        const GravEntry32* e32 = gs.t32 + grav_col_offset(m, gs.Lt);
+        if (m <= kMixedSplit) { // FP64 terms n = m..8, then FP32 terms 9..L
+            double Q1[K], Q2[K];
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                Q1[k] = qm[k];
+                Q2[k] = 0.0;
+            }
+            const int top = L < kMixedSplit ? L : kMixedSplit;
+            const GravEntry64* e = gs.t64 + grav_col_offset(m, kMixedSplit);
+            s.add(e, Q1);
+            column64<K>(e, 1, top - m, u, w, Q1, Q2, s);
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                Q1f[k] = (float)Q1[k];
+                Q2f[k] = (float)Q2[k];
+            }
+            column32_comp<K>(e32, kMixedSplit + 1 - m, L - m, uf, wf, Q1f, Q2f, sum, cmp);
+        } else { // FP32 terms n = m..L: Q(m) = q^m, Q(m-1) = 0
+            const float4* p = reinterpret_cast<const float4*>(e32);
+            const float4 a = p[0], b = p[1];
+            const float coef[6] = { a.z, a.w, b.x, b.y, b.z, b.w };
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                const float Qm = (float)qm[k];
+#pragma unroll
+                for (int c = 0; c < 6; ++c)
+                    sum[k][c] = __fmul_rn(Qm, coef[c]);
+                Q1f[k] = Qm;
+                Q2f[k] = 0.f;
+            }
+            column32_comp<K>(e32, 1, L - m, uf, wf, Q1f, Q2f, sum, cmp);
+        }
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            s.g1[k] += (double)sum[k][0] + (double)cmp[k][0];
+            s.g2[k] += (double)sum[k][1] + (double)cmp[k][1];
+            s.j1[k] += (double)sum[k][2] + (double)cmp[k][2];
+            s.j2[k] += (double)sum[k][3] + (double)cmp[k][3];
+            s.h1[k] += (double)sum[k][4] + (double)cmp[k][4];
+            s.h2[k] += (double)sum[k][5] + (double)cmp[k][5];
+        }
+        const double dm = (double)m;
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            G[k] += Cm[k] * s.g1[k] + Sm[k] * s.g2[k];
+            J[k] += dm * (Cp[k] * s.j1[k] + Sp[k] * s.j2[k]);
+            KK[k] -= dm * (Sp[k] * s.j1[k] - Cp[k] * s.j2[k]);
+            H[k] += Cp[k] * s.h1[k] + Sp[k] * s.h2[k];
+            Cp[k] = Cm[k];
+            Sp[k] = Sm[k];
+            const double Cn = C1[k] * Cm[k] - S1[k] * Sm[k];
+            const double Sn = S1[k] * Cm[k] + C1[k] * Sm[k];
+            Cm[k] = Cn;
+            Sm[k] = Sn;
+            qm[k] *= q[k];
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < K; ++k) { // eq. 4-13
+        const double Gk = G[k] + 1.0;
+        const double Lambda = Gk + z[k] * H[k] / r[k];
+        const double c = -gs.gm / (r[k] * r[k]);
+        ax[k] = c * (Lambda * x[k] / r[k] - J[k]);
+        ay[k] = c * (Lambda * y[k] / r[k] - KK[k]);
+        az[k] = c * (Lambda * z[k] / r[k] - H[k]);
+    }
+}
+
 // GCRS accelerations of K objects at GCRS positions r[k] with the ITRS->GCRS matrix M
 // (column-major): r_itrs = M^T r, a = M a_itrs (the two cublasDgemvStridedBatched of
 // gravity_source.cu:176-210).
 // LANE: the tables are in the lane layout, two objects (K = 2) and, in mixed mode, L > 8; the
 // walk is then the two-column walk (the other cases have no plain-walk form in that layout).
-template <bool MIXED, int K, bool LANE = false>
+template <bool MIXED, int K, bool LANE = false, bool COMP = false>
 __device__ __forceinline__ void gravity_gcrs(const GravSmem& gs, const double* __restrict__ M,
     const double (&r)[K][3], double (&a)[K][3])
 {
@@ -907,7 +1053,10 @@ __device__ __forceinline__ void gravity_gcrs(const GravSmem& gs, const double* _
         py[k] = m[3] * r[k][0] + m[4] * r[k][1] + m[5] * r[k][2];
         pz[k] = m[6] * r[k][0] + m[7] * r[k][1] + m[8] * r[k][2];
     }
-    if constexpr (LANE) {
+    if constexpr (COMP) {
+        static_assert(MIXED && !LANE, "compensated sums belong to the plain mixed walk");
+        gravity_itrs_comp<K>(gs, px, py, pz, ax, ay, az);
+    } else if constexpr (LANE) {
         static_assert(K == 2, "the lane-layout two-column walk carries two objects");
         if constexpr (MIXED)
             gravity_itrs_groups<true>(gs, px, py, pz, ax, ay, az);
@@ -925,13 +1074,13 @@ __device__ __forceinline__ void gravity_gcrs(const GravSmem& gs, const double* _
 }
 
 // One object (startup, single-evaluation and unit kernels).
-template <bool MIXED>
+template <bool MIXED, bool COMP = false>
 __device__ __forceinline__ void gravity_gcrs1(const GravSmem& gs, const double* __restrict__ M,
     const double* r, double* a)
 {
     double rr[1][3] = { { r[0], r[1], r[2] } };
     double aa[1][3];
-    gravity_gcrs<MIXED, 1>(gs, M, rr, aa);
+    gravity_gcrs<MIXED, 1, false, COMP>(gs, M, rr, aa);
     a[0] = aa[0][0];
     a[1] = aa[0][1];
     a[2] = aa[0][2];

@@ -15,7 +15,8 @@
 namespace gpop {
 
 // ---- force models seen by the integrator (IForceModel, iforce_model.cuh:19-33) ----
-template <bool MIXED> struct ForceGravity {
+// COMP: mixed precision with compensated FP32 sums (GPOP_MIXED_COMPENSATED).
+template <bool MIXED, bool COMP = false> struct ForceGravity {
     static constexpr bool kTable = true;
     static constexpr bool kMixed = MIXED;
     GravSmem g;
@@ -24,19 +25,19 @@ template <bool MIXED> struct ForceGravity {
     // ForceModel::ComputePropagationAcceleration (force_model.cu:91-109): epoch index idx
     __device__ __forceinline__ void prop(const double* r, const double*, int idx, double* a) const
     {
-        gravity_gcrs1<MIXED>(g, prop_m + (size_t)idx * 9, r, a);
+        gravity_gcrs1<MIXED, COMP>(g, prop_m + (size_t)idx * 9, r, a);
     }
     template <int K>
     __device__ __forceinline__ void prop_k(const double (&r)[K][3], const double (&)[K][3], int idx,
         double (&a)[K][3]) const
     {
-        gravity_gcrs<MIXED, K>(g, prop_m + (size_t)idx * 9, r, a);
+        gravity_gcrs<MIXED, K, false, COMP>(g, prop_m + (size_t)idx * 9, r, a);
     }
     // ForceModel::ComputeGenerationAcceleration (force_model.cu:59-89): table (s'+4)*10 + k
     __device__ __forceinline__ void gen(const double* r, const double*, int step, int k, double* a) const
     {
         const int s = step > 0 ? step - 1 : step;
-        gravity_gcrs1<MIXED>(g, gen_m + (size_t)((s + 4) * 10 + k) * 9, r, a);
+        gravity_gcrs1<MIXED, COMP>(g, gen_m + (size_t)((s + 4) * 10 + k) * 9, r, a);
     }
 };
 
@@ -121,7 +122,7 @@ __global__ void __launch_bounds__(256) startup_kernel(F f, TableSrc ts, PropArgs
 {
     extern __shared__ __align__(128) uint8_t smem[];
     if constexpr (F::kTable) {
-        if (!bind_table<std::is_same<F, ForceGravity<true>>::value>(smem, ts, a.err, f.g))
+        if (!bind_table<F::kMixed>(smem, ts, a.err, f.g))
             return;
     }
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -211,7 +212,7 @@ __global__ void __launch_bounds__(K == 1 ? kOneObjectBlock : 256, 1) gj8_kernel(
     constexpr bool kStage = STAGE && stage_corrector<F>();
     double* stage = nullptr;
     if constexpr (F::kTable) {
-        if (!bind_table<std::is_same<F, ForceGravity<true>>::value>(smem, ts, a.err, f.g))
+        if (!bind_table<F::kMixed>(smem, ts, a.err, f.g))
             return;
         stage = reinterpret_cast<double*>(smem + stage_offset(ts)) + threadIdx.x;
     }
@@ -638,7 +639,15 @@ cudaError_t launch_startup(const TableSrc& ts, const PropArgs& a, int num_sms, c
     LaunchShape ls = pick_shape(a.n, 256, num_sms);
     if (a.kind == 0) {
         size_t smem = table_smem_bytes(ts);
-        if (ts.mixed) {
+        if (ts.mixed && (a.flags & kFlagMixedCompensated)) {
+            ForceGravity<true, true> f {};
+            f.gen_m = a.gen_m;
+            f.prop_m = a.prop_m;
+            cudaError_t e = set_smem(startup_kernel<ForceGravity<true, true>>, smem);
+            if (e != cudaSuccess)
+                return e;
+            startup_kernel<<<ls.grid, ls.block, smem, s>>>(f, ts, a);
+        } else if (ts.mixed) {
             ForceGravity<true> f {};
             f.gen_m = a.gen_m;
             f.prop_m = a.prop_m;
@@ -745,8 +754,16 @@ cudaError_t launch_gj8(const TableSrc& ts, const PropArgs& a, int num_sms, cudaS
 {
     if (a.n <= 0 || a.step_end <= a.step_begin)
         return cudaSuccess;
+    const bool comp = a.kind == 0 && ts.mixed && (a.flags & kFlagMixedCompensated);
     if (walk <= 0)
-        walk = default_walk(a.n, num_sms, lane_ts && a.kind == 0, a.kind == 0 && !ts.mixed);
+        walk = default_walk(a.n, num_sms, lane_ts && a.kind == 0 && !comp, a.kind == 0 && !ts.mixed);
+    if (comp) { // compensated sums: the plain walks only
+        ForceGravity<true, true> f {};
+        f.gen_m = a.gen_m;
+        f.prop_m = a.prop_m;
+        return launch_gj8_f(f, ts, a, num_sms, s, block_override,
+            walk == kWalkTwoObjects ? walk : kWalkOneObject);
+    }
     if ((walk == kWalkLanes || walk == kWalkLanesTwo) && a.kind == 0 && lane_ts) {
         const TableSrc& lt = *lane_ts;
         const int K = walk == kWalkLanesTwo ? 2 : 1;

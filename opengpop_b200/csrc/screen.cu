@@ -5,8 +5,9 @@
 // copying up to 54 doubles of node states on every new minimum and racing on a shared "last" array.
 // Here a block owns a 64 x 64 tile of (a, b) object pairs and walks every step of a phase: the
 // positions of its 128 objects are staged into shared memory 16 steps at a time from the
-// trajectory store, each thread keeps the running minimum of the squared distance and its step
-// for a 4 x 4 micro-tile in registers, and writes once at the end. Squared distances are compared
+// trajectory store (asynchronous copies, double-buffered, so the next chunk loads while this one
+// is screened), each thread keeps the running minimum of the squared distance and its step for a
+// 4 x 4 micro-tile in registers, and writes once at the end. Squared distances are compared
 // with the reference's strict "<", so the first step attaining the minimum wins as in the
 // reference (sqrt is monotonic). Node states for the refinement are read back from the trajectory
 // store, so "before" is always the previous step's state (no race).
@@ -22,20 +23,51 @@ namespace gpop {
 constexpr int kTile = 64; // objects per tile side
 constexpr int kSub = 4; // pairs per thread side
 constexpr int kStepChunk = 16; // steps staged per pass
+// shared memory: two chunk buffers of [step][axis][a tile | b tile][64] doubles
+constexpr int kChunkDoubles = kStepChunk * 3 * 2 * kTile;
+constexpr size_t kScreenSmem = 2 * (size_t)kChunkDoubles * sizeof(double);
 
+__device__ __forceinline__ uint32_t smem_addr(const void* p)
+{
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Issues the asynchronous copies of steps [k0, k0 + kc) of the a and b tiles into buf
+// (cp.async, 8 bytes each: rows start on any double, so no 16-byte alignment is assumed).
+// Objects past n read object n - 1 (their pairs are masked).
+__device__ __forceinline__ void stage_chunk(double* buf, const double* __restrict__ traj, int64_t N,
+    int a0, int b0, int k0, int kc)
+{
+    for (int e = threadIdx.x; e < kc * 3 * 2 * kTile; e += blockDim.x) {
+        const int o = e % kTile;
+        const int side = (e / kTile) & 1;
+        const int c = (e / (2 * kTile)) % 3;
+        const int k = e / (6 * kTile);
+        int64_t obj = (side ? b0 : a0) + o;
+        obj = obj < N ? obj : N - 1;
+        const double* src = traj + ((int64_t)(k0 + k) * 3 + c) * N + obj;
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_addr(buf + e)), "l"(src)
+                     : "memory");
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
+// Running minimum of the squared distance per pair: the thread's 4 x 4 pairs are
+// a = a0 + ty*4 + i (contiguous, read as broadcast double2 pairs) and b = b0 + tx + 16 j (strided, so
+// the 16 lanes of a half warp read 16 consecutive doubles: no bank conflicts). The squared distance
+// is never negative (not even -0), and non-negative doubles order like their bit patterns read as
+// unsigned integers, with every NaN above every number, as the floating-point "<" never picks a
+// NaN: so "d2 < best" is an integer compare on the integer pipe, which leaves the FP64 pipe the six
+// operations of the distance.
 __global__ void __launch_bounds__(256) screen_kernel(ScreenArgs a)
 {
-    __shared__ __align__(16) double sa[kStepChunk][3][kTile];
-    __shared__ __align__(16) double sb[kStepChunk][3][kTile];
+    extern __shared__ __align__(16) double sbuf[];
     const int2 tile = a.tiles[blockIdx.x];
     const int a0 = tile.x, b0 = tile.y;
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
     const int64_t N = a.n;
-    // per-thread pairs: a = a0 + ty*4 + i, b = b0 + tx*4 + j
-    double best[kSub][kSub];
+    unsigned long long best[kSub][kSub];
     uint32_t bstep[kSub][kSub];
-    bool valid[kSub][kSub];
-    int64_t pidx[kSub][kSub];
 #pragma unroll
     for (int i = 0; i < kSub; ++i) {
         const int ai = a0 + ty * kSub + i;
@@ -43,40 +75,51 @@ __global__ void __launch_bounds__(256) screen_kernel(ScreenArgs a)
         const int64_t base = ai < N ? a.base[ai] : 0;
 #pragma unroll
         for (int j = 0; j < kSub; ++j) {
-            const int bj = b0 + tx * kSub + j;
-            valid[i][j] = ai < N && bj < N && bj >= bound;
-            pidx[i][j] = base + bj;
-            best[i][j] = DBL_MAX;
+            const int bj = b0 + tx + 16 * j;
+            best[i][j] = (unsigned long long)__double_as_longlong(DBL_MAX);
             bstep[i][j] = 0xFFFFFFFFu;
-            if (valid[i][j] && a.init == 0) {
-                best[i][j] = a.min_d2[pidx[i][j]];
-                bstep[i][j] = a.min_step[pidx[i][j]];
+            if (ai < N && bj < N && bj >= bound && a.init == 0) {
+                best[i][j] = (unsigned long long)__double_as_longlong(a.min_d2[base + bj]);
+                bstep[i][j] = a.min_step[base + bj];
             }
         }
     }
-    for (int k0 = a.step_lo; k0 < a.step_hi; k0 += kStepChunk) {
+    const int nchunks = (a.step_hi - a.step_lo + kStepChunk - 1) / kStepChunk;
+    if (nchunks > 0)
+        stage_chunk(sbuf, a.traj_r, N, a0, b0, a.step_lo, min(kStepChunk, a.step_hi - a.step_lo));
+    for (int ch = 0; ch < nchunks; ++ch) {
+        const int k0 = a.step_lo + ch * kStepChunk;
         const int kc = min(kStepChunk, a.step_hi - k0);
-        __syncthreads();
-        // stage kc steps x 3 axes x 64 objects for the a and b tiles (coalesced rows of 64)
-        for (int e = threadIdx.x; e < kc * 3 * kTile; e += blockDim.x) {
-            const int o = e % kTile;
-            const int c = (e / kTile) % 3;
-            const int k = e / (3 * kTile);
-            const int64_t row = ((int64_t)(k0 + k) * 3 + c) * N;
-            sa[k][c][o] = (a0 + o < N) ? a.traj_r[row + a0 + o] : 0.0;
-            sb[k][c][o] = (b0 + o < N) ? a.traj_r[row + b0 + o] : 0.0;
+        if (ch + 1 < nchunks) { // the next chunk's copies fly while this chunk is screened
+            const int k1 = k0 + kStepChunk;
+            stage_chunk(sbuf + ((ch + 1) & 1) * kChunkDoubles, a.traj_r, N, a0, b0, k1,
+                min(kStepChunk, a.step_hi - k1));
+            asm volatile("cp.async.wait_group 1;" ::: "memory");
+        } else {
+            asm volatile("cp.async.wait_group 0;" ::: "memory");
         }
         __syncthreads();
+        const double* buf = sbuf + (ch & 1) * kChunkDoubles;
         for (int k = 0; k < kc; ++k) {
+            const double* row = buf + k * 3 * 2 * kTile; // [axis][a | b][64]
             double ax[kSub], ay[kSub], az[kSub], bx[kSub], by[kSub], bz[kSub];
 #pragma unroll
-            for (int i = 0; i < kSub; ++i) {
-                ax[i] = sa[k][0][ty * kSub + i];
-                ay[i] = sa[k][1][ty * kSub + i];
-                az[i] = sa[k][2][ty * kSub + i];
-                bx[i] = sb[k][0][tx * kSub + i];
-                by[i] = sb[k][1][tx * kSub + i];
-                bz[i] = sb[k][2][tx * kSub + i];
+            for (int i = 0; i < kSub; i += 2) {
+                const double2 x = *reinterpret_cast<const double2*>(row + 0 * 2 * kTile + ty * kSub + i);
+                const double2 y = *reinterpret_cast<const double2*>(row + 1 * 2 * kTile + ty * kSub + i);
+                const double2 z = *reinterpret_cast<const double2*>(row + 2 * 2 * kTile + ty * kSub + i);
+                ax[i] = x.x;
+                ax[i + 1] = x.y;
+                ay[i] = y.x;
+                ay[i + 1] = y.y;
+                az[i] = z.x;
+                az[i + 1] = z.y;
+            }
+#pragma unroll
+            for (int j = 0; j < kSub; ++j) {
+                bx[j] = row[0 * 2 * kTile + kTile + tx + 16 * j];
+                by[j] = row[1 * 2 * kTile + kTile + tx + 16 * j];
+                bz[j] = row[2 * 2 * kTile + kTile + tx + 16 * j];
             }
             const uint32_t step = (uint32_t)(a.step_offset + k0 + k);
 #pragma unroll
@@ -86,22 +129,32 @@ __global__ void __launch_bounds__(256) screen_kernel(ScreenArgs a)
                     const double dx = ax[i] - bx[j];
                     const double dy = ay[i] - by[j];
                     const double dz = az[i] - bz[j];
-                    const double d2 = dx * dx + dy * dy + dz * dz;
+                    const unsigned long long d2
+                        = (unsigned long long)__double_as_longlong(dx * dx + dy * dy + dz * dz);
                     if (d2 < best[i][j]) {
                         best[i][j] = d2;
                         bstep[i][j] = step;
                     }
                 }
         }
+        __syncthreads(); // the buffer is staged again two chunks on
     }
 #pragma unroll
-    for (int i = 0; i < kSub; ++i)
+    for (int i = 0; i < kSub; ++i) {
+        const int ai = a0 + ty * kSub + i;
+        if (ai >= N)
+            continue;
+        const int bound = a.bound[ai];
+        const int64_t base = a.base[ai];
 #pragma unroll
-        for (int j = 0; j < kSub; ++j)
-            if (valid[i][j]) {
-                a.min_d2[pidx[i][j]] = best[i][j];
-                a.min_step[pidx[i][j]] = bstep[i][j];
+        for (int j = 0; j < kSub; ++j) {
+            const int bj = b0 + tx + 16 * j;
+            if (bj < N && bj >= bound) {
+                a.min_d2[base + bj] = __longlong_as_double((long long)best[i][j]);
+                a.min_step[base + bj] = bstep[i][j];
             }
+        }
+    }
 }
 
 __global__ void __launch_bounds__(128) refine_kernel(RefineArgs a)
@@ -194,7 +247,11 @@ cudaError_t launch_screen(const ScreenArgs& a, int num_tiles, cudaStream_t s)
 {
     if (num_tiles <= 0 || a.step_hi <= a.step_lo)
         return cudaSuccess;
-    screen_kernel<<<num_tiles, 256, 0, s>>>(a);
+    cudaError_t e = cudaFuncSetAttribute(screen_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        (int)kScreenSmem);
+    if (e != cudaSuccess)
+        return e;
+    screen_kernel<<<num_tiles, 256, kScreenSmem, s>>>(a);
     return cudaGetLastError();
 }
 
