@@ -215,7 +215,12 @@ def w_jac(L):
     return 44 * terms(L) + 100 * (L + 1) + 200
 
 
-def _peaks(torch, dev):
+def _peaks(torch, dev, clocks):
+    """FP64 and FP32 peaks (TFLOP/s) at the SM clock sampled during the timed region (the FMA
+    probe's figures when no clock was sampled)."""
+    p64, p32 = clock_peaks(clocks.get("sm_mhz"), dev)
+    if p64:
+        return p64, p32
     return probe_peak(torch, True, dev), probe_peak(torch, False, dev)
 
 
@@ -270,7 +275,7 @@ def run_batch(args, torch, G, dev):
         dist.destroy_process_group()
     if rank != 0:
         return 0
-    peak64, peak32 = _peaks(torch, dev)
+    peak64, peak32 = _peaks(torch, dev, clocks)
     achieved = f_total / t / 1e12
     t_min = (f_total - f32) / (peak64 * 1e12) + f32 / (peak32 * 1e12) if peak64 and peak32 else None
     io = sum(q["r"].shape[0] for q in all_reqs) * 6 * 8
@@ -354,7 +359,7 @@ def run_screen(args, torch, G, dev):
         return 0
     args.gpus = world
     pair_steps = pairs * steps
-    peak64 = probe_peak(torch, True, dev)
+    peak64 = _peaks(torch, dev, clocks)[0]
     achieved = 9.0 * pair_steps / t_screen / 1e12
     _common(args, "conjunction pair-steps/s of the screen (FP64)", pair_steps / t_screen,
             "pair-steps/s", "f64",
@@ -416,7 +421,7 @@ def run_adjoint(args, torch, G, dev):
     units = 2 * n_pairs
     f_miss = units * steps * (2 * flops_per_object_step() + w_jac(DEGREE)) + units * 145 * w_jac(DEGREE)
     f_stm = n_stm * steps * (flops_per_object_step() + w_jac(DEGREE) + 6 * 500) + n_stm * 145 * w_jac(DEGREE)
-    peak64 = probe_peak(torch, True, dev)
+    peak64 = _peaks(torch, dev, clocks)[0]
     ach = f_miss / tm / 1e12
     _common(args, "miss-distance gradients/s (adjoint, FP64)", n_pairs / tm, "pairs/s", "f64",
             {"workload": "%d LEO pairs (seed %d), 70x70, 30 s, %d steps (24 h), checkpoint every 64 "
@@ -451,6 +456,131 @@ def accuracy_7d(G, n_sample):
             "bound_m": 1.0}
 
 
+def screen_problem(n=20000, seed=SEED):
+    """The closest-approach configuration: n LEO objects, n/10 seed-chosen objects first as
+    singleton sets, the rest one set (each chosen object against all others)."""
+    from opengpop_b200 import orbits
+    n_sel = n // 10
+    r, v = orbits.leo(n, seed)
+    sel = np.random.default_rng(seed).choice(n, n_sel, replace=False)
+    order = np.concatenate([sel, np.setdiff1d(np.arange(n), sel)])
+    set_ids = np.concatenate([np.arange(n_sel), np.full(n - n_sel, n_sel)]).astype(np.uint32)
+    return r[order], v[order], set_ids
+
+
+def screen_cpu_baseline(torch, G, r, v, rows=40, window=240, seconds_target=10.0):
+    """Oracle screen (CPU FP64 restatement of UpdateClosestApproachKernel, OpenMP over pairs) on a
+    row sample of the closest-approach configuration: `rows` set objects against all others over
+    the first steps of the GPU trajectory. Returns pair-steps/s, cores and a description."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_api as O
+    n = r.shape[0]
+    ctx = G.Context(precision=G.FP64)
+    rd = torch.tensor(r, dtype=torch.float64, device="cuda")
+    vd = torch.tensor(v, dtype=torch.float64, device="cuda")
+    prop = ctx.propagator(START, H, window, rd, vd)
+    tr = torch.empty((window, 3, n), dtype=torch.float64, device="cuda")
+    tv, ta = torch.empty_like(tr), torch.empty_like(tr)
+    prop.step(window, tr, tv, ta)
+    torch.cuda.synchronize()
+    arrs = [np.ascontiguousarray(x.cpu().numpy().transpose(0, 2, 1)) for x in (tr, tv, ta)]
+    prop.close()
+    ctx.close()
+    ids = np.concatenate([np.arange(rows), np.full(n - rows, rows)]).astype(np.uint32)
+    part = O.partition(ids)
+    P = int(part["num_pairs"])
+    cores = cpu_cores()
+
+    def run(steps):
+        md = np.zeros(P)
+        cs = np.zeros(P, np.uint32)
+        nodes = np.zeros(P * 54)
+        last = np.zeros(n * 9)
+        st = O.OrCaState(md.ctypes.data, cs.ctypes.data, nodes.ctypes.data, last.ctypes.data)
+        t0 = time.perf_counter()
+        O.lib().or_ca_screen(n, steps, O.ptr(arrs[0]), O.ptr(arrs[1]), O.ptr(arrs[2]), O.ptr(ids),
+                             0, 1, C.byref(st), cores)
+        return time.perf_counter() - t0
+
+    t4 = run(4)
+    steps = int(min(window, max(4, seconds_target * 4 / max(t4, 1e-6))))
+    dt = run(steps)
+    return P * steps / dt, cores, ("%d set objects against the other %d objects (%d pairs) x %d "
+                                   "steps of the GPU trajectory, %.1f s of CPU work"
+                                   % (rows, n - rows, P, steps, dt))
+
+
+def screen_leg(torch, G, dev, steps, warmup=1, cpu=True):
+    """One closest-approach job of the configuration (20,000 LEO objects, 2,000 against all,
+    `steps` 30 s steps, 5 km) through the public calls: host buffers in, records out."""
+    r, v, set_ids = screen_problem()
+    n = r.shape[0]
+    res = None
+    ctx = G.Context(device=dev.index, precision=G.FP64)
+    launches0 = 0
+    for i in range(warmup + 1):
+        if i == warmup:
+            launches0 = ctx.kernel_launches
+        t0 = time.perf_counter()
+        ca = ctx.closest_approach(START, H, r, v, set_ids)
+        ca.propagate(steps)
+        recs = ca.find(5000.0)
+        wall = time.perf_counter() - t0
+        secs = ca.device_seconds()
+        pairs = ca.num_pairs
+        ca.close()
+        res = (wall, secs, len(recs))
+    launches = ctx.kernel_launches - launches0
+    ctx.close()
+    wall, secs, found = res
+    pair_steps = pairs * steps
+    out = {"value": pair_steps / secs[1], "unit": "pair-steps/s",
+           "what": "screen kernel: pairs x steps / device time of the screen (CUDA events)",
+           "workload": "%d LEO objects (seed %d), %d against all = %d pairs, 70x70, 30 s, %d steps, "
+                       "threshold 5 km, FP64" % (n, SEED, n // 10, pairs, steps),
+           "pairs_per_s_whole_job": pairs / wall, "job_seconds": wall,
+           "device_seconds": {"propagation": float(secs[0]), "screen": float(secs[1]),
+                              "refinement": float(secs[2])},
+           "found_below_threshold": found, "gpu_launches": launches,
+           "e2e": {"value": pair_steps / wall, "unit": "pair-steps/s",
+                   "h2d_bytes_per_step": n * 6 * 8 + n * 4, "d2h_bytes_per_step": found * 64,
+                   "call": "gpop_ca_create + gpop_ca_propagate + gpop_ca_find (host buffers)"}}
+    if cpu:
+        rate, cores, desc = screen_cpu_baseline(torch, G, r, v)
+        out["cpu_baseline"] = {"value": rate, "unit": "pair-steps/s", "cores": cores, "kind": "port",
+                               "sample": desc}
+    return out
+
+
+def reference_cuda_rate(n=16384, s1=8, s2=40):
+    """The reference's own CUDA build (compiled from its sources into oracle/_ref/libref.so), timed
+    on this GPU in child processes: object-steps/s of its step loop from two durations (startup
+    cancels), FP64 at 70x70 on n objects of the mixed population. None when that build is absent."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import ref_build_runner as RB
+    from opengpop_b200 import orbits
+    if not RB.available():
+        return None
+    r0, v0 = orbits.mixed_population(n, SEED)
+    RB.run("propagate", START, H, 2, r0[:256], v0[:256])  # loads its kernels
+    t = [min(float(RB.run("propagate", START, H, s, r0, v0)["ms"]) * 1e-3 for _ in range(2))
+         for s in (s1, s2)]
+    rate = n * (s2 - s1) / max(t[1] - t[0], 1e-9)
+    return {"value": rate, "unit": "object-steps/s", "kind": "reference CUDA build",
+            "sample": "%d objects of the mixed population, 70x70, 30 s, FP64; step loop of %d and %d "
+                      "steps (CUDA events), rate from the difference" % (n, s1, s2)}
+
+
+def clock_peaks(sm_mhz, dev):
+    """FP64 and FP32 FMA peaks (TFLOP/s) from the SM count and the SM clock sampled under load:
+    64 FP64 and 128 FP32 FMAs per SM per cycle."""
+    import torch
+    if not sm_mhz:
+        return None, None
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    return sms * 64 * 2 * sm_mhz * 1e6 / 1e12, sms * 128 * 2 * sm_mhz * 1e6 / 1e12
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -476,6 +606,10 @@ def main():
     ap.add_argument("--stm-objects", type=int, default=8192)
     ap.add_argument("--accuracy-objects", type=int, default=8192,
                     help="objects of the 7-day mixed-vs-FP64 error sample (0 = skip)")
+    ap.add_argument("--no-screen", action="store_true",
+                    help="headline: skip the closest-approach job (conj pairs/s)")
+    ap.add_argument("--no-reference-cuda", action="store_true",
+                    help="headline: skip timing the reference's own CUDA build")
     args = ap.parse_args()
     short = args.workload != "propagate"  # whole-job workloads of several seconds per step
     if args.steps is None:
@@ -594,8 +728,13 @@ def main():
     ctx.close()
 
     # ---- roofline of the dominant kernel (the mixed GJ8 kernel) ----
-    peak64 = probe_peak(torch, True, dev)
-    peak32 = probe_peak(torch, False, dev)
+    # denominators: the FMA rates per SM and cycle at the SM clock sampled during the timed runs
+    # (the probe's live FMA-chain figures are reported beside them)
+    probe64 = probe_peak(torch, True, dev)
+    probe32 = probe_peak(torch, False, dev)
+    peak64, peak32 = clock_peaks(clocks.get("sm_mhz"), dev)
+    if not peak64:
+        peak64, peak32 = probe64, probe32
     launch_t = sum(times_mixed) / max(1, launches_mixed)
     steps_per_launch = args.prop_steps * args.steps / max(1, launches_mixed)
     f_total = flops_per_object_step() * n * steps_per_launch
@@ -608,6 +747,20 @@ def main():
     fp64_achieved = flops_per_object_step() * n * steps_per_launch / fp64_launch_t / 1e12
 
     accuracy = accuracy_7d(G, args.accuracy_objects) if args.accuracy_objects > 0 and rank == 0 else None
+    # the metric's second half (conj pairs/s) and the reference's CUDA build: one GPU only
+    screen = None
+    if world == 1 and not args.no_screen:
+        screen = screen_leg(torch, G, dev, args.screen_steps, cpu=not args.no_cpu_baseline)
+        screen["roofline"] = {"bound": "fp64", "achieved": 9.0 * screen["value"] / 1e12,
+                              "peak": peak64, "unit": "TFLOP/s",
+                              "frac": 9.0 * screen["value"] / 1e12 / peak64 if peak64 else None,
+                              "traffic": None, "per_unit": "9 FP64 flops per pair-step"}
+    ref_cuda = None
+    if world == 1 and not args.no_reference_cuda:
+        try:
+            ref_cuda = reference_cuda_rate()
+        except Exception as e:  # the reference build exits on its own errors; report, do not fail
+            ref_cuda = {"unavailable": str(e)[:200]}
 
     if rank == 0:
         cpu = None
@@ -631,7 +784,8 @@ def main():
                      "ms_per_step": 1e3 * t_fp64 / args.steps,
                      "roofline": {"bound": "fp64", "achieved": fp64_achieved, "peak": peak64,
                                   "unit": "TFLOP/s",
-                                  "frac": fp64_achieved / peak64 if peak64 else None}},
+                                  "frac": fp64_achieved / peak64 if peak64 else None,
+                                  "frac_vs_probe": fp64_achieved / probe64 if probe64 else None}},
             "mixed_vs_fp64": value / value_fp64,
             "accuracy_7d": accuracy,
             "e2e": {"value": e2e_value, "unit": "object-steps/s",
@@ -640,13 +794,23 @@ def main():
             "roofline": {"bound": "fp64+fp32", "achieved": achieved, "peak": eff_peak,
                          "unit": "TFLOP/s", "frac": achieved / eff_peak if eff_peak else None,
                          "traffic": MIXED_GJ8_DRAM_BYTES,
-                         "traffic_note": "dram read+write bytes of one launch of this kernel "
-                                         "(ncu, 65,536 objects, 4-step launch: the state is read "
-                                         "once per launch, later steps hit L2); algorithmic "
-                                         "state bytes per launch %d" % (600 * n),
-                         "peaks_measured": {"fp64_tflops": peak64, "fp32_tflops": peak32,
-                                            "how": "live FMA-chain probe (libgpop_probe.so)"}},
+                         "traffic_note": "a stated constant, not measured in this run: dram "
+                                         "read+write bytes of one launch of this kernel from an "
+                                         "ncu capture (65,536 objects, 4-step launch; the state "
+                                         "is read once per launch, later steps hit L2); "
+                                         "algorithmic state bytes per launch %d" % (600 * n),
+                         "peak_note": "not in MEASURED_PEAKS.json (HBM and bf16 only): SMs x "
+                                      "(64 FP64 | 128 FP32 FMAs per cycle) x 2 x the median SM "
+                                      "clock sampled during the timed runs",
+                         "frac_vs_probe": (achieved / (f_total / (f64 / (probe64 * 1e12)
+                                                                  + f32 / (probe32 * 1e12)) / 1e12)
+                                           if probe64 and probe32 else None),
+                         "peaks_measured": {"fp64_tflops": probe64, "fp32_tflops": probe32,
+                                            "how": "live FMA-chain probe (libgpop_probe.so)"},
+                         "peaks_clock": {"fp64_tflops": peak64, "fp32_tflops": peak32}},
             "cpu_baseline": cpu,
+            "screen": screen,
+            "reference_cuda": ref_cuda,
             "clocks": clocks,
             "gpu_launches": launches_mixed,
             "checksum": [chk_m, chk_d],
