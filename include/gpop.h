@@ -172,15 +172,20 @@ gpop_status gpop_propagate_batch(gpop_ctx* ctx, const gpop_request* reqs, int32_
  * its status for every request that was to run. */
 gpop_status gpop_propagate_batch_status(gpop_ctx* ctx, const gpop_request* reqs, int32_t n_req,
     int32_t* status);
-/* The batch plan: lanes per object chosen for each request and the estimated makespan (s). */
+/* The batch plan: lanes per object chosen for each request and the estimated makespan (s). The
+ * planner also picks the block shape of the persistent grid (4 or 8 warps per SM), the one with the
+ * shorter simulated makespan; gpop_batch_warps_per_sm gives the last planned batch's. */
 gpop_status gpop_batch_plan(gpop_ctx* ctx, const gpop_request* reqs, int32_t n_req,
     int32_t* lanes_per_object, double* est_seconds);
+/* No counterpart in the reference. Warps per SM (the block shape) of the last planned batch. */
+int32_t gpop_batch_warps_per_sm(const gpop_ctx* ctx);
 /* Device time (s, CUDA events) of the last gpop_propagate_batch launch: frames, startup and the
  * persistent GJ8 kernel, without the host copies. */
 double gpop_batch_device_seconds(const gpop_ctx* ctx);
-/* Autotuner: measures the throughput of the batched GJ8 kernel for each gravity degree in
- * {8, 20, 36, 70} (up to the context's) and 1..32 lanes per object, which the batch planner then
- * uses. cache_path (may be NULL) is read if it exists and written otherwise. */
+/* Autotuner: measures the throughput of the batched GJ8 kernel for each block shape (4 and 8 warps
+ * per SM), gravity degree in {8, 20, 36, 70} (up to the context's) and 1..32 lanes per object (the
+ * item tile: 32/P objects, 64 with one lane), which the batch planner then uses. cache_path (may
+ * be NULL) is read if it exists and written otherwise. */
 gpop_status gpop_tune(gpop_ctx* ctx, const char* cache_path);
 
 /* ---- variational equations and adjoint (FP64; the reference has no counterpart) ----

@@ -31,7 +31,7 @@ EXPORTS = (
     "gpop_gravity_degree", "gpop_kernel_launches", "gpop_propagate", "gpop_propagate_device",
     "gpop_propagate_device_noalloc", "gpop_propagate_trajectory", "gpop_propagator_create", "gpop_propagator_step",
     "gpop_propagator_steps_done", "gpop_propagator_destroy", "gpop_propagate_analytic",
-    "gpop_propagate_batch", "gpop_propagate_batch_status", "gpop_batch_plan", "gpop_tune", "gpop_batch_device_seconds", "gpop_gravity_jacobian", "gpop_stm", "gpop_propagate_vjp",
+    "gpop_propagate_batch", "gpop_propagate_batch_status", "gpop_batch_plan", "gpop_batch_warps_per_sm", "gpop_tune", "gpop_batch_device_seconds", "gpop_gravity_jacobian", "gpop_stm", "gpop_propagate_vjp",
     "gpop_miss_gradient", "gpop_sample_states", "gpop_startup", "gpop_corrector_unit",
     "gpop_predict_unit", "gpop_finalize_correction_unit", "gpop_rk8_stage", "gpop_rk8_finish",
     "gpop_startup_init", "gpop_startup_correct", "gpop_gj8_predict", "gpop_gj8_correct",
@@ -107,6 +107,7 @@ def load_library(path=LIB_PATH):
         "gpop_propagate_batch_status": (i32, [_VP, _VP, i32, _VP]),
         "gpop_batch_plan": (i32, [_VP, _VP, i32, _VP, C.POINTER(f64)]),
         "gpop_tune": (i32, [_VP, C.c_char_p]),
+        "gpop_batch_warps_per_sm": (i32, [_VP]),
         "gpop_batch_device_seconds": (f64, [_VP]),
         "gpop_gravity_jacobian": (i32, [_VP, i64, _VP, _VP, _VP, _VP, _VP]),
         "gpop_sample_states": (i32, [_VP, _VP, _VP, f64, f64, C.c_uint64, i64, _VP, _VP, _VP]),
@@ -335,6 +336,11 @@ class Context:
         msg = None if st == OK else load_library().gpop_last_error(self._h).decode()
         out = [(k[2], k[3]) if status[i] == OK else None for i, k in enumerate(keep)]
         return out, status, st, msg
+
+    @property
+    def batch_warps_per_sm(self):
+        """Block shape (warps per SM) the planner chose for the last batch."""
+        return load_library().gpop_batch_warps_per_sm(self._h)
 
     def batch_plan(self, reqs):
         arr, keep = self._requests(reqs)

@@ -17,17 +17,22 @@ using namespace gpop;
 
 namespace {
 
-constexpr int kWarpsPerSm = 8; // persistent grid: one 256-thread block per SM
+// Persistent grid: one block per SM of 4 or 8 warps (the block shapes the planner chooses from);
+// the two-object path needs the registers of 8 warps at most.
+constexpr int kWarpOptions[2] = { 4, 8 };
+inline int warp_index(int W) { return W == kWarpOptions[0] ? 0 : 1; }
 constexpr int kDegrees[4] = { 8, 20, 36, 70 };
 const double kNodesH[10] = { 0.0, 4.0 / 27.0, 2.0 / 9.0, 1.0 / 3.0, 1.0 / 2.0, 2.0 / 3.0, 1.0 / 6.0, 1.0, 5.0 / 6.0, 1.0 };
 
 int terms(int L) { return (L + 1) * (L + 2) / 2 - 3; }
 
-// Object-steps per second per SM of the batched kernel at degree L with P lanes per object.
-// Measured by gpop_tune; before tuning a model is used: cost proportional to the terms walked,
-// with a per-lane overhead for the column split and the shuffles.
-double eta(const gpop_ctx* ctx, int L, int P)
+// Object-steps per second per SM of the batched kernel at degree L with P lanes per object, with
+// W warps per SM. Measured by gpop_tune; before tuning a model is used: cost proportional to the
+// terms walked, with a per-lane overhead for the column split and the shuffles, and three
+// quarters of the throughput with four warps (one per scheduler) as with eight.
+double eta(const gpop_ctx* ctx, int W, int L, int P)
 {
+    const int wi = warp_index(W);
     int lp = 0;
     while ((1 << lp) < P)
         ++lp;
@@ -38,14 +43,14 @@ double eta(const gpop_ctx* ctx, int L, int P)
             ++i;
         const int j = std::min(i + 1, 3);
         const double t0 = terms(kDegrees[i]), t1 = terms(kDegrees[j]), t = terms(std::max(L, 2));
-        const double c0 = 1.0 / ctx->eta[i][lp], c1 = 1.0 / ctx->eta[j][lp];
+        const double c0 = 1.0 / ctx->eta[wi][i][lp], c1 = 1.0 / ctx->eta[wi][j][lp];
         const double f = (t1 > t0) ? std::min(1.0, std::max(0.0, (t - t0) / (t1 - t0))) : 0.0;
         return 1.0 / (c0 + f * (c1 - c0));
     }
     const bool mixed = ctx->cfg.precision == GPOP_MIXED;
     const double base70 = mixed ? 6.5e5 : 4.5e5; // object-steps/s per SM at 70x70, one lane
     const double cost = (terms(std::max(L, 2)) + 60.0) / (terms(70) + 60.0);
-    return base70 / cost / (1.0 + 0.12 * lp);
+    return base70 / cost / (1.0 + 0.12 * lp) * (wi == 0 ? 0.75 : 1.0);
 }
 
 // Speed of single-lane items in a batch of single-lane items (two-column walk on the plain table)
@@ -157,29 +162,43 @@ struct Plan {
     std::vector<int> lpo;
     std::vector<BatchItem> items;
     double est = 0.0;
+    int warps_per_sm = 8; // block shape of the persistent grid
 };
 
+// The plan: for each block shape (warps per SM), lanes per object and the simulated makespan with
+// that shape's rates; the shape with the shorter makespan wins (four warps give a batch with at
+// most one item per scheduler a whole scheduler per item).
 Plan make_plan(const gpop_ctx* ctx, const std::vector<int64_t>& n, const std::vector<int>& steps,
     const std::vector<int>& L)
 {
     const size_t R = n.size();
     Plan p;
-    p.lpo.assign(R, 1);
-    const double warps = (double)ctx->num_sms * kWarpsPerSm;
-    auto item_time = [&](size_t r, int P) { // seconds for one warp to run its group through all steps
-        return (double)steps[r] * kWarpsPerSm * batch_item_objects(P) / eta(ctx, L[r], P);
-    };
-    const bool fixed = ctx->force_lpo > 0; // autotuner: fixed lanes per object
-    if (fixed)
-        p.lpo.assign(R, ctx->force_lpo);
-    p.est = choose_lanes(n, steps, warps, item_time, p.lpo, fixed,
-        ctx->cfg.precision == GPOP_MIXED ? kPairWalkGainMixed : kPairWalkGainFp64);
+    p.est = -1.0;
+    for (int W : kWarpOptions) {
+        if (ctx->force_warps > 0 && W != ctx->force_warps)
+            continue;
+        std::vector<int> lpo(R, 1);
+        const double warps = (double)ctx->num_sms * W;
+        auto item_time = [&](size_t r, int P) { // seconds for one warp to run its group through all steps
+            return (double)steps[r] * W * batch_item_objects(P) / eta(ctx, W, L[r], P);
+        };
+        const bool fixed = ctx->force_lpo > 0; // autotuner: fixed lanes per object
+        if (fixed)
+            lpo.assign(R, ctx->force_lpo);
+        const double est = choose_lanes(n, steps, warps, item_time, lpo, fixed,
+            ctx->cfg.precision == GPOP_MIXED ? kPairWalkGainMixed : kPairWalkGainFp64);
+        if (p.est < 0.0 || est < p.est) {
+            p.est = est;
+            p.lpo = lpo;
+            p.warps_per_sm = W;
+        }
+    }
     std::vector<std::pair<double, BatchItem>> items;
     for (size_t r = 0; r < R; ++r) {
         if (steps[r] <= 0)
             continue;
         const int per = batch_item_objects(p.lpo[r]);
-        const double t = item_time(r, p.lpo[r]);
+        const double t = (double)steps[r] * p.warps_per_sm * per / eta(ctx, p.warps_per_sm, L[r], p.lpo[r]);
         for (int64_t f = 0; f < n[r]; f += per) {
             items.push_back({ t, BatchItem { (int)r, (int)f, (int)std::min<int64_t>(per, n[r] - f) } });
         }
@@ -333,6 +352,7 @@ static gpop_status run_batch(gpop_ctx* ctx, const gpop_request* reqs, int32_t n_
     if (N == 0)
         return GPOP_OK;
     Plan plan = make_plan(ctx, n, steps, L);
+    ctx->batch_warps = plan.warps_per_sm;
     // epoch table offsets (in matrices): [gen 80 | prop len] per table
     std::vector<int64_t> t_off(tables.size());
     int64_t E = 0;
@@ -350,7 +370,7 @@ static gpop_status run_batch(gpop_ctx* ctx, const gpop_request* reqs, int32_t n_
         pair_walk = pair_walk && plan.lpo[i] == 1;
     // shape signature: the graph is replayed only for an identical plan and layout
     std::vector<int64_t> sig { (int64_t)ctx->cfg.precision, (int64_t)ctx->cfg.flags, N, E, (int64_t)n_req,
-        (int64_t)pair_walk };
+        (int64_t)pair_walk, (int64_t)plan.warps_per_sm };
     for (int i = 0; i < n_req; ++i) {
         sig.push_back(n[i]);
         sig.push_back(steps[i]);
@@ -499,7 +519,8 @@ static gpop_status run_batch(gpop_ctx* ctx, const gpop_request* reqs, int32_t n_
         if (le == cudaSuccess)
             le = cudaMemsetAsync(bc->queue.p, 0, sizeof(int), s);
         if (le == cudaSuccess)
-            le = launch_batch_gj8(ctx->lane_table(mixed), ctx->table(mixed), a, ctx->num_sms, 32 * kWarpsPerSm, s);
+            le = launch_batch_gj8(ctx->lane_table(mixed), ctx->table(mixed), a, ctx->num_sms,
+                32 * plan.warps_per_sm, s);
         e = cudaStreamEndCapture(s, &graph);
         if (le != cudaSuccess || e != cudaSuccess) {
             if (graph)
@@ -589,37 +610,41 @@ gpop_status gpop_propagate_batch(gpop_ctx* ctx, const gpop_request* reqs, int32_
 
 double gpop_batch_device_seconds(const gpop_ctx* ctx) { return ctx ? ctx->batch_seconds : -1.0; }
 
+int32_t gpop_batch_warps_per_sm(const gpop_ctx* ctx) { return ctx ? ctx->batch_warps : -1; }
+
 gpop_status gpop_tune(gpop_ctx* ctx, const char* cache_path)
 {
     if (!ctx)
         return GPOP_ERR_INVALID_ARG;
     const bool mixed = ctx->cfg.precision == GPOP_MIXED;
-    if (cache_path) { // "<precision> <L> <P> <eta>" lines
+    if (cache_path) { // "<precision> <warps per SM> <L> <P> <eta>" lines
         std::ifstream f(cache_path);
         if (f.is_open()) {
-            int prec, Lc, P;
+            int prec, W, Lc, P;
             double val;
             int found = 0;
-            while (f >> prec >> Lc >> P >> val)
-                for (int i = 0; i < 4; ++i)
-                    for (int lp = 0; lp < 6; ++lp)
-                        if (prec == (int)mixed && Lc == kDegrees[i] && P == (1 << lp) && val > 0) {
-                            ctx->eta[i][lp] = val;
-                            ++found;
-                        }
-            if (found == 24) {
+            while (f >> prec >> W >> Lc >> P >> val)
+                for (int wi = 0; wi < 2; ++wi)
+                    for (int i = 0; i < 4; ++i)
+                        for (int lp = 0; lp < 6; ++lp)
+                            if (prec == (int)mixed && W == kWarpOptions[wi] && Lc == kDegrees[i]
+                                && P == (1 << lp) && val > 0) {
+                                ctx->eta[wi][i][lp] = val;
+                                ++found;
+                            }
+            if (found == 48) {
                 ctx->tuned = true;
                 return GPOP_OK;
             }
         }
     }
-    // Calibration: one request per (degree, lanes) that fills every warp of the persistent grid,
-    // on near-circular orbits. The captured graph is replayed at two durations (fastest of three
-    // replays each); the difference (32 GJ8 steps) removes the frames, startup and launch
-    // overheads.
+    // Calibration: for each block shape (warps per SM), one request per (degree, lanes) that fills
+    // every warp of the persistent grid, on near-circular orbits. The captured graph is replayed
+    // at two durations (fastest of three replays each); the difference (32 GJ8 steps) removes the
+    // frames, startup and launch overheads.
     const gpop_time t0 { 2024, 1, 1, 0, 0, 0.0 };
     const bool saved = ctx->tuned;
-    double measured[4][6];
+    double measured[2][4][6];
     auto replay_ms = [&](gpop_request& q, int steps, float& ms) -> gpop_status {
         q.steps = steps;
         ctx->tuned = false;
@@ -649,47 +674,56 @@ gpop_status gpop_tune(gpop_ctx* ctx, const char* cache_path)
             return cuda_fail(ctx, e, "timing the batch graph");
         return check_device_errors(ctx, ctx->batch_stream);
     };
-    for (int i = 0; i < 4; ++i) {
-        const int Lc = std::min(kDegrees[i], ctx->md.degree);
-        for (int lp = 0; lp < 6; ++lp) {
-            const int P = 1 << lp;
-            const int64_t nobj = (int64_t)ctx->num_sms * kWarpsPerSm * batch_item_objects(P);
-            std::vector<double> r(3 * nobj), v(3 * nobj), ro(3 * nobj), vo(3 * nobj);
-            for (int64_t o = 0; o < nobj; ++o) {
-                const double ang = 0.001 * (double)o, a = 7.0e6 + 10.0 * (double)(o % 97);
-                const double sp = std::sqrt(ctx->md.gm / a), inc = 0.3 + 1e-4 * (double)(o % 31);
-                r[3 * o] = a * std::cos(ang);
-                r[3 * o + 1] = a * std::sin(ang) * std::cos(inc);
-                r[3 * o + 2] = a * std::sin(ang) * std::sin(inc);
-                v[3 * o] = -sp * std::sin(ang);
-                v[3 * o + 1] = sp * std::cos(ang) * std::cos(inc);
-                v[3 * o + 2] = sp * std::cos(ang) * std::sin(inc);
+    for (int wi = 0; wi < 2; ++wi) {
+        const int W = kWarpOptions[wi];
+        for (int i = 0; i < 4; ++i) {
+            const int Lc = std::min(kDegrees[i], ctx->md.degree);
+            for (int lp = 0; lp < 6; ++lp) {
+                const int P = 1 << lp;
+                const int64_t nobj = (int64_t)ctx->num_sms * W * batch_item_objects(P);
+                std::vector<double> r(3 * nobj), v(3 * nobj), ro(3 * nobj), vo(3 * nobj);
+                for (int64_t o = 0; o < nobj; ++o) {
+                    const double ang = 0.001 * (double)o, a = 7.0e6 + 10.0 * (double)(o % 97);
+                    const double sp = std::sqrt(ctx->md.gm / a), inc = 0.3 + 1e-4 * (double)(o % 31);
+                    r[3 * o] = a * std::cos(ang);
+                    r[3 * o + 1] = a * std::sin(ang) * std::cos(inc);
+                    r[3 * o + 2] = a * std::sin(ang) * std::sin(inc);
+                    v[3 * o] = -sp * std::sin(ang);
+                    v[3 * o + 1] = sp * std::cos(ang) * std::cos(inc);
+                    v[3 * o + 2] = sp * std::cos(ang) * std::sin(inc);
+                }
+                gpop_request q { t0, 30.0, 0, Lc, nobj, r.data(), v.data(), ro.data(), vo.data() };
+                // pin the lanes and the block shape: the planner keeps them for a request that
+                // fills the grid exactly
+                float ms_short = 0.f, ms_long = 0.f;
+                ctx->force_lpo = P;
+                ctx->force_warps = W;
+                gpop_status st = replay_ms(q, 8, ms_short);
+                if (st == GPOP_OK)
+                    st = replay_ms(q, 40, ms_long);
+                ctx->force_lpo = 0;
+                ctx->force_warps = 0;
+                if (st != GPOP_OK) {
+                    ctx->tuned = saved;
+                    return st;
+                }
+                const double dt = std::max(1e-6, (double)(ms_long - ms_short) * 1e-3);
+                measured[wi][i][lp] = (double)nobj * 32.0 / dt / ctx->num_sms;
             }
-            gpop_request q { t0, 30.0, 0, Lc, nobj, r.data(), v.data(), ro.data(), vo.data() };
-            // pin the lanes: the planner keeps P for a request that fills the grid exactly
-            float ms_short = 0.f, ms_long = 0.f;
-            ctx->force_lpo = P;
-            gpop_status st = replay_ms(q, 8, ms_short);
-            if (st == GPOP_OK)
-                st = replay_ms(q, 40, ms_long);
-            ctx->force_lpo = 0;
-            if (st != GPOP_OK) {
-                ctx->tuned = saved;
-                return st;
-            }
-            const double dt = std::max(1e-6, (double)(ms_long - ms_short) * 1e-3);
-            measured[i][lp] = (double)nobj * 32.0 / dt / ctx->num_sms;
         }
     }
-    for (int i = 0; i < 4; ++i)
-        for (int lp = 0; lp < 6; ++lp)
-            ctx->eta[i][lp] = measured[i][lp];
+    for (int wi = 0; wi < 2; ++wi)
+        for (int i = 0; i < 4; ++i)
+            for (int lp = 0; lp < 6; ++lp)
+                ctx->eta[wi][i][lp] = measured[wi][i][lp];
     ctx->tuned = true;
     if (cache_path) {
         std::ofstream f(cache_path);
-        for (int i = 0; i < 4; ++i)
-            for (int lp = 0; lp < 6; ++lp)
-                f << (int)mixed << " " << kDegrees[i] << " " << (1 << lp) << " " << ctx->eta[i][lp] << "\n";
+        for (int wi = 0; wi < 2; ++wi)
+            for (int i = 0; i < 4; ++i)
+                for (int lp = 0; lp < 6; ++lp)
+                    f << (int)mixed << " " << kWarpOptions[wi] << " " << kDegrees[i] << " " << (1 << lp)
+                      << " " << ctx->eta[wi][i][lp] << "\n";
     }
     return GPOP_OK;
 }

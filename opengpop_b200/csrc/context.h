@@ -97,10 +97,13 @@ struct gpop_ctx {
     cudaStream_t batch_stream = nullptr;
     void* batch_host = nullptr;
     size_t batch_host_cap = 0;
-    // batched-kernel throughput (object-steps/s per SM) for degrees {8, 20, 36, 70} x lanes 1..32
+    // batched-kernel throughput (object-steps/s per SM) for the persistent grid's block shapes
+    // (4 or 8 warps per SM) x degrees {8, 20, 36, 70} x lanes 1..32
     bool tuned = false;
-    double eta[4][6] = {};
+    double eta[2][4][6] = {};
     int force_lpo = 0; // lanes per object fixed by the autotuner while it measures (0 = planner)
+    int force_warps = 0; // warps per SM fixed by the autotuner while it measures (0 = planner)
+    int batch_warps = 8; // warps per SM of the last planned batch
     double batch_seconds = 0; // device time of the last batch launch (CUDA events around the graph)
 
     gpop::TableSrc lane_table(bool mixed_mode) const

@@ -154,3 +154,18 @@ def test_tune_cache_roundtrip(contexts, tmp_path):
     ctx.tune(path)  # read back from the cache
     reqs = _requests(SPEC[:4], 8)
     _compare(ctx.propagate_batch(reqs), reqs, lambda q: contexts(q["degree"]), 1e-3, 1e-6)
+
+
+def test_planner_block_shape(contexts):
+    """The planner picks the persistent grid's block shape: a batch with fewer work items than
+    schedulers runs four warps per SM (one item per scheduler), a batch that fills many waves
+    eight; the results are those of single requests either way."""
+    ctx = contexts(70)
+    few = _requests([(20, 30, 30.0, 70), (40, 25, 60.0, 36), (9, 12, 30.0, 20)], 5)
+    outs = ctx.propagate_batch(few)
+    assert ctx.batch_warps_per_sm == 4
+    _compare(outs, few, lambda q: contexts(q["degree"]), 1e-6, 1e-9)
+    many = _requests([(512, 40, 30.0, 70)] * 120, 6)
+    outs = ctx.propagate_batch(many)
+    assert ctx.batch_warps_per_sm == 8
+    _compare(outs[:3], many[:3], lambda q: contexts(q["degree"]), 1e-6, 1e-9)
