@@ -319,17 +319,9 @@ gpop_status gpop_create(const gpop_config* cfg_in, gpop_ctx** out)
         || (e = ctx->lane_mixed.ensure(lane_mixed.size())) != cudaSuccess)
         return cuda_fail(ctx, e, "allocating model data");
     uint8_t* mixed = ctx->mixed.as<uint8_t>();
-    // the plain mixed table: with the FP64 recursion, -c as a double in each FP32 entry
-    std::vector<GravEntry32> t32p(t32);
-    if (kRec64)
-        for (int m = 0; m <= L; ++m)
-            for (int n = m; n <= L; ++n) {
-                const double negc = -t64[grav_col_offset(m, L) + (n - m)].c;
-                std::memcpy(&t32p[grav_col_offset(m, L) + (n - m)].c, &negc, sizeof(double));
-            }
     if ((e = cudaMemcpy(ctx->t64.p, t64.data(), ctx->t64_bytes, cudaMemcpyHostToDevice)) != cudaSuccess
         || (e = cudaMemcpy(mixed, head.data(), ctx->mixed_off32, cudaMemcpyHostToDevice)) != cudaSuccess
-        || (e = cudaMemcpy(mixed + ctx->mixed_off32, t32p.data(), t32p.size() * sizeof(GravEntry32),
+        || (e = cudaMemcpy(mixed + ctx->mixed_off32, t32.data(), t32.size() * sizeof(GravEntry32),
                 cudaMemcpyHostToDevice))
             != cudaSuccess
         || (e = cudaMemcpy(ctx->nut.p, nut.data(), nut.size() * sizeof(NutTerm), cudaMemcpyHostToDevice))

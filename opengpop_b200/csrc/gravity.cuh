@@ -351,140 +351,6 @@ __device__ __forceinline__ void column32x2_group(const GravEntry32* const (&e)[C
     }
 }
 
-// ---- FP64 recursion, FP32 sums (kRec64; plain mixed table with -c as a double) ----
-// Per term and object: the recursion Q(n) = u Q(n-1) + (-c w) Q(n-2) in FP64 (one FMA and two
-// products on the FP64 pipe), then Q rounded to FP32 and the six coefficient sums as packed FP32
-// FMAs on the FMA pipe. The two pipes work side by side.
-struct Rec64x2 {
-    double Q1[2], Q2[2], t2[2];
-};
-
-__device__ __forceinline__ double negc64(const GravEntry32* e) { return *reinterpret_cast<const double*>(e); }
-
-__device__ __forceinline__ void sums_r64(const float4& a, const float4& b, const double (&Q)[2], ColSums32<2>& s)
-{
-    const float qa = (float)Q[0], qb = (float)Q[1];
-    const float2 QA = make_float2(qa, qa), QB = make_float2(qb, qb);
-    const float2 cg = make_float2(a.z, a.w), cj = make_float2(b.x, b.y), ch = make_float2(b.z, b.w);
-    s.g[0] = __ffma2_rn(QA, cg, s.g[0]);
-    s.j[0] = __ffma2_rn(QA, cj, s.j[0]);
-    s.h[0] = __ffma2_rn(QA, ch, s.h[0]);
-    s.g[1] = __ffma2_rn(QB, cg, s.g[1]);
-    s.j[1] = __ffma2_rn(QB, cj, s.j[1]);
-    s.h[1] = __ffma2_rn(QB, ch, s.h[1]);
-}
-
-// t2 = (-c(n) w) Q(n-2) for the first term n at entry e
-__device__ __forceinline__ void first_t2_r64(const GravEntry32* __restrict__ e, const double (&w)[2], Rec64x2& R)
-{
-    const double c = negc64(e);
-#pragma unroll
-    for (int k = 0; k < 2; ++k)
-        R.t2[k] = (c * w[k]) * R.Q2[k];
-}
-
-// One term at entry e: t2 holds (-c(n) w) Q(n-2) on entry and (-c(n+1) w) Q(n-1) on exit.
-__device__ __forceinline__ void term_r64(const GravEntry32* __restrict__ e, const double (&u)[2],
-    const double (&w)[2], Rec64x2& R, ColSums32<2>& s)
-{
-    const float4* p = reinterpret_cast<const float4*>(e);
-    const float4 a = p[0], b = p[1];
-    const double cn = negc64(e + 1);
-    double Q[2];
-#pragma unroll
-    for (int k = 0; k < 2; ++k) {
-        Q[k] = fma(u[k], R.Q1[k], R.t2[k]);
-        R.t2[k] = (cn * w[k]) * R.Q1[k];
-        R.Q2[k] = R.Q1[k];
-        R.Q1[k] = Q[k];
-    }
-    sums_r64(a, b, Q, s);
-}
-
-// The single term at entry e of a column whose walk ends there (t2 formed from Q2 first).
-__device__ __forceinline__ void last_term_r64(const GravEntry32* __restrict__ e, const double (&u)[2],
-    const double (&w)[2], Rec64x2& R, ColSums32<2>& s)
-{
-    const float4* p = reinterpret_cast<const float4*>(e);
-    const float4 a = p[0], b = p[1];
-    const double c = negc64(e);
-    double Q[2];
-#pragma unroll
-    for (int k = 0; k < 2; ++k) {
-        Q[k] = fma(u[k], R.Q1[k], (c * w[k]) * R.Q2[k]);
-        R.Q2[k] = R.Q1[k];
-        R.Q1[k] = Q[k];
-    }
-    sums_r64(a, b, Q, s);
-}
-
-__device__ __forceinline__ void column_r64(const GravEntry32* __restrict__ e, int first, int last,
-    const double (&u)[2], const double (&w)[2], Rec64x2& R, ColSums32<2>& s)
-{
-    if (first > last)
-        return;
-    first_t2_r64(e + first, w, R);
-#pragma unroll(kCol32x2Unroll)
-    for (int i = first; i <= last; ++i)
-        term_r64(e + i, u, w, R, s);
-}
-
-// C columns side by side, N terms each (the blocks of column32x2_group).
-template <int C>
-__device__ __forceinline__ void column_r64_group(const GravEntry32* const (&e)[C], int N,
-    const double (&u)[2], const double (&w)[2], Rec64x2 (&R)[C], ColSums32<2> (&s)[C])
-{
-    if (N <= 0)
-        return;
-#pragma unroll
-    for (int c = 0; c < C; ++c)
-        first_t2_r64(e[c], w, R[c]);
-    constexpr int U = C == 2 ? kColPairUnroll : kColGroupUnroll;
-    int i = 0;
-#pragma unroll 1
-    for (; i + U <= N; i += U)
-#pragma unroll
-        for (int j = 0; j < U; ++j)
-#pragma unroll
-            for (int c = 0; c < C; ++c)
-                term_r64(e[c] + i + j, u, w, R[c], s[c]);
-#pragma unroll 1
-    for (; i + 2 <= N; i += 2)
-#pragma unroll
-        for (int j = 0; j < 2; ++j)
-#pragma unroll
-            for (int c = 0; c < C; ++c)
-                term_r64(e[c] + i + j, u, w, R[c], s[c]);
-    if (i < N)
-#pragma unroll
-        for (int c = 0; c < C; ++c)
-            term_r64(e[c] + i, u, w, R[c], s[c]);
-}
-
-// One object (K = 1, the plain table): the same FP64 recursion with FP32 sums.
-__device__ __forceinline__ void column_r64_1(const GravEntry32* __restrict__ e, int first, int last,
-    double u, double w, double& Q1, double& Q2, ColSums32<1>& s)
-{
-    if (first > last)
-        return;
-    double t2 = (negc64(e + first) * w) * Q2;
-#pragma unroll 4
-    for (int i = first; i <= last; ++i) {
-        const float4* p = reinterpret_cast<const float4*>(e + i);
-        const float4 a = p[0], b = p[1];
-        const double cn = negc64(e + i + 1);
-        const double Q = fma(u, Q1, t2);
-        t2 = (cn * w) * Q1;
-        const float qf = (float)Q;
-        const float2 QQ = make_float2(qf, qf);
-        s.g[0] = __ffma2_rn(QQ, make_float2(a.z, a.w), s.g[0]);
-        s.j[0] = __ffma2_rn(QQ, make_float2(b.x, b.y), s.j[0]);
-        s.h[0] = __ffma2_rn(QQ, make_float2(b.z, b.w), s.h[0]);
-        Q2 = Q1;
-        Q1 = Q;
-    }
-}
-
 // Mixed precision, two objects, degree L > 8: the walk of gravity_itrs<true, 2> with the FP32
 // parts of the columns taken kHeadGroup (columns m <= 8) or kTailGroup (m > 8) columns at a time.
 // Every column's sums, their combination and the order of the combinations are those of the
@@ -497,7 +363,6 @@ template <bool LANE> struct MixedWalk2 {
     double G[K], H[K], J[K], KK[K];
     float2 uf, wf;
     float cf[K], sf[K], cpf[K], spf[K], qmf[K], c1f[K], s1f[K], qf[K];
-    double qmd[K]; // q^m in FP64 for the columns m > 8 (kRec64)
     float Gf[K], Hf[K], Jf[K], Kf[K];
 
     __device__ __forceinline__ MixedWalk2(const GravSmem& g, const double (&r)[K], const double (&x)[K],
@@ -583,30 +448,15 @@ template <bool LANE> struct MixedWalk2 {
             for (int c = 0; c < C; ++c)
                 column64<K>(e64[c], 1, kMixedSplit - m - c, u, w, Q1[c], Q2[c], s[c]);
         }
-        if constexpr (kRec64 && !LANE) { // the FP64 recursion continues from its FP64 values
-            Rec64x2 R[C];
 #pragma unroll
-            for (int c = 0; c < C; ++c)
-#pragma unroll
-                for (int k = 0; k < K; ++k) {
-                    R[c].Q1[k] = Q1[c][k];
-                    R[c].Q2[k] = Q2[c][k];
-                }
-            if constexpr (C == 1)
-                column_r64(e[0], 0, L - kMixedSplit - 1, u, w, R[0], f[0]);
-            else
-                column_r64_group<C>(e, L - kMixedSplit, u, w, R, f);
-        } else {
-#pragma unroll
-            for (int c = 0; c < C; ++c) {
-                Q1f[c] = make_float2((float)Q1[c][0], (float)Q1[c][1]);
-                Q2f[c] = make_float2((float)Q2[c][0], (float)Q2[c][1]);
-            }
-            if constexpr (C == 1)
-                column32x2(e[0], 0, L - kMixedSplit - 1, uf, wf, Q1f[0], Q2f[0], f[0]);
-            else
-                column32x2_group<C>(e, L - kMixedSplit, uf, wf, Q1f, Q2f, f);
+        for (int c = 0; c < C; ++c) {
+            Q1f[c] = make_float2((float)Q1[c][0], (float)Q1[c][1]);
+            Q2f[c] = make_float2((float)Q2[c][0], (float)Q2[c][1]);
         }
+        if constexpr (C == 1)
+            column32x2(e[0], 0, L - kMixedSplit - 1, uf, wf, Q1f[0], Q2f[0], f[0]);
+        else
+            column32x2_group<C>(e, L - kMixedSplit, uf, wf, Q1f, Q2f, f);
 #pragma unroll
         for (int c = 0; c < C; ++c) {
 #pragma unroll
@@ -631,7 +481,6 @@ template <bool LANE> struct MixedWalk2 {
             cpf[k] = (float)Cp[k];
             spf[k] = (float)Sp[k];
             qmf[k] = (float)qm[k];
-            qmd[k] = qm[k];
             c1f[k] = (float)C1[k];
             s1f[k] = (float)S1[k];
             qf[k] = (float)q[k];
@@ -654,70 +503,12 @@ template <bool LANE> struct MixedWalk2 {
             cf[k] = cn;
             sf[k] = sn;
             qmf[k] *= qf[k];
-            if constexpr (kRec64 && !LANE)
-                qmd[k] *= q[k];
         }
-    }
-    // tail_group with the FP64 recursion (kRec64): the same terms and order, Q in FP64
-    template <int C> __device__ __forceinline__ void tail_group_r64(int m)
-    {
-        ColSums32<K> f[C];
-        Rec64x2 R[C];
-        const GravEntry32* e[C];
-        double qs[K];
-#pragma unroll
-        for (int k = 0; k < K; ++k)
-            qs[k] = qmd[k];
-#pragma unroll
-        for (int c = 0; c < C; ++c) {
-            if (c > 0) {
-#pragma unroll
-                for (int k = 0; k < K; ++k)
-                    qs[k] = qs[k] * q[k]; // the value combine32 gives qmd at column m + c
-            }
-            const GravEntry32* base = col32<LANE>(gs, m + c);
-            const float4* p = reinterpret_cast<const float4*>(base);
-            const float4 a = p[0], b = p[1];
-#pragma unroll
-            for (int k = 0; k < K; ++k) {
-                const float qf1 = (float)qs[k];
-                const float2 QQ = make_float2(qf1, qf1);
-                f[c].g[k] = __fmul2_rn(QQ, make_float2(a.z, a.w));
-                f[c].j[k] = __fmul2_rn(QQ, make_float2(b.x, b.y));
-                f[c].h[k] = __fmul2_rn(QQ, make_float2(b.z, b.w));
-                R[c].Q1[k] = qs[k];
-                R[c].Q2[k] = 0.0;
-            }
-            e[c] = base + 1;
-        }
-        const int N = L - m - (C - 1);
-        if constexpr (C > 1) {
-            column_r64_group<C>(e, N, u, w, R, f);
-            if constexpr (C == 2) {
-                last_term_r64(e[0] + N, u, w, R[0], f[0]); // column m: one term more
-            } else {
-#pragma unroll
-                for (int c = 0; c + 1 < C; ++c) // column m + c has C - 1 - c terms more
-                    column_r64(e[c] - 1, N + 1, L - m - c, u, w, R[c], f[c]);
-            }
-        } else {
-            column_r64(e[0] - 1, 1, L - m, u, w, R[0], f[0]);
-        }
-#pragma unroll
-        for (int c = 0; c < C; ++c)
-            combine32(m + c, f[c]);
     }
     // columns m .. m + C - 1 (> 8, m + C - 1 <= L) in FP32: the n = m term (Q = q^m) of each, the
     // L - m - C + 1 terms all of them have left side by side, the remaining terms of the longer
     // columns one column at a time, then the combinations in order
     template <int C> __device__ __forceinline__ void tail_group(int m)
-    {
-        if constexpr (kRec64 && !LANE)
-            tail_group_r64<C>(m);
-        else
-            tail_group_fp32<C>(m);
-    }
-    template <int C> __device__ __forceinline__ void tail_group_fp32(int m)
     {
         ColSums32<K> f[C];
         float2 Q1f[C], Q2f[C];
@@ -975,26 +766,12 @@ __device__ __forceinline__ void gravity_itrs(const GravSmem& gs, const double (&
                 const GravEntry64* e = gs.t64 + grav_col_offset(m, kMixedSplit);
                 s.add(e, Q1);
                 column64<K>(e, 1, top - m, u, w, Q1, Q2, s);
-                if constexpr (kRec64) { // FP64 recursion on from the FP64 head values
-                    if constexpr (K == 1) {
-                        column_r64_1(e32, kMixedSplit + 1 - m, L - m, u[0], w[0], Q1[0], Q2[0], f);
-                    } else {
-                        Rec64x2 R;
 #pragma unroll
-                        for (int k = 0; k < K; ++k) {
-                            R.Q1[k] = Q1[k];
-                            R.Q2[k] = Q2[k];
-                        }
-                        column_r64(e32, kMixedSplit + 1 - m, L - m, u, w, R, f);
-                    }
-                } else {
-#pragma unroll
-                    for (int k = 0; k < K; ++k) {
-                        Q1f[k] = (float)Q1[k];
-                        Q2f[k] = (float)Q2[k];
-                    }
-                    column32k<K>(e32, kMixedSplit + 1 - m, L - m, uf, wf, Q1f, Q2f, f);
+                for (int k = 0; k < K; ++k) {
+                    Q1f[k] = (float)Q1[k];
+                    Q2f[k] = (float)Q2[k];
                 }
+                column32k<K>(e32, kMixedSplit + 1 - m, L - m, uf, wf, Q1f, Q2f, f);
             } else {
                 // n = m term (Q = q^m), then the rest of the column with Q(m-1, m) = 0
                 const float4* p = reinterpret_cast<const float4*>(e32);
@@ -1045,10 +822,8 @@ __device__ __forceinline__ void gravity_itrs(const GravSmem& gs, const double (&
             // K, H, added to the FP64 totals once
             float cf[K], sf[K], cpf[K], spf[K], qmf[K], c1f[K], s1f[K], qf[K];
             float Gf[K], Hf[K], Jf[K], Kf[K];
-            double qmd[K]; // q^m in FP64 (kRec64)
 #pragma unroll
             for (int k = 0; k < K; ++k) {
-                qmd[k] = qm[k];
                 cf[k] = (float)Cm[k];
                 sf[k] = (float)Sm[k];
                 cpf[k] = (float)Cp[k];
@@ -1068,30 +843,14 @@ __device__ __forceinline__ void gravity_itrs(const GravSmem& gs, const double (&
                 float Q1f[K], Q2f[K];
 #pragma unroll
                 for (int k = 0; k < K; ++k) {
-                    const float qs = kRec64 ? (float)qmd[k] : qmf[k];
-                    const float2 QQ = make_float2(qs, qs);
+                    const float2 QQ = make_float2(qmf[k], qmf[k]);
                     f.g[k] = __fmul2_rn(QQ, make_float2(a.z, a.w));
                     f.j[k] = __fmul2_rn(QQ, make_float2(b.x, b.y));
                     f.h[k] = __fmul2_rn(QQ, make_float2(b.z, b.w));
                     Q1f[k] = qmf[k];
                     Q2f[k] = 0.f;
                 }
-                if constexpr (kRec64) {
-                    if constexpr (K == 1) {
-                        double Q1d = qmd[0], Q2d = 0.0;
-                        column_r64_1(e32, 1, L - m, u[0], w[0], Q1d, Q2d, f);
-                    } else {
-                        Rec64x2 R;
-#pragma unroll
-                        for (int k = 0; k < K; ++k) {
-                            R.Q1[k] = qmd[k];
-                            R.Q2[k] = 0.0;
-                        }
-                        column_r64(e32, 1, L - m, u, w, R, f);
-                    }
-                } else {
-                    column32k<K>(e32, 1, L - m, uf, wf, Q1f, Q2f, f);
-                }
+                column32k<K>(e32, 1, L - m, uf, wf, Q1f, Q2f, f);
                 const float dm = (float)m;
 #pragma unroll
                 for (int k = 0; k < K; ++k) {
@@ -1106,7 +865,6 @@ __device__ __forceinline__ void gravity_itrs(const GravSmem& gs, const double (&
                     cf[k] = cn;
                     sf[k] = sn;
                     qmf[k] *= qf[k];
-                    qmd[k] *= q[k];
                 }
             }
 #pragma unroll
@@ -1158,10 +916,9 @@ __device__ __forceinline__ void column32_comp(const GravEntry32* __restrict__ e,
         const float4* p = reinterpret_cast<const float4*>(e + i);
         const float4 a = p[0], b = p[1]; // (-c, -c, g1, g2 | j1, j2, h1, h2)
         const float coef[6] = { a.z, a.w, b.x, b.y, b.z, b.w };
-        const float negc = kRec64 ? (float)negc64(e + i) : a.x; // -c as a double (kRec64 table)
 #pragma unroll
         for (int k = 0; k < K; ++k) {
-            const float t2 = (negc * w[k]) * Q2[k];
+            const float t2 = (a.x * w[k]) * Q2[k];
             const float Q = fmaf(u[k], Q1[k], t2);
 #pragma unroll
             for (int c = 0; c < 6; ++c)

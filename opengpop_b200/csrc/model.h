@@ -58,15 +58,6 @@ struct alignas(16) GravEntry32 {
 static_assert(sizeof(GravEntry64) == 64, "layout");
 static_assert(sizeof(GravEntry32) == 32, "layout");
 
-// Mixed precision with the recursion in FP64: the Q(n, m) recursion of the degree > 8 terms runs
-// in FP64 (on the FP64 pipe, which the FP32 walk leaves idle) and only the six coefficient sums
-// run in FP32. The plain mixed table then holds -c as a double in the first 8 bytes of each FP32
-// entry (c and pad); the lane-layout tables keep the FP32 pair.
-#ifndef GPOP_REC64
-#define GPOP_REC64 0
-#endif
-constexpr bool kRec64 = GPOP_REC64 != 0;
-
 #ifdef __CUDACC__
 #define GPOP_HOST_DEVICE __host__ __device__
 #else
