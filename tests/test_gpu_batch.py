@@ -147,10 +147,11 @@ def test_tune_cache_roundtrip(contexts, tmp_path):
     ctx.tune(path)
     lines = open(path).read().split("\n")
     rows = [l.split() for l in lines if l.strip()]
-    assert len(rows) == 24
-    eta = {(int(L), int(P)): float(e) for _, L, P, e in rows}
+    assert len(rows) == 48  # (warps per SM 4 | 8) x degrees {8, 20, 36, 70} x lanes 1..32
+    eta = {(int(W), int(L), int(P)): float(e) for _, W, L, P, e in rows}
     assert all(e > 0 for e in eta.values())
-    assert eta[(8, 1)] > eta[(70, 1)]  # lower degree, more object-steps per second
+    for W in (4, 8):
+        assert eta[(W, 8, 1)] > eta[(W, 70, 1)]  # lower degree, more object-steps per second
     ctx.tune(path)  # read back from the cache
     reqs = _requests(SPEC[:4], 8)
     _compare(ctx.propagate_batch(reqs), reqs, lambda q: contexts(q["degree"]), 1e-3, 1e-6)
