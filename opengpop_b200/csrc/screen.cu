@@ -26,6 +26,10 @@ constexpr int kStepChunk = 16; // steps staged per pass
 // shared memory: two chunk buffers of [step][axis][a tile | b tile][64] doubles
 constexpr int kChunkDoubles = kStepChunk * 3 * 2 * kTile;
 constexpr size_t kScreenSmem = 2 * (size_t)kChunkDoubles * sizeof(double);
+#ifndef GPOP_SCREEN_INT_COMPARE
+#define GPOP_SCREEN_INT_COMPARE 1
+#endif
+constexpr bool kIntCompare = GPOP_SCREEN_INT_COMPARE != 0;
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p)
 {
@@ -129,9 +133,11 @@ __global__ void __launch_bounds__(256) screen_kernel(ScreenArgs a)
                     const double dx = ax[i] - bx[j];
                     const double dy = ay[i] - by[j];
                     const double dz = az[i] - bz[j];
-                    const unsigned long long d2
-                        = (unsigned long long)__double_as_longlong(dx * dx + dy * dy + dz * dz);
-                    if (d2 < best[i][j]) {
+                    const double d2f = dx * dx + dy * dy + dz * dz;
+                    const unsigned long long d2 = (unsigned long long)__double_as_longlong(d2f);
+                    const bool better = kIntCompare ? d2 < best[i][j]
+                                                    : d2f < __longlong_as_double((long long)best[i][j]);
+                    if (better) {
                         best[i][j] = d2;
                         bstep[i][j] = step;
                     }
