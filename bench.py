@@ -208,6 +208,36 @@ def probe_peak(torch, fp64, dev):
     return best
 
 
+def probe_pipes(torch, dev):
+    """Milliseconds of 6 packed FP32 FMA chains, 6 FP64 FMA chains, and both interleaved, per
+    thread, one 256-thread block per SM (libgpop_probe.so): whether the FP64 pipe can work beside
+    the FMA pipe (both interleaved taking the longer of the two times) or not (their sum)."""
+    lib = C.CDLL(os.path.join(ROOT, "opengpop_b200", "lib", "libgpop_probe.so"))
+    lib.gpop_probe_mix.restype = C.c_int
+    lib.gpop_probe_mix.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p]
+    scratch = torch.zeros(16, dtype=torch.float32, device=dev)
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    stream = torch.cuda.current_stream()
+    out = {}
+    for mode, name in ((0, "fp32x2_ms"), (1, "fp64_ms"), (2, "interleaved_ms")):
+        best = None
+        for it in range(4):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            rc = lib.gpop_probe_mix(mode, sms, 4000, C.c_void_p(scratch.data_ptr()),
+                                    C.c_void_p(stream.cuda_stream))
+            e1.record(stream)
+            torch.cuda.synchronize()
+            if rc != 0:
+                return None
+            if it:
+                ms = e0.elapsed_time(e1)
+                best = ms if best is None else min(best, ms)
+        out[name] = best
+    return out
+
+
 # ---- auxiliary workloads (one GPU; each prints its own JSON line) ----
 def w_jac(L):
     """FP64 flops of one gravity evaluation with its 3x3 Jacobian at degree L: per (n, m) term
@@ -738,6 +768,7 @@ def main():
     # (the probe's live FMA-chain figures are reported beside them)
     probe64 = probe_peak(torch, True, dev)
     probe32 = probe_peak(torch, False, dev)
+    pipes = probe_pipes(torch, dev)
     peak64, peak32 = clock_peaks(clocks.get("sm_mhz"), dev)
     if not peak64:
         peak64, peak32 = probe64, probe32
@@ -813,7 +844,8 @@ def main():
                                            if probe64 and probe32 else None),
                          "peaks_measured": {"fp64_tflops": probe64, "fp32_tflops": probe32,
                                             "how": "live FMA-chain probe (libgpop_probe.so)"},
-                         "peaks_clock": {"fp64_tflops": peak64, "fp32_tflops": peak32}},
+                         "peaks_clock": {"fp64_tflops": peak64, "fp32_tflops": peak32},
+                         "fp64_beside_fp32_probe": pipes},
             "cpu_baseline": cpu,
             "screen": screen,
             "reference_cuda": ref_cuda,

@@ -45,7 +45,54 @@ __global__ void __launch_bounds__(256) fma32_kernel(float* out, int iters, float
         out[0] = s;
 }
 
+// Packed FP32 chains, FP64 chains, or both interleaved (6 + 6 per iteration): whether the FP64
+// pipe can work beside the FMA pipe. Time with one block of 256 threads per SM.
+__global__ void __launch_bounds__(256) mix_kernel(float* out, int mode, int iters, float a, float b,
+    double da, double db)
+{
+    float2 x[6];
+    double y[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        x[k] = make_float2(threadIdx.x * 1e-7f + k, k * 0.5f);
+        y[k] = threadIdx.x * 1e-9 + k;
+    }
+    const float2 A = make_float2(a, a), B = make_float2(b, b);
+    if (mode == 0) {
+        for (int i = 0; i < iters; ++i)
+#pragma unroll
+            for (int k = 0; k < 6; ++k)
+                x[k] = __ffma2_rn(x[k], A, B);
+    } else if (mode == 1) {
+        for (int i = 0; i < iters; ++i)
+#pragma unroll
+            for (int k = 0; k < 6; ++k)
+                y[k] = fma(y[k], da, db);
+    } else {
+        for (int i = 0; i < iters; ++i)
+#pragma unroll
+            for (int k = 0; k < 6; ++k) {
+                x[k] = __ffma2_rn(x[k], A, B);
+                y[k] = fma(y[k], da, db);
+            }
+    }
+    float s = 0.f;
+#pragma unroll
+    for (int k = 0; k < 6; ++k)
+        s += x[k].x + x[k].y + (float)y[k];
+    if (s == 12345.f)
+        out[0] = s;
+}
+
 } // namespace
+
+extern "C" __attribute__((visibility("default"))) int gpop_probe_mix(int mode, int blocks, int iters,
+    void* scratch, void* stream)
+{
+    mix_kernel<<<blocks, 256, 0, (cudaStream_t)stream>>>((float*)scratch, mode, iters, 0.999f, 1e-4f,
+        0.999999, 1e-7);
+    return (int)cudaGetLastError();
+}
 
 extern "C" __attribute__((visibility("default"))) int gpop_probe_fma(int fp64, int blocks,
     int iters, void* scratch, void* stream, double* flops_out)
