@@ -262,6 +262,59 @@ def _common(args, metric, value, unit, dtype, config, extra):
     print(json.dumps(line), flush=True)
 
 
+def batch_cpu_baseline(reqs, seconds_target=12.0, max_object_steps=200000):
+    """Oracle (CPU FP64 restatement, OpenMP over objects) on whole requests of the batch, in a
+    seeded random order, until about seconds_target of CPU work; requests of more than
+    max_object_steps object-steps are left out of the sample. Returns object-steps/s, cores and a
+    description."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_api as O
+    cores = cpu_cores()
+    data = {}
+    order = np.random.default_rng(SEED).permutation(len(reqs))
+    done, osteps, t_all, used = 0, 0, 0.0, 0
+    for i in order:
+        q = reqs[i]
+        n = q["r"].shape[0]
+        if q["steps"] == 0 or n * q["steps"] > max_object_steps:
+            continue
+        L = q["degree"]
+        if L not in data:
+            data[L] = O.Data(degree=L)
+        t0 = time.perf_counter()
+        O.propagate(data[L], "gravity", q["start"], q["h"], q["steps"], q["r"], q["v"], threads=cores)
+        t_all += time.perf_counter() - t0
+        osteps += n * q["steps"]
+        used += 1
+        if t_all >= seconds_target:
+            break
+    return osteps / max(t_all, 1e-9), cores, ("%d of the %d requests (seeded random order; those of "
+                                              "at most %d object-steps), %d object-steps, %.1f s of "
+                                              "CPU work" % (used, len(reqs), max_object_steps, osteps,
+                                                            t_all))
+
+
+def adjoint_cpu_baseline(r, v, pairs, steps, seconds_target=12.0):
+    """Miss-distance gradients on the CPU by central differences of the oracle (FP64, 25 runs of
+    the pair per gradient, OpenMP over the runs): gradients per second on pairs taken in order
+    until about seconds_target of CPU work."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_api as O
+    data = O.Data()
+    cores = cpu_cores()
+    t_all, k = 0.0, 0
+    while t_all < seconds_target and k < len(pairs):
+        a, b = pairs[k]
+        t0 = time.perf_counter()
+        O.miss_fd_ld(data, START, H, steps, r[a], v[a], r[b], v[b], 1.0, 1e-3, threads=cores,
+                     long=False)
+        t_all += time.perf_counter() - t0
+        k += 1
+    return k / max(t_all, 1e-9), cores, ("%d pairs over %d steps, gradient by central differences "
+                                         "(25 FP64 propagations of the pair each), %.1f s of CPU "
+                                         "work" % (k, steps, t_all))
+
+
 def run_batch(args, torch, G, dev):
     """Batched uneven requests: 4,096 requests in one persistent launch under a captured graph.
     Under torchrun the requests are split over the ranks by longest-processing-time bin packing of
@@ -297,6 +350,7 @@ def run_batch(args, torch, G, dev):
         dev_t.append(ctx.batch_device_seconds)
     clocks = sampler.stop()
     launches = ctx.kernel_launches - launches0
+    warps = ctx.batch_warps_per_sm
     ctx.close()
     t = sharding.max_over_ranks(sum(dev_t) / len(dev_t), dev)
     t_wall = sharding.max_over_ranks(sum(wall_t) / len(wall_t), dev)
@@ -306,6 +360,10 @@ def run_batch(args, torch, G, dev):
     if rank != 0:
         return 0
     peak64, peak32 = _peaks(torch, dev, clocks)
+    cpu = None
+    if not args.no_cpu_baseline:
+        rate, cores, desc = batch_cpu_baseline(all_reqs)
+        cpu = {"value": rate, "unit": "object-steps/s", "cores": cores, "kind": "port", "sample": desc}
     achieved = f_total / t / 1e12
     t_min = (f_total - f32) / (peak64 * 1e12) + f32 / (peak32 * 1e12) if peak64 and peak32 else None
     io = sum(q["r"].shape[0] for q in all_reqs) * 6 * 8
@@ -329,7 +387,8 @@ def run_batch(args, torch, G, dev):
                           "peak": f_total / t_min / 1e12 if t_min else None, "unit": "TFLOP/s",
                           "frac": achieved / (f_total / t_min / 1e12) if t_min else None,
                           "traffic": None},
-             "cpu_baseline": None, "clocks": clocks, "gpu_launches": launches})
+             "warps_per_sm": warps,
+             "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches})
     return 0
 
 
@@ -390,6 +449,10 @@ def run_screen(args, torch, G, dev):
     args.gpus = world
     pair_steps = pairs * steps
     peak64 = _peaks(torch, dev, clocks)[0]
+    cpu = None
+    if not args.no_cpu_baseline:
+        rate, cores, desc = screen_cpu_baseline(torch, G, r, v)
+        cpu = {"value": rate, "unit": "pair-steps/s", "cores": cores, "kind": "port", "sample": desc}
     achieved = 9.0 * pair_steps / t_screen / 1e12
     _common(args, "conjunction pair-steps/s of the screen (FP64)", pair_steps / t_screen,
             "pair-steps/s", "f64",
@@ -412,7 +475,7 @@ def run_screen(args, torch, G, dev):
              "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak64, "unit": "TFLOP/s",
                           "frac": achieved / peak64 if peak64 else None, "traffic": None,
                           "per_unit": "9 FP64 flops per pair-step"},
-             "cpu_baseline": None, "clocks": clocks, "gpu_launches": launches})
+             "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches})
     return 0
 
 
@@ -452,6 +515,10 @@ def run_adjoint(args, torch, G, dev):
     f_miss = units * steps * (2 * flops_per_object_step() + w_jac(DEGREE)) + units * 145 * w_jac(DEGREE)
     f_stm = n_stm * steps * (flops_per_object_step() + w_jac(DEGREE) + 6 * 500) + n_stm * 145 * w_jac(DEGREE)
     peak64 = _peaks(torch, dev, clocks)[0]
+    cpu = None
+    if not args.no_cpu_baseline:
+        rate, cores, desc = adjoint_cpu_baseline(r, v, pairs, steps)
+        cpu = {"value": rate, "unit": "pairs/s", "cores": cores, "kind": "port", "sample": desc}
     ach = f_miss / tm / 1e12
     _common(args, "miss-distance gradients/s (adjoint, FP64)", n_pairs / tm, "pairs/s", "f64",
             {"workload": "%d LEO pairs (seed %d), 70x70, 30 s, %d steps (24 h), checkpoint every 64 "
@@ -465,7 +532,7 @@ def run_adjoint(args, torch, G, dev):
                           "frac": ach / peak64 if peak64 else None, "traffic": None,
                           "per_unit": "per unit-step 2 (7 W + 500) + W_J, W(70) = %d, "
                                       "W_J(70) = %d flops" % (W, w_jac(DEGREE))},
-             "cpu_baseline": None, "clocks": clocks, "gpu_launches": launches})
+             "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches})
     return 0
 
 

@@ -1674,18 +1674,20 @@ void or_ca_refine(int64_t n, const uint32_t* ids, double h, uint32_t total_steps
     }
 }
 
-int32_t or_miss_fd_ld(const void* dv, const or_time* st, double h, int32_t steps, int32_t ncorr,
+} // extern "C"
+
+template <typename LD>
+static int32_t miss_fd(const void* dv, const or_time* st, double h, int32_t steps, int32_t ncorr,
     int64_t n_pairs, const double* rA, const double* vA, const double* rB, const double* vB, double dr,
     double dvel, double* miss, double* tca, double* grad, int32_t threads)
 {
-    typedef long double LD;
     if (!dv || n_pairs <= 0 || steps < 1 || h == 0.0)
         return 1;
     Force f = make_force(dv, OR_FORCE_GRAVITY, st, h, steps, 0);
     // run 0: the pair as given; run 1 + 2 c + s: component c (0..11: r_A, v_A, r_B, v_B) moved by
     // +step (s = 0) or -step (s = 1)
     const int runs = 25;
-    std::vector<LD> out((size_t)n_pairs * runs * 2, 0.0L);
+    std::vector<LD> out((size_t)n_pairs * runs * 2, LD(0));
 #pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads(threads))
     for (int64_t job = 0; job < n_pairs * runs; ++job) {
         const int64_t p = job / runs;
@@ -1706,7 +1708,7 @@ int32_t or_miss_fd_ld(const void* dv, const or_time* st, double h, int32_t steps
         LD rf[3], vf[3];
         for (int o = 0; o < 2; ++o) {
             for (int k = 0; k < 3; ++k)
-                tr[o][k].assign((size_t)steps * 3, 0.0L);
+                tr[o][k].assign((size_t)steps * 3, LD(0));
             propagate_one<LD>(f, steps, ncorr, x0[o], x0[o] + 3, 1, 0, tr[o][0].data(), tr[o][1].data(),
                 tr[o][2].data(), rf, vf);
         }
@@ -1726,6 +1728,24 @@ int32_t or_miss_fd_ld(const void* dv, const or_time* st, double h, int32_t steps
         }
     }
     return 0;
+}
+
+extern "C" {
+
+int32_t or_miss_fd_ld(const void* dv, const or_time* st, double h, int32_t steps, int32_t ncorr,
+    int64_t n_pairs, const double* rA, const double* vA, const double* rB, const double* vB, double dr,
+    double dvel, double* miss, double* tca, double* grad, int32_t threads)
+{
+    return miss_fd<long double>(dv, st, h, steps, ncorr, n_pairs, rA, vA, rB, vB, dr, dvel, miss, tca, grad,
+        threads);
+}
+
+int32_t or_miss_fd(const void* dv, const or_time* st, double h, int32_t steps, int32_t ncorr,
+    int64_t n_pairs, const double* rA, const double* vA, const double* rB, const double* vB, double dr,
+    double dvel, double* miss, double* tca, double* grad, int32_t threads)
+{
+    return miss_fd<double>(dv, st, h, steps, ncorr, n_pairs, rA, vA, rB, vB, dr, dvel, miss, tca, grad,
+        threads);
 }
 
 } // extern "C"

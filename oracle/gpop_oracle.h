@@ -145,6 +145,10 @@ void or_ca_refine(int64_t n, const uint32_t* set_ids, double h, uint32_t total_s
 int32_t or_miss_fd_ld(const void* data, const or_time* start, double h, int32_t steps, int32_t ncorr,
     int64_t n_pairs, const double* rA, const double* vA, const double* rB, const double* vB, double dr,
     double dv, double* miss, double* tca, double* grad, int32_t threads);
+/* The same in double precision (the CPU baseline of the miss-gradient workload). */
+int32_t or_miss_fd(const void* data, const or_time* start, double h, int32_t steps, int32_t ncorr,
+    int64_t n_pairs, const double* rA, const double* vA, const double* rB, const double* vB, double dr,
+    double dv, double* miss, double* tca, double* grad, int32_t threads);
 
 #ifdef __cplusplus
 }

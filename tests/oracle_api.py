@@ -97,10 +97,11 @@ def lib():
                                       C.c_int32]
         _lib.or_ca_refine.argtypes = [C.c_int64, C.c_void_p, C.c_double, C.c_uint32,
                                       C.POINTER(OrCaState)] + [C.c_void_p] * 4 + [C.c_int32]
-        _lib.or_miss_fd_ld.restype = C.c_int32
-        _lib.or_miss_fd_ld.argtypes = [C.c_void_p, C.POINTER(OrTime), C.c_double, C.c_int32,
-                                       C.c_int32, C.c_int64] + [C.c_void_p] * 4 + [
-            C.c_double, C.c_double] + [C.c_void_p] * 3 + [C.c_int32]
+        for fn in ("or_miss_fd_ld", "or_miss_fd"):
+            getattr(_lib, fn).restype = C.c_int32
+            getattr(_lib, fn).argtypes = [C.c_void_p, C.POINTER(OrTime), C.c_double, C.c_int32,
+                                          C.c_int32, C.c_int64] + [C.c_void_p] * 4 + [
+                C.c_double, C.c_double] + [C.c_void_p] * 3 + [C.c_int32]
     return _lib
 
 
@@ -224,17 +225,18 @@ def closest_approach(r_steps, v_steps, a_steps, set_ids, h, phases=None, threads
                 partition=p)
 
 
-def miss_fd_ld(data, start, h, steps, rA, vA, rB, vB, dr, dv, ncorr=7, threads=0):
+def miss_fd_ld(data, start, h, steps, rA, vA, rB, vB, dr, dv, ncorr=7, threads=0, long=True):
     """Miss distance, TCA and the central-difference gradient of the miss distance (steps dr in
-    m, dv in m/s) per pair, computed in long double (or_miss_fd_ld). Returns (miss, tca, grad
-    [n, 12] ordered r0_A, v0_A, r0_B, v0_B)."""
+    m, dv in m/s) per pair, computed in long double (or_miss_fd_ld; double with long=False).
+    Returns (miss, tca, grad [n, 12] ordered r0_A, v0_A, r0_B, v0_B)."""
     rA, vA, rB, vB = (f64(x).reshape(-1, 3) for x in (rA, vA, rB, vB))
     n = rA.shape[0]
     miss = np.zeros(n)
     tca = np.zeros(n)
     grad = np.zeros((n, 12))
-    rc = lib().or_miss_fd_ld(data.h, C.byref(tstruct(start)), h, steps, ncorr, n, ptr(rA), ptr(vA),
-                             ptr(rB), ptr(vB), dr, dv, ptr(miss), ptr(tca), ptr(grad), threads)
+    fn = lib().or_miss_fd_ld if long else lib().or_miss_fd
+    rc = fn(data.h, C.byref(tstruct(start)), h, steps, ncorr, n, ptr(rA), ptr(vA), ptr(rB), ptr(vB),
+            dr, dv, ptr(miss), ptr(tca), ptr(grad), threads)
     if rc != 0:
         raise RuntimeError("oracle or_miss_fd_ld failed")
     return miss, tca, grad
