@@ -605,9 +605,12 @@ def screen_cpu_baseline(torch, G, r, v, rows=40, window=240, seconds_target=10.0
             done += k
         return time.perf_counter() - t0
 
-    t8 = run(8)
-    steps = int(max(8, seconds_target * 8 / max(t8, 1e-6)))
-    dt = run(steps)
+    steps = 8
+    for _ in range(4):  # the first runs are dominated by the state set-up: scale until the work dominates
+        dt = run(steps)
+        if dt >= 0.5 * seconds_target:
+            break
+        steps = int(steps * seconds_target / max(dt, 1e-3))
     return P * steps / dt, cores, ("%d set objects against the other %d objects (%d pairs) x %d "
                                    "steps (the first %d steps of the GPU trajectory, repeated), "
                                    "%.1f s of CPU work" % (rows, n - rows, P, steps, window, dt))
