@@ -604,11 +604,14 @@ __global__ void finalize_unit_kernel(double h, double* r, double* v, const doubl
 }
 
 // ---- launchers ----
+// Blocks of exactly the threads each SM needs (a multiple of 2, at least 32), so that one block per
+// SM covers n on every SM: rounding the block up to whole warps left SMs idle (65,536 objects at
+// two per thread: 147 of 148 SMs; the last warp of a block may be partial).
 LaunchShape pick_shape(int64_t n, int max_block, int num_sms)
 {
     LaunchShape ls;
     int64_t per_sm = (n + num_sms - 1) / num_sms;
-    int64_t block = ((per_sm + 31) / 32) * 32;
+    int64_t block = ((per_sm + 1) / 2) * 2;
     if (block < 32)
         block = 32;
     if (block > max_block)
@@ -772,7 +775,10 @@ cudaError_t launch_gj8(const TableSrc& ts, const PropArgs& a, int num_sms, cudaS
         const int64_t threads = groups * P;
         const int64_t per_sm = (threads + num_sms - 1) / num_sms; // spread over every SM
         const int cap = K == 1 ? 512 : 256;
-        const int block = (int)std::min<int64_t>(cap, std::max<int64_t>(32, ((per_sm + 31) / 32) * 32));
+        // whole lane groups per block (a multiple of P, at least a warp), sized so that every SM
+        // gets a block: rounding up to whole warps left SMs idle (20,000 objects with two lanes:
+        // 139 of 148 SMs busy with 288-thread blocks, 148 with 272)
+        const int block = (int)std::min<int64_t>(cap, std::max<int64_t>(32, ((per_sm + P - 1) / P) * P));
         const unsigned grid = (unsigned)((threads + block - 1) / block);
         const size_t smem = table_smem_bytes(lt);
         cudaError_t e;
