@@ -54,6 +54,7 @@ struct PropArgs {
     int traj_step0 = 1;
     double* out_r = nullptr; // AoS [n][3] written at the end of the range (may be NULL)
     double* out_v = nullptr;
+    int64_t obj_lo = 0, obj_hi = -1; // lane kernel: objects [obj_lo, obj_hi) of n (-1: n)
 };
 
 struct LaunchShape {

@@ -383,8 +383,9 @@ __global__ void __launch_bounds__(MAXT, 1) gj8_lanes_kernel(TableSrc ts, PropArg
     const int64_t groups = ((int64_t)gridDim.x * blockDim.x) / P;
     const int lane = (int)(threadIdx.x & 31);
     const int l = lane & (P - 1);
-    const int64_t n = a.n;
-    if (grp >= n)
+    const int64_t n = a.n; // the state's stride; this launch runs objects [lo, hi)
+    const int64_t lo = a.obj_lo, hi = a.obj_hi < 0 ? n : a.obj_hi;
+    if (grp >= hi - lo)
         return; // whole groups leave: shuffles name the group only
     const unsigned mask = P == 32 ? 0xffffffffu : ((1u << P) - 1u) << (lane & ~(P - 1));
     const bool lead = l == 0;
@@ -392,9 +393,9 @@ __global__ void __launch_bounds__(MAXT, 1) gj8_lanes_kernel(TableSrc ts, PropArg
     bool live[K];
 #pragma unroll
     for (int k = 0; k < K; ++k) {
-        const int64_t o = grp + k * groups;
-        live[k] = o < n;
-        obj[k] = live[k] ? o : grp; // idle slots shadow the group's first object and never store
+        const int64_t o = lo + grp + k * groups;
+        live[k] = o < hi;
+        obj[k] = live[k] ? o : lo + grp; // idle slots shadow the group's first object and never store
     }
     double* st = a.state;
     const double h = a.h;
@@ -752,6 +753,61 @@ int default_walk(int64_t n, int num_sms, bool lanes, bool fp64_gravity)
     return kWalkOneObject;
 }
 
+#ifndef GPOP_SPLIT_LANES
+#define GPOP_SPLIT_LANES 1
+#endif
+constexpr bool kSplitLanes = GPOP_SPLIT_LANES != 0;
+
+// The lane kernel over objects [lo, hi) (of a.n) with P lanes per group of K objects: whole lane
+// groups per block (a multiple of P, at least a warp), sized so that every SM gets a block
+// (rounding up to whole warps left SMs idle: 20,000 objects with two lanes ran on 139 of 148 SMs
+// with 288-thread blocks, on 148 with 272).
+static cudaError_t launch_lanes_range(const TableSrc& lt, const PropArgs& a0, int K, int P, int64_t lo,
+    int64_t hi, int num_sms, cudaStream_t s)
+{
+    PropArgs a = a0;
+    a.obj_lo = lo;
+    a.obj_hi = hi;
+    const int64_t groups = (hi - lo + K - 1) / K;
+    const int64_t threads = groups * P;
+    const int64_t per_sm = (threads + num_sms - 1) / num_sms; // spread over every SM
+    const int cap = K == 1 ? 512 : 256;
+    const int block = (int)std::min<int64_t>(cap, std::max<int64_t>(32, ((per_sm + P - 1) / P) * P));
+    const unsigned grid = (unsigned)((threads + block - 1) / block);
+    const size_t smem = table_smem_bytes(lt);
+    cudaError_t e;
+    if (lt.mixed) {
+        if (K == 1 && block <= kLanesBlockMid) {
+            if ((e = set_smem(gj8_lanes_kernel<true, 1, kLanesBlockMid>, smem)) != cudaSuccess)
+                return e;
+            gj8_lanes_kernel<true, 1, kLanesBlockMid><<<grid, block, smem, s>>>(lt, a, P);
+        } else if (K == 1) {
+            if ((e = set_smem(gj8_lanes_kernel<true, 1>, smem)) != cudaSuccess)
+                return e;
+            gj8_lanes_kernel<true, 1><<<grid, block, smem, s>>>(lt, a, P);
+        } else {
+            if ((e = set_smem(gj8_lanes_kernel<true, 2>, smem)) != cudaSuccess)
+                return e;
+            gj8_lanes_kernel<true, 2><<<grid, block, smem, s>>>(lt, a, P);
+        }
+    } else {
+        if (K == 1 && block <= kLanesBlockMid) {
+            if ((e = set_smem(gj8_lanes_kernel<false, 1, kLanesBlockMid>, smem)) != cudaSuccess)
+                return e;
+            gj8_lanes_kernel<false, 1, kLanesBlockMid><<<grid, block, smem, s>>>(lt, a, P);
+        } else if (K == 1) {
+            if ((e = set_smem(gj8_lanes_kernel<false, 1>, smem)) != cudaSuccess)
+                return e;
+            gj8_lanes_kernel<false, 1><<<grid, block, smem, s>>>(lt, a, P);
+        } else {
+            if ((e = set_smem(gj8_lanes_kernel<false, 2>, smem)) != cudaSuccess)
+                return e;
+            gj8_lanes_kernel<false, 2><<<grid, block, smem, s>>>(lt, a, P);
+        }
+    }
+    return cudaGetLastError();
+}
+
 cudaError_t launch_gj8(const TableSrc& ts, const PropArgs& a, int num_sms, cudaStream_t s,
     int block_override, int walk, const TableSrc* lane_ts)
 {
@@ -768,50 +824,23 @@ cudaError_t launch_gj8(const TableSrc& ts, const PropArgs& a, int num_sms, cudaS
             walk == kWalkTwoObjects ? walk : kWalkOneObject);
     }
     if ((walk == kWalkLanes || walk == kWalkLanesTwo) && a.kind == 0 && lane_ts) {
-        const TableSrc& lt = *lane_ts;
         const int K = walk == kWalkLanesTwo ? 2 : 1;
-        const int64_t groups = (a.n + K - 1) / K;
         const int P = walk == kWalkLanesTwo ? 2 : lanes_per_object(a.n, num_sms);
-        const int64_t threads = groups * P;
-        const int64_t per_sm = (threads + num_sms - 1) / num_sms; // spread over every SM
-        const int cap = K == 1 ? 512 : 256;
-        // whole lane groups per block (a multiple of P, at least a warp), sized so that every SM
-        // gets a block: rounding up to whole warps left SMs idle (20,000 objects with two lanes:
-        // 139 of 148 SMs busy with 288-thread blocks, 148 with 272)
-        const int block = (int)std::min<int64_t>(cap, std::max<int64_t>(32, ((per_sm + P - 1) / P) * P));
-        const unsigned grid = (unsigned)((threads + block - 1) / block);
-        const size_t smem = table_smem_bytes(lt);
-        cudaError_t e;
-        if (lt.mixed) {
-            if (K == 1 && block <= kLanesBlockMid) {
-                if ((e = set_smem(gj8_lanes_kernel<true, 1, kLanesBlockMid>, smem)) != cudaSuccess)
+        if (K == 1 && kSplitLanes) {
+            // A block of 8 warps and a bit leaves three warps on one scheduler of every SM: the
+            // objects of 8 warps per SM run in one launch, the rest, with more lanes each, in a
+            // second one.
+            const int64_t per_sm = ((a.n * P + num_sms - 1) / num_sms + P - 1) / P * P;
+            const int64_t main_objects = (int64_t)num_sms * 256 / P;
+            if (per_sm > 256 && per_sm <= 288 && main_objects < a.n) {
+                cudaError_t e = launch_lanes_range(*lane_ts, a, 1, P, 0, main_objects, num_sms, s);
+                if (e != cudaSuccess)
                     return e;
-                gj8_lanes_kernel<true, 1, kLanesBlockMid><<<grid, block, smem, s>>>(lt, a, P);
-            } else if (K == 1) {
-                if ((e = set_smem(gj8_lanes_kernel<true, 1>, smem)) != cudaSuccess)
-                    return e;
-                gj8_lanes_kernel<true, 1><<<grid, block, smem, s>>>(lt, a, P);
-            } else {
-                if ((e = set_smem(gj8_lanes_kernel<true, 2>, smem)) != cudaSuccess)
-                    return e;
-                gj8_lanes_kernel<true, 2><<<grid, block, smem, s>>>(lt, a, P);
-            }
-        } else {
-            if (K == 1 && block <= kLanesBlockMid) {
-                if ((e = set_smem(gj8_lanes_kernel<false, 1, kLanesBlockMid>, smem)) != cudaSuccess)
-                    return e;
-                gj8_lanes_kernel<false, 1, kLanesBlockMid><<<grid, block, smem, s>>>(lt, a, P);
-            } else if (K == 1) {
-                if ((e = set_smem(gj8_lanes_kernel<false, 1>, smem)) != cudaSuccess)
-                    return e;
-                gj8_lanes_kernel<false, 1><<<grid, block, smem, s>>>(lt, a, P);
-            } else {
-                if ((e = set_smem(gj8_lanes_kernel<false, 2>, smem)) != cudaSuccess)
-                    return e;
-                gj8_lanes_kernel<false, 2><<<grid, block, smem, s>>>(lt, a, P);
+                const int P2 = lanes_per_object(a.n - main_objects, num_sms);
+                return launch_lanes_range(*lane_ts, a, 1, P2, main_objects, a.n, num_sms, s);
             }
         }
-        return cudaGetLastError();
+        return launch_lanes_range(*lane_ts, a, K, P, 0, a.n, num_sms, s);
     }
     if (walk == kWalkLanes || walk == kWalkLanesTwo)
         walk = kWalkOneObject;
