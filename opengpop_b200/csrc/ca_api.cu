@@ -50,7 +50,7 @@ struct gpop_ca {
 
 namespace {
 
-constexpr int kTile = 64; // rows and columns of a screen tile (screen_kernel's block)
+constexpr int kTile = kScreenTileA; // rows of a screen tile (screen_kernel's block)
 
 __global__ void gather_kernel(const int64_t* idx, int64_t count, const double* dist, const double* time,
     const double* pa, const double* pb, double* out)
@@ -101,9 +101,9 @@ std::vector<int2> staircase_tiles(const gpop_ca* ca, int64_t row_lo, int64_t row
         bound.push_back(s + 1 >= ca->num_sets ? (int)n : (int)ca->set_offsets[s + 1]);
     }
     std::vector<int2> tiles;
-    for (int64_t b0 = 0; b0 < n; b0 += kTile)
+    for (int64_t b0 = 0; b0 < n; b0 += kScreenTileB)
         for (size_t t = 0; t < bound.size(); ++t)
-            if (bound[t] < n && b0 + kTile > bound[t])
+            if (bound[t] < n && b0 + kScreenTileB > bound[t])
                 tiles.push_back(make_int2((int)(row_lo + (int64_t)t * kTile), (int)b0));
     return tiles;
 }

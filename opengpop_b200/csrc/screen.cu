@@ -20,11 +20,14 @@
 
 namespace gpop {
 
-constexpr int kTile = 64; // objects per tile side
-constexpr int kSub = 4; // pairs per thread side
+constexpr int kTileA = kScreenTileA; // rows (first objects) per tile
+constexpr int kTileB = kScreenTileB; // columns (second objects) per tile
+constexpr int kSub = 4; // rows per thread
+constexpr int kSubB = kScreenSubB; // columns per thread (strided by 16)
+constexpr int kRow = kTileA + kTileB; // doubles per staged (step, axis) row: a tile, then b tile
 constexpr int kStepChunk = 16; // steps staged per pass
-// shared memory: two chunk buffers of [step][axis][a tile | b tile][64] doubles
-constexpr int kChunkDoubles = kStepChunk * 3 * 2 * kTile;
+// shared memory: two chunk buffers of [step][axis][a tile | b tile] doubles
+constexpr int kChunkDoubles = kStepChunk * 3 * kRow;
 constexpr size_t kScreenSmem = 2 * (size_t)kChunkDoubles * sizeof(double);
 
 
@@ -39,12 +42,11 @@ __device__ __forceinline__ uint32_t smem_addr(const void* p)
 __device__ __forceinline__ void stage_chunk(double* buf, const double* __restrict__ traj, int64_t N,
     int a0, int b0, int k0, int kc)
 {
-    for (int e = threadIdx.x; e < kc * 3 * 2 * kTile; e += blockDim.x) {
-        const int o = e % kTile;
-        const int side = (e / kTile) & 1;
-        const int c = (e / (2 * kTile)) % 3;
-        const int k = e / (6 * kTile);
-        int64_t obj = (side ? b0 : a0) + o;
+    for (int e = threadIdx.x; e < kc * 3 * kRow; e += blockDim.x) {
+        const int w = e % kRow; // place in the row: a tile then b tile
+        const int c = (e / kRow) % 3;
+        const int k = e / (3 * kRow);
+        int64_t obj = w < kTileA ? a0 + w : b0 + (w - kTileA);
         obj = obj < N ? obj : N - 1;
         const double* src = traj + ((int64_t)(k0 + k) * 3 + c) * N + obj;
         asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_addr(buf + e)), "l"(src)
@@ -66,15 +68,15 @@ __global__ void __launch_bounds__(256) screen_kernel(ScreenArgs a)
     const int a0 = tile.x, b0 = tile.y;
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
     const int64_t N = a.n;
-    double best[kSub][kSub];
-    uint32_t bstep[kSub][kSub];
+    double best[kSub][kSubB];
+    uint32_t bstep[kSub][kSubB];
 #pragma unroll
     for (int i = 0; i < kSub; ++i) {
         const int ai = a0 + ty * kSub + i;
         const int bound = ai < N ? a.bound[ai] : (int)N;
         const int64_t base = ai < N ? a.base[ai] : 0;
 #pragma unroll
-        for (int j = 0; j < kSub; ++j) {
+        for (int j = 0; j < kSubB; ++j) {
             const int bj = b0 + tx + 16 * j;
             best[i][j] = DBL_MAX;
             bstep[i][j] = 0xFFFFFFFFu;
@@ -101,13 +103,13 @@ __global__ void __launch_bounds__(256) screen_kernel(ScreenArgs a)
         __syncthreads();
         const double* buf = sbuf + (ch & 1) * kChunkDoubles;
         for (int k = 0; k < kc; ++k) {
-            const double* row = buf + k * 3 * 2 * kTile; // [axis][a | b][64]
-            double ax[kSub], ay[kSub], az[kSub], bx[kSub], by[kSub], bz[kSub];
+            const double* row = buf + k * 3 * kRow; // [axis][a tile | b tile]
+            double ax[kSub], ay[kSub], az[kSub], bx[kSubB], by[kSubB], bz[kSubB];
 #pragma unroll
             for (int i = 0; i < kSub; i += 2) {
-                const double2 x = *reinterpret_cast<const double2*>(row + 0 * 2 * kTile + ty * kSub + i);
-                const double2 y = *reinterpret_cast<const double2*>(row + 1 * 2 * kTile + ty * kSub + i);
-                const double2 z = *reinterpret_cast<const double2*>(row + 2 * 2 * kTile + ty * kSub + i);
+                const double2 x = *reinterpret_cast<const double2*>(row + 0 * kRow + ty * kSub + i);
+                const double2 y = *reinterpret_cast<const double2*>(row + 1 * kRow + ty * kSub + i);
+                const double2 z = *reinterpret_cast<const double2*>(row + 2 * kRow + ty * kSub + i);
                 ax[i] = x.x;
                 ax[i + 1] = x.y;
                 ay[i] = y.x;
@@ -116,16 +118,16 @@ __global__ void __launch_bounds__(256) screen_kernel(ScreenArgs a)
                 az[i + 1] = z.y;
             }
 #pragma unroll
-            for (int j = 0; j < kSub; ++j) {
-                bx[j] = row[0 * 2 * kTile + kTile + tx + 16 * j];
-                by[j] = row[1 * 2 * kTile + kTile + tx + 16 * j];
-                bz[j] = row[2 * 2 * kTile + kTile + tx + 16 * j];
+            for (int j = 0; j < kSubB; ++j) {
+                bx[j] = row[0 * kRow + kTileA + tx + 16 * j];
+                by[j] = row[1 * kRow + kTileA + tx + 16 * j];
+                bz[j] = row[2 * kRow + kTileA + tx + 16 * j];
             }
             const uint32_t step = (uint32_t)(a.step_offset + k0 + k);
 #pragma unroll
             for (int i = 0; i < kSub; ++i)
 #pragma unroll
-                for (int j = 0; j < kSub; ++j) {
+                for (int j = 0; j < kSubB; ++j) {
                     const double dx = ax[i] - bx[j];
                     const double dy = ay[i] - by[j];
                     const double dz = az[i] - bz[j];
@@ -146,7 +148,7 @@ __global__ void __launch_bounds__(256) screen_kernel(ScreenArgs a)
         const int bound = a.bound[ai];
         const int64_t base = a.base[ai];
 #pragma unroll
-        for (int j = 0; j < kSub; ++j) {
+        for (int j = 0; j < kSubB; ++j) {
             const int bj = b0 + tx + 16 * j;
             if (bj < N && bj >= bound) {
                 a.min_d2[base + bj] = best[i][j];

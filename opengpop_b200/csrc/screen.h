@@ -5,6 +5,15 @@
 
 namespace gpop {
 
+// Screen tile: 64 rows (first objects) x kScreenTileB columns (second objects); each thread holds
+// 4 rows x kScreenSubB columns of pairs.
+#ifndef GPOP_SCREEN_SUBB
+#define GPOP_SCREEN_SUBB 4
+#endif
+constexpr int kScreenSubB = GPOP_SCREEN_SUBB;
+constexpr int kScreenTileA = 64;
+constexpr int kScreenTileB = 16 * kScreenSubB;
+
 struct ScreenArgs {
     int64_t n = 0; // objects
     const double* traj_r = nullptr; // trajectory store positions [step][3][n]
