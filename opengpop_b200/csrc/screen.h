@@ -6,7 +6,8 @@
 namespace gpop {
 
 // Screen tile: 64 rows (first objects) x kScreenTileB columns (second objects); each thread holds
-// 4 rows x kScreenSubB columns of pairs.
+// 4 rows x kScreenSubB columns of pairs. Measured on B200 (20,000 objects, 2,000 against all, 8,640
+// steps): 4 columns 0.207 s, 8 columns 0.224 s (238 registers, 144 KB of staging).
 #ifndef GPOP_SCREEN_SUBB
 #define GPOP_SCREEN_SUBB 4
 #endif
