@@ -121,6 +121,12 @@ int32_t gpop_propagator_steps_done(const gpop_propagator* p);
  * thread, 3 = lanes (*lanes_out = lanes per object, else 1); -1 for invalid arguments. Host
  * arithmetic only, no CUDA call. */
 int32_t gpop_walk_policy(int64_t n, int32_t num_sms, int32_t precision, int32_t* lanes_out);
+/* No counterpart in the reference. Where the walk is two objects per thread: the owner warps of
+ * the split block it launches (8 warps per SM, of which the owners carry the objects and the
+ * others walk the low gravity columns of the owners' objects), 5 to 7 when each SM carries 5 to 7
+ * sets of 64 objects and the degree is above 8; 0 for the plain block. -1 for invalid arguments.
+ * Host arithmetic only. */
+int32_t gpop_split_block(int64_t n, int32_t num_sms, int32_t degree);
 void gpop_propagator_destroy(gpop_propagator* p);
 /* No counterpart in the reference. gpop_propagate_device for callers that may not allocate device
  * memory while running (services that reserve their memory budget at start-up and forbid later

@@ -37,7 +37,7 @@ EXPORTS = (
     "gpop_startup_init", "gpop_startup_correct", "gpop_gj8_predict", "gpop_gj8_correct",
     "gpop_matrix_column", "gpop_gj8_coefficients", "gpop_gravity", "gpop_frame_matrices",
     "gpop_ca_create", "gpop_ca_create_analytic", "gpop_ca_create_external", "gpop_ca_append", "gpop_ca_propagate", "gpop_ca_find", "gpop_ca_pairs", "gpop_ca_num_pairs",
-    "gpop_ca_set_rows", "gpop_ca_pair_range", "gpop_ca_reserve", "gpop_walk_policy", "gpop_ca_trajectory", "gpop_ca_device_seconds", "gpop_ca_destroy",
+    "gpop_ca_set_rows", "gpop_ca_pair_range", "gpop_ca_reserve", "gpop_walk_policy", "gpop_split_block", "gpop_ca_trajectory", "gpop_ca_device_seconds", "gpop_ca_destroy",
 )
 
 
@@ -132,6 +132,7 @@ def load_library(path=LIB_PATH):
         "gpop_ca_set_rows": (i32, [_VP, i64, i64]),
         "gpop_ca_reserve": (i32, [_VP, i32]),
         "gpop_walk_policy": (i32, [i64, i32, i32, C.POINTER(i32)]),
+        "gpop_split_block": (i32, [i64, i32, i32]),
         "gpop_ca_pair_range": (i32, [_VP, C.POINTER(i64), C.POINTER(i64)]),
         "gpop_ca_trajectory": (i32, [_VP] * 4 + [C.POINTER(i32)]),
         "gpop_ca_device_seconds": (i32, [_VP, _VP]),
@@ -155,6 +156,15 @@ def walk_policy(n, num_sms=148, precision=FP64):
     if w < 0:
         raise GpopError(1, "invalid arguments to gpop_walk_policy")
     return w, lanes.value
+
+
+def split_block(n, num_sms=148, degree=70):
+    """Owner warps of the split block two objects per thread take for n objects (0: a plain
+    block; gpop_split_block)."""
+    s = load_library().gpop_split_block(int(n), int(num_sms), int(degree))
+    if s < 0:
+        raise GpopError(1, "invalid arguments to gpop_split_block")
+    return s
 
 
 def as_time(t):

@@ -270,7 +270,7 @@ gpop_status gpop_create(const gpop_config* cfg_in, gpop_ctx** out)
     if (const char* spl = std::getenv("GPOP_STEPS_PER_LAUNCH"))
         ctx->steps_per_launch = std::max(1, atoi(spl));
     if (const char* wm = std::getenv("GPOP_WALK_MODE"))
-        ctx->walk_mode = std::min(4, std::max(0, atoi(wm)));
+        ctx->walk_mode = std::min((int)kWalkTwoPlain, std::max(0, atoi(wm)));
     if (const char* ws = std::getenv("GPOP_TEST_FIRST_WAIT_SPINS"))
         ctx->first_wait_spins = (uint32_t)std::min(1L << 22, std::max(0L, atol(ws)));
     cudaError_t e = cudaSetDevice(cfg.device);
@@ -460,6 +460,13 @@ int32_t gpop_walk_policy(int64_t n, int32_t num_sms, int32_t precision, int32_t*
     if (lanes_out)
         *lanes_out = walk == kWalkLanes ? lanes_per_object(n, num_sms) : 1;
     return walk;
+}
+
+int32_t gpop_split_block(int64_t n, int32_t num_sms, int32_t degree)
+{
+    if (n <= 0 || num_sms <= 0 || degree < 0)
+        return -1;
+    return split_owner_warps(n, num_sms, degree);
 }
 
 void gpop_propagator_destroy(gpop_propagator* p) { delete p; }

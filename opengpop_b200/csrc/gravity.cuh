@@ -355,6 +355,26 @@ __device__ __forceinline__ void column32x2_group(const GravEntry32* const (&e)[C
 // parts of the columns taken kHeadGroup (columns m <= 8) or kTailGroup (m > 8) columns at a time.
 // Every column's sums, their combination and the order of the combinations are those of the
 // one-column walk, so the accelerations are bit-identical to it.
+// Start values of a two-object walk at Earth-fixed (x, y, z): q = R/r, u = q eps, w = q^2 and the
+// eq. 3-18 seeds x/r, y/r (the arithmetic of the walks' own constructors).
+struct WalkStart {
+    double q[2], u[2], w[2], C1[2], S1[2];
+};
+__device__ __forceinline__ void walk_start(double radius, const double (&x)[2], const double (&y)[2],
+    const double (&z)[2], WalkStart& s)
+{
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        const double r = sqrt(x[k] * x[k] + y[k] * y[k] + z[k] * z[k]);
+        const double eps = z[k] / r;
+        s.q[k] = radius / r;
+        s.u[k] = s.q[k] * eps;
+        s.w[k] = s.q[k] * s.q[k];
+        s.C1[k] = x[k] / r;
+        s.S1[k] = y[k] / r;
+    }
+}
+
 template <bool LANE> struct MixedWalk2 {
     static constexpr int K = 2;
     const GravSmem& gs;
@@ -378,6 +398,27 @@ template <bool LANE> struct MixedWalk2 {
             w[k] = q[k] * q[k];
             C1[k] = x[k] / r[k];
             S1[k] = y[k] / r[k];
+            Cm[k] = 1.0;
+            Sm[k] = 0.0;
+            Cp[k] = 0.0;
+            Sp[k] = 0.0;
+            qm[k] = 1.0;
+            G[k] = H[k] = J[k] = KK[k] = 0.0;
+        }
+        uf = make_float2((float)u[0], (float)u[1]);
+        wf = make_float2((float)w[0], (float)w[1]);
+    }
+    __device__ __forceinline__ MixedWalk2(const GravSmem& g, const WalkStart& s)
+        : gs(g)
+        , L(g.L)
+    {
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            q[k] = s.q[k];
+            u[k] = s.u[k];
+            w[k] = s.w[k];
+            C1[k] = s.C1[k];
+            S1[k] = s.S1[k];
             Cm[k] = 1.0;
             Sm[k] = 0.0;
             Cp[k] = 0.0;
@@ -469,6 +510,20 @@ template <bool LANE> struct MixedWalk2 {
                 s[c].h2[k] += (double)f[c].h[k].y;
             }
             combine64(m + c, s[c]);
+        }
+    }
+    // the recursions of combine64 over one column, without its sums (for a walk that starts past it)
+    __device__ __forceinline__ void skip64()
+    {
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            Cp[k] = Cm[k];
+            Sp[k] = Sm[k];
+            const double Cn = C1[k] * Cm[k] - S1[k] * Sm[k];
+            const double Sn = S1[k] * Cm[k] + C1[k] * Sm[k];
+            Cm[k] = Cn;
+            Sm[k] = Sn;
+            qm[k] *= q[k];
         }
     }
     // FP32 state of the columns m > 8 from the FP64 recursions after column 8
@@ -568,18 +623,27 @@ constexpr int kHeadGroup = GPOP_HEAD_GROUP;
 constexpr int kTailGroup = GPOP_TAIL_GROUP;
 
 
+// Eq. 4-13: Earth-fixed acceleration from the totals G, H, J, K of eq. 4-11.
+__device__ __forceinline__ void assemble_itrs(double gm, double x, double y, double z, double r,
+    double G, double H, double J, double KK, double& ax, double& ay, double& az)
+{
+    const double Gk = G + 1.0;
+    const double Lambda = Gk + z * H / r;
+    const double c = -gm / (r * r);
+    ax = c * (Lambda * x / r - J);
+    ay = c * (Lambda * y / r - KK);
+    az = c * (Lambda * z / r - H);
+}
+
+// The mixed two-object walk from column m0 (a multiple of kHeadGroup, <= 8; the recursions
+// already stepped to it) to L: head groups, then the FP32 tail, whose totals are added into the
+// FP64 ones.
 template <bool LANE>
-__device__ __forceinline__ void gravity_itrs_groups(const GravSmem& gs, const double (&x)[2],
-    const double (&y)[2], const double (&z)[2], double (&ax)[2], double (&ay)[2], double (&az)[2])
+__device__ __forceinline__ void walk_groups_from(MixedWalk2<LANE>& W, int m0)
 {
     constexpr int K = 2;
-    double r[K];
-#pragma unroll
-    for (int k = 0; k < K; ++k)
-        r[k] = sqrt(x[k] * x[k] + y[k] * y[k] + z[k] * z[k]);
-    MixedWalk2<LANE> W(gs, r, x, y, z);
-    const int L = gs.L;
-    int m = 0;
+    const int L = W.L;
+    int m = m0;
 #pragma unroll 1
     for (; m + kHeadGroup - 1 <= kMixedSplit; m += kHeadGroup)
         W.template head_group<kHeadGroup>(m);
@@ -610,50 +674,81 @@ __device__ __forceinline__ void gravity_itrs_groups(const GravSmem& gs, const do
         W.J[k] += (double)W.Jf[k];
         W.KK[k] += (double)W.Kf[k];
     }
+}
+
+template <bool LANE>
+__device__ __forceinline__ void gravity_itrs_groups(const GravSmem& gs, const double (&x)[2],
+    const double (&y)[2], const double (&z)[2], double (&ax)[2], double (&ay)[2], double (&az)[2])
+{
+    constexpr int K = 2;
+    double r[K];
 #pragma unroll
-    for (int k = 0; k < K; ++k) { // eq. 4-13
-        const double Gk = W.G[k] + 1.0;
-        const double Lambda = Gk + z[k] * W.H[k] / r[k];
-        const double c = -gs.gm / (r[k] * r[k]);
-        ax[k] = c * (Lambda * x[k] / r[k] - W.J[k]);
-        ay[k] = c * (Lambda * y[k] / r[k] - W.KK[k]);
-        az[k] = c * (Lambda * z[k] / r[k] - W.H[k]);
-    }
+    for (int k = 0; k < K; ++k)
+        r[k] = sqrt(x[k] * x[k] + y[k] * y[k] + z[k] * z[k]);
+    MixedWalk2<LANE> W(gs, r, x, y, z);
+    walk_groups_from(W, 0);
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+        assemble_itrs(gs.gm, x[k], y[k], z[k], r[k], W.G[k], W.H[k], W.J[k], W.KK[k], ax[k], ay[k],
+            az[k]);
 }
 
 // FP64, K objects: columns (0, 1), (2, 3), ... walked side by side, each combined in order as the
 // one-column walk does (bit-identical accelerations).
-template <bool LANE, int K>
-__device__ __forceinline__ void gravity_itrs_pairs64(const GravSmem& gs, const double (&x)[K],
-    const double (&y)[K], const double (&z)[K], double (&ax)[K], double (&ay)[K], double (&az)[K])
-{
-    const int L = gs.L;
+template <bool LANE, int K> struct PairWalk64 {
+    const GravSmem& gs;
+    int L;
     double r[K], q[K], u[K], w[K], C1[K], S1[K], Cm[K], Sm[K], Cp[K], Sp[K], qm[K];
     double G[K], H[K], J[K], KK[K];
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-        r[k] = sqrt(x[k] * x[k] + y[k] * y[k] + z[k] * z[k]);
-        const double eps = z[k] / r[k];
-        q[k] = gs.radius / r[k];
-        u[k] = q[k] * eps;
-        w[k] = q[k] * q[k];
-        C1[k] = x[k] / r[k];
-        S1[k] = y[k] / r[k];
-        Cm[k] = 1.0;
-        Sm[k] = 0.0;
-        Cp[k] = 0.0;
-        Sp[k] = 0.0;
-        qm[k] = 1.0;
-        G[k] = H[k] = J[k] = KK[k] = 0.0;
-    }
-    auto combine = [&](int m, const ColSums64<K>& s) {
-        const double dm = (double)m;
+
+    __device__ __forceinline__ PairWalk64(const GravSmem& g, const double (&x)[K], const double (&y)[K],
+        const double (&z)[K])
+        : gs(g)
+        , L(g.L)
+    {
 #pragma unroll
         for (int k = 0; k < K; ++k) {
-            G[k] += Cm[k] * s.g1[k] + Sm[k] * s.g2[k];
-            J[k] += dm * (Cp[k] * s.j1[k] + Sp[k] * s.j2[k]);
-            KK[k] -= dm * (Sp[k] * s.j1[k] - Cp[k] * s.j2[k]);
-            H[k] += Cp[k] * s.h1[k] + Sp[k] * s.h2[k];
+            r[k] = sqrt(x[k] * x[k] + y[k] * y[k] + z[k] * z[k]);
+            const double eps = z[k] / r[k];
+            q[k] = gs.radius / r[k];
+            u[k] = q[k] * eps;
+            w[k] = q[k] * q[k];
+            C1[k] = x[k] / r[k];
+            S1[k] = y[k] / r[k];
+            Cm[k] = 1.0;
+            Sm[k] = 0.0;
+            Cp[k] = 0.0;
+            Sp[k] = 0.0;
+            qm[k] = 1.0;
+            G[k] = H[k] = J[k] = KK[k] = 0.0;
+        }
+    }
+    __device__ __forceinline__ PairWalk64(const GravSmem& g, const WalkStart& s)
+        : gs(g)
+        , L(g.L)
+    {
+        static_assert(K == 2, "a walk start carries two objects");
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            r[k] = 0.0; // not needed: the caller assembles
+            q[k] = s.q[k];
+            u[k] = s.u[k];
+            w[k] = s.w[k];
+            C1[k] = s.C1[k];
+            S1[k] = s.S1[k];
+            Cm[k] = 1.0;
+            Sm[k] = 0.0;
+            Cp[k] = 0.0;
+            Sp[k] = 0.0;
+            qm[k] = 1.0;
+            G[k] = H[k] = J[k] = KK[k] = 0.0;
+        }
+    }
+    // the cos/sin(m lambda) and q^m recursions over one column
+    __device__ __forceinline__ void step()
+    {
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
             Cp[k] = Cm[k];
             Sp[k] = Sm[k];
             const double Cn = C1[k] * Cm[k] - S1[k] * Sm[k];
@@ -662,44 +757,138 @@ __device__ __forceinline__ void gravity_itrs_pairs64(const GravSmem& gs, const d
             Sm[k] = Sn;
             qm[k] *= q[k];
         }
-    };
-#pragma unroll 1
-    for (int m = 0; m <= L; m += 2) {
-        ColSums64<K> sa, sb;
-        double Qa1[K], Qa2[K], Qb1[K], Qb2[K];
-        sa.zero();
+    }
+    __device__ __forceinline__ void combine(int m, const ColSums64<K>& s)
+    {
+        const double dm = (double)m;
 #pragma unroll
         for (int k = 0; k < K; ++k) {
-            Qa1[k] = qm[k];
-            Qa2[k] = 0.0;
+            G[k] += Cm[k] * s.g1[k] + Sm[k] * s.g2[k];
+            J[k] += dm * (Cp[k] * s.j1[k] + Sp[k] * s.j2[k]);
+            KK[k] -= dm * (Sp[k] * s.j1[k] - Cp[k] * s.j2[k]);
+            H[k] += Cp[k] * s.h1[k] + Sp[k] * s.h2[k];
         }
-        const GravEntry64* ea = col64<LANE>(gs, m, gs.Lt);
-        sa.add(ea, Qa1);
-        if (m < L) {
-            sb.zero();
+        step();
+    }
+    // columns [m0, m1) (m1 <= L + 1), two at a time from m0
+    __device__ __forceinline__ void walk(int m0, int m1)
+    {
+#pragma unroll 1
+        for (int m = m0; m < m1; m += 2) {
+            ColSums64<K> sa, sb;
+            double Qa1[K], Qa2[K], Qb1[K], Qb2[K];
+            sa.zero();
 #pragma unroll
             for (int k = 0; k < K; ++k) {
-                Qb1[k] = qm[k] * q[k];
-                Qb2[k] = 0.0;
+                Qa1[k] = qm[k];
+                Qa2[k] = 0.0;
             }
-            const GravEntry64* eb = col64<LANE>(gs, m + 1, gs.Lt);
-            sb.add(eb, Qb1);
-            column64_pair<K>(ea + 1, eb + 1, L - m - 1, u, w, Qa1, Qa2, sa, Qb1, Qb2, sb);
-            column64<K>(ea, L - m, L - m, u, w, Qa1, Qa2, sa);
-            combine(m, sa);
-            combine(m + 1, sb);
-        } else {
-            combine(m, sa);
+            const GravEntry64* ea = col64<LANE>(gs, m, gs.Lt);
+            sa.add(ea, Qa1);
+            if (m + 1 < m1) {
+                sb.zero();
+#pragma unroll
+                for (int k = 0; k < K; ++k) {
+                    Qb1[k] = qm[k] * q[k];
+                    Qb2[k] = 0.0;
+                }
+                const GravEntry64* eb = col64<LANE>(gs, m + 1, gs.Lt);
+                sb.add(eb, Qb1);
+                column64_pair<K>(ea + 1, eb + 1, L - m - 1, u, w, Qa1, Qa2, sa, Qb1, Qb2, sb);
+                column64<K>(ea, L - m, L - m, u, w, Qa1, Qa2, sa);
+                combine(m, sa);
+                combine(m + 1, sb);
+            } else {
+                column64<K>(ea, 1, L - m, u, w, Qa1, Qa2, sa);
+                combine(m, sa);
+            }
         }
     }
+};
+
+template <bool LANE, int K>
+__device__ __forceinline__ void gravity_itrs_pairs64(const GravSmem& gs, const double (&x)[K],
+    const double (&y)[K], const double (&z)[K], double (&ax)[K], double (&ay)[K], double (&az)[K])
+{
+    PairWalk64<LANE, K> W(gs, x, y, z);
+    W.walk(0, gs.L + 1);
 #pragma unroll
-    for (int k = 0; k < K; ++k) { // eq. 4-13
-        const double Gk = G[k] + 1.0;
-        const double Lambda = Gk + z[k] * H[k] / r[k];
-        const double c = -gs.gm / (r[k] * r[k]);
-        ax[k] = c * (Lambda * x[k] / r[k] - J[k]);
-        ay[k] = c * (Lambda * y[k] / r[k] - KK[k]);
-        az[k] = c * (Lambda * z[k] / r[k] - H[k]);
+    for (int k = 0; k < K; ++k)
+        assemble_itrs(gs.gm, x[k], y[k], z[k], W.r[k], W.G[k], W.H[k], W.J[k], W.KK[k], ax[k], ay[k],
+            az[k]);
+}
+
+// ---- column-split walk of two objects (gj8_split_kernel) ----
+// Each object's columns are walked as two pieces, each summed from zero into its own totals (G, H,
+// J, K of eq. 4-11): the low columns m < kSplitColumn and the columns from kSplitColumn on. The
+// object's totals are low + high, in that order, whichever threads walked the pieces, so every
+// object of a launch takes the same arithmetic. The high piece starts from the cos/sin(m lambda)
+// and q^m recursions stepped over the low columns without their sums. Both need L > 8.
+constexpr int kSplitColumn = 4;
+static_assert(kSplitColumn % kHeadGroup == 0 && kSplitColumn <= kMixedSplit,
+    "the split falls between head groups");
+
+struct SplitTotals {
+    double G[2], H[2], J[2], K[2];
+};
+
+template <bool MIXED>
+__device__ __forceinline__ void split_low(const GravSmem& gs, const WalkStart& ws, SplitTotals& t)
+{
+    if constexpr (MIXED) {
+        MixedWalk2<false> W(gs, ws);
+#pragma unroll 1
+        for (int m = 0; m < kSplitColumn; m += kHeadGroup)
+            W.template head_group<kHeadGroup>(m);
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            t.G[k] = W.G[k];
+            t.H[k] = W.H[k];
+            t.J[k] = W.J[k];
+            t.K[k] = W.KK[k];
+        }
+    } else {
+        PairWalk64<false, 2> W(gs, ws);
+        W.walk(0, kSplitColumn);
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            t.G[k] = W.G[k];
+            t.H[k] = W.H[k];
+            t.J[k] = W.J[k];
+            t.K[k] = W.KK[k];
+        }
+    }
+}
+
+template <bool MIXED>
+__device__ __forceinline__ void split_high(const GravSmem& gs, const WalkStart& ws, SplitTotals& t)
+{
+    if constexpr (MIXED) {
+        MixedWalk2<false> W(gs, ws);
+#pragma unroll
+        for (int m = 0; m < kSplitColumn; ++m)
+            W.skip64();
+        walk_groups_from(W, kSplitColumn);
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            t.G[k] = W.G[k];
+            t.H[k] = W.H[k];
+            t.J[k] = W.J[k];
+            t.K[k] = W.KK[k];
+        }
+    } else {
+        PairWalk64<false, 2> W(gs, ws);
+#pragma unroll
+        for (int m = 0; m < kSplitColumn; ++m)
+            W.step();
+        W.walk(kSplitColumn, gs.L + 1);
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            t.G[k] = W.G[k];
+            t.H[k] = W.H[k];
+            t.J[k] = W.J[k];
+            t.K[k] = W.KK[k];
+        }
     }
 }
 

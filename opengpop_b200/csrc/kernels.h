@@ -29,7 +29,9 @@ inline __host__ __device__ size_t stage_offset(const TableSrc& ts)
 
 // Per-object propagation state, SoA: array k (n doubles each) at state + k * n.
 enum StateSlot : int {
-    kR = 0, kV = 3, kSs = 6, kSb = 9, kHist = 12, kRep = 39, kRepA = 63, kStateArrays = 75
+    kR = 0, kV = 3, kSs = 6, kSb = 9, kHist = 12, kRep = 39, kRepA = 63,
+    kX0 = 75, // split block exchange (12 values per object) when it does not fit in shared memory
+    kStateArrays = 87
 };
 
 struct PropArgs {
@@ -55,6 +57,7 @@ struct PropArgs {
     double* out_r = nullptr; // AoS [n][3] written at the end of the range (may be NULL)
     double* out_v = nullptr;
     int64_t obj_lo = 0, obj_hi = -1; // lane kernel: objects [obj_lo, obj_hi) of n (-1: n)
+    int split_owners = 0; // split block (gj8_kernel with SPLIT): owner warps of its 8
 };
 
 struct LaunchShape {
@@ -72,13 +75,18 @@ cudaError_t launch_startup(const TableSrc& ts, const PropArgs& a, int num_sms, c
 // kWalkLanes: P lanes per object split the gravity columns (few objects; P from lanes_per_object).
 // kWalkLanesTwo: two lanes per group of two objects (only when forced; the default walks take
 // kWalkLanes where they would have taken it).
-enum WalkMode : int { kWalkOneObject = 1, kWalkTwoObjects = 2, kWalkLanes = 3, kWalkLanesTwo = 4 };
+// kWalkTwoPlain: two objects per thread in a plain block, never the split block (for comparisons).
+enum WalkMode : int {
+    kWalkOneObject = 1, kWalkTwoObjects = 2, kWalkLanes = 3, kWalkLanesTwo = 4, kWalkTwoPlain = 5
+};
 // Lanes per object (1..32, a power of 2): the most that keep n objects in one wave of blocks of at
 // most 384 threads, one per SM.
 int lanes_per_object(int64_t n, int num_sms);
 // The walk launch_gj8 takes for n objects when none is forced (lanes: a lane-layout table is at
 // hand and the force is the gravity model; fp64_gravity: the FP64 build of it).
 int default_walk(int64_t n, int num_sms, bool lanes, bool fp64_gravity);
+// Owner warps of the split block two objects per thread take for n objects (0: a plain block).
+int split_owner_warps(int64_t n, int num_sms, int L);
 // lane_ts: the lane-layout table of the same precision (NULL: no lane-split walk).
 cudaError_t launch_gj8(const TableSrc& ts, const PropArgs& a, int num_sms, cudaStream_t s,
     int block_override = 0, int walk = 0, const TableSrc* lane_ts = nullptr);

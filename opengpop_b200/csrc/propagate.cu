@@ -19,6 +19,7 @@ namespace gpop {
 template <bool MIXED, bool COMP = false> struct ForceGravity {
     static constexpr bool kTable = true;
     static constexpr bool kMixed = MIXED;
+    static constexpr bool kComp = COMP;
     GravSmem g;
     const double* gen_m;
     const double* prop_m;
@@ -205,31 +206,237 @@ template <class F> constexpr bool stage_corrector()
 }
 
 
-template <class F, int K, bool STAGE>
+// ---- column-split block (gj8_kernel with SPLIT) ----
+// With two objects per thread, a block of 5 to 7 warps loads the four schedulers of an SM
+// unevenly (65,536 objects: 7 warps, spread 2-2-2-1, so the SM takes as long as for 8 warps). The
+// split block has 8 warps: S owner warps carry two objects per thread through the step and walk
+// the high columns of their objects (split_high); warp S + b walks the low columns (split_low) of
+// the objects of owner warps b, b + (8 - S), ... Per evaluation the owners publish each object's
+// Earth-fixed position and walk start values, a barrier, both walks, the low totals are
+// published, a barrier, and the owners add them to their own. The exchange lives in shared memory
+// when it fits beside the table and the corrector state (kSplitSmem), else in the state arrays
+// kX0.. (per object). Every thread of the block takes the same barriers: the loops over steps and
+// evaluations are the same for all threads and none leaves early.
+constexpr int kSplitWarps = 8;
+constexpr int kSplitBlock = 32 * kSplitWarps;
+enum SplitMode : int { kSplitNone = 0, kSplitGlobal = 1, kSplitSmem = 2 };
+// exchanged values per object: x y z | q u w C1 S1 | low totals G H J K
+constexpr int kXchValues = 12;
+constexpr size_t kSplitSmemBytes = (size_t)kXchValues * 2 * kSplitBlock * sizeof(double);
+static_assert(kXchValues == kStateArrays - kX0, "the state carries one exchange array per value");
+
+// Owner thread t of a split launch carries objects t and t + (owner threads in the grid); an idle
+// slot shadows the thread's first object (or object n - 1) and never stores.
+__device__ __forceinline__ void split_objects(int64_t t, int64_t gown, int64_t n, int64_t (&obj)[2],
+    bool (&live)[2])
+{
+    const int64_t shadow = t < n ? t : n - 1;
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        const int64_t o = t + k * gown;
+        live[k] = o < n;
+        obj[k] = live[k] ? o : shadow;
+    }
+}
+
+// Exchange value v of a slot: in shared memory slot k * kSplitBlock + (owner thread of the block),
+// in the state arrays the object itself.
+template <int SPLIT> struct Exchange {
+    double* base;
+    int64_t stride;
+    __device__ __forceinline__ double* at(int v, int64_t slot) const { return base + v * stride + slot; }
+    __device__ __forceinline__ void put(int v, int64_t slot, double x) const
+    {
+        if constexpr (SPLIT == kSplitSmem)
+            *at(v, slot) = x;
+        else
+            __stcg(at(v, slot), x);
+    }
+    __device__ __forceinline__ double get(int v, int64_t slot) const
+    {
+        if constexpr (SPLIT == kSplitSmem)
+            return *at(v, slot);
+        else
+            return __ldcg(at(v, slot));
+    }
+};
+
+// One gravity evaluation of a split block: a8 (owners) = GCRS accelerations at the GCRS positions r.
+template <bool MIXED, int SPLIT>
+__device__ __forceinline__ void split_eval(const GravSmem& g, const double* __restrict__ M,
+    const PropArgs& a, bool owner, const bool (&live)[2], const int64_t (&obj)[2],
+    const double (&r)[2][3], double (&a8)[2][3], double* xsmem)
+{
+    constexpr int K = 2;
+    const int S = a.split_owners;
+    const int64_t n = a.n;
+    const int tau = (int)threadIdx.x; // owner thread of the block (owners only)
+    Exchange<SPLIT> X;
+    if constexpr (SPLIT == kSplitSmem) {
+        X.base = xsmem;
+        X.stride = 2 * kSplitBlock;
+    } else {
+        X.base = a.state + (int64_t)kX0 * n;
+        X.stride = n;
+    }
+    // slot of value k of owner thread t whose object k is ok
+    auto slot = [](int k, int t, int64_t ok) -> int64_t {
+        if constexpr (SPLIT == kSplitSmem)
+            return (int64_t)k * kSplitBlock + t;
+        else
+            return ok;
+    };
+    double m[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i)
+        m[i] = __ldg(M + i);
+    if (owner) {
+        double x[K], y[K], z[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            x[k] = m[0] * r[k][0] + m[1] * r[k][1] + m[2] * r[k][2];
+            y[k] = m[3] * r[k][0] + m[4] * r[k][1] + m[5] * r[k][2];
+            z[k] = m[6] * r[k][0] + m[7] * r[k][1] + m[8] * r[k][2];
+        }
+        WalkStart ws;
+        walk_start(g.radius, x, y, z, ws);
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            if (!live[k])
+                continue;
+            const int64_t sl = slot(k, tau, obj[k]);
+            X.put(0, sl, x[k]);
+            X.put(1, sl, y[k]);
+            X.put(2, sl, z[k]);
+            X.put(3, sl, ws.q[k]);
+            X.put(4, sl, ws.u[k]);
+            X.put(5, sl, ws.w[k]);
+            X.put(6, sl, ws.C1[k]);
+            X.put(7, sl, ws.S1[k]);
+        }
+    }
+    __syncthreads();
+    SplitTotals hi;
+    if (owner) {
+        // the start values are read back rather than held across the barrier; an idle slot walks
+        // the thread's first object again
+        WalkStart ws;
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const int64_t sl = live[k] ? slot(k, tau, obj[k]) : slot(0, tau, obj[0]);
+            ws.q[k] = X.get(3, sl);
+            ws.u[k] = X.get(4, sl);
+            ws.w[k] = X.get(5, sl);
+            ws.C1[k] = X.get(6, sl);
+            ws.S1[k] = X.get(7, sl);
+        }
+        split_high<MIXED>(g, ws, hi);
+    } else {
+        const int64_t gown = (int64_t)gridDim.x * 32 * S;
+        const int lane = (int)(threadIdx.x & 31);
+        const int nb = kSplitWarps - S;
+        for (int w = (int)(threadIdx.x >> 5) - S; w < S; w += nb) {
+            const int t = w * 32 + lane; // the owner thread whose objects this lane walks
+            int64_t o[K];
+            bool lv[K];
+            split_objects((int64_t)blockIdx.x * 32 * S + t, gown, n, o, lv);
+            if (!lv[0])
+                continue; // no object (then the second slot is empty too)
+            WalkStart ws;
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                const int64_t sl = lv[k] ? slot(k, t, o[k]) : slot(0, t, o[0]);
+                ws.q[k] = X.get(3, sl);
+                ws.u[k] = X.get(4, sl);
+                ws.w[k] = X.get(5, sl);
+                ws.C1[k] = X.get(6, sl);
+                ws.S1[k] = X.get(7, sl);
+            }
+            SplitTotals lo;
+            split_low<MIXED>(g, ws, lo);
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                if (!lv[k])
+                    continue;
+                const int64_t sl = slot(k, t, o[k]);
+                X.put(8, sl, lo.G[k]);
+                X.put(9, sl, lo.H[k]);
+                X.put(10, sl, lo.J[k]);
+                X.put(11, sl, lo.K[k]);
+            }
+        }
+    }
+    __syncthreads();
+    // The rotation and the positions are read again rather than held through the walk, and every
+    // thread writes a8 (zero for an idle slot or a walk-only thread), so that no earlier value
+    // lives through the walks.
+#pragma unroll
+    for (int i = 0; i < 9; ++i)
+        m[i] = __ldg(M + i);
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        if (!live[k]) {
+            a8[k][0] = a8[k][1] = a8[k][2] = 0.0;
+            continue;
+        }
+        const int64_t sl = slot(k, tau, obj[k]);
+        const double x = X.get(0, sl), y = X.get(1, sl), z = X.get(2, sl);
+        const double rk = sqrt(x * x + y * y + z * z);
+        double ax, ay, az;
+        assemble_itrs(g.gm, x, y, z, rk, X.get(8, sl) + hi.G[k], X.get(9, sl) + hi.H[k],
+            X.get(10, sl) + hi.J[k], X.get(11, sl) + hi.K[k], ax, ay, az);
+        a8[k][0] = m[0] * ax + m[3] * ay + m[6] * az;
+        a8[k][1] = m[1] * ax + m[4] * ay + m[7] * az;
+        a8[k][2] = m[2] * ax + m[5] * ay + m[8] * az;
+    }
+}
+
+template <class F, int K, bool STAGE, int SPLIT = kSplitNone>
 __global__ void __launch_bounds__(K == 1 ? kOneObjectBlock : 256, 1) gj8_kernel(F f, TableSrc ts, PropArgs a)
 {
     extern __shared__ __align__(128) uint8_t smem[];
     constexpr bool kStage = STAGE && stage_corrector<F>();
+    static_assert(SPLIT == kSplitNone || (K == 2 && F::kTable),
+        "the split block carries two objects per thread");
     double* stage = nullptr;
     if constexpr (F::kTable) {
-        if (!bind_table<F::kMixed>(smem, ts, a.err, f.g))
+        bool ok = bind_table<F::kMixed>(smem, ts, a.err, f.g);
+        if constexpr (SPLIT != kSplitNone)
+            ok = __syncthreads_and(ok); // the block leaves as one: barriers follow
+        if (!ok)
             return;
         stage = reinterpret_cast<double*>(smem + stage_offset(ts)) + threadIdx.x;
     }
     // staged value q (0..4: s1, s2, prev, a7, S) of object k, axis j
     auto slot = [&](int q, int k, int j) { return stage + (size_t)((q * K + k) * 3 + j) * blockDim.x; };
-    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int64_t G = (int64_t)gridDim.x * blockDim.x;
     const int64_t n = a.n;
-    if (g >= n)
-        return;
     int64_t obj[K];
     bool live[K];
+    // split block: owner warps carry objects; the other warps walk low columns and run the step on
+    // a shadow of the block's first objects (never stored), so that no value lives on only for them
+    bool owner = true;
+    double* xsmem = nullptr; // split block: the exchange in shared memory, after the staged state
+    if constexpr (SPLIT != kSplitNone) {
+        if constexpr (SPLIT == kSplitSmem)
+            xsmem = reinterpret_cast<double*>(smem + stage_offset(ts)
+                + (kStage ? (size_t)kStageDoubles * K * 8 * blockDim.x : 0));
+        const int S = a.split_owners;
+        owner = (int)(threadIdx.x >> 5) < S;
+        const int64_t gown = (int64_t)gridDim.x * 32 * S;
+        split_objects((int64_t)blockIdx.x * 32 * S + (owner ? threadIdx.x : 0), gown, n, obj, live);
+        if (!owner)
+            live[0] = live[1] = false;
+    } else {
+        const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+        const int64_t G = (int64_t)gridDim.x * blockDim.x;
+        if (g >= n)
+            return;
 #pragma unroll
-    for (int k = 0; k < K; ++k) {
-        const int64_t o = g + k * G;
-        live[k] = o < n;
-        obj[k] = live[k] ? o : g; // idle slots shadow object g and never store
+        for (int k = 0; k < K; ++k) {
+            const int64_t o = g + k * G;
+            live[k] = o < n;
+            obj[k] = live[k] ? o : g; // idle slots shadow object g and never store
+        }
     }
     double* st = a.state;
     const double h = a.h;
@@ -301,12 +508,21 @@ __global__ void __launch_bounds__(K == 1 ? kOneObjectBlock : 256, 1) gj8_kernel(
                 }
             }
             const int idx = step + 4;
-            f.template prop_k<K>(r, v, idx, a8);
+            if constexpr (SPLIT != kSplitNone)
+                split_eval<F::kMixed, SPLIT>(f.g, f.prop_m + (size_t)idx * 9, a, owner, live, obj, r,
+                    a8, xsmem);
+            else
+                f.template prop_k<K>(r, v, idx, a8);
             // Corrector: the first pass reuses the predictor's evaluation at the unchanged
             // position (bit-identical to the reference's repeated call).
             for (int it = 0; it < a.ncorr; ++it) {
-                if (it > 0)
-                    f.template prop_k<K>(r, v, idx, a8);
+                if (it > 0) {
+                    if constexpr (SPLIT != kSplitNone)
+                        split_eval<F::kMixed, SPLIT>(f.g, f.prop_m + (size_t)idx * 9, a, owner, live,
+                            obj, r, a8, xsmem);
+                    else
+                        f.template prop_k<K>(r, v, idx, a8);
+                }
 #pragma unroll
                 for (int k = 0; k < K; ++k)
 #pragma unroll
@@ -679,10 +895,56 @@ cudaError_t launch_startup(const TableSrc& ts, const PropArgs& a, int num_sms, c
     return cudaGetLastError();
 }
 
+#ifndef GPOP_SPLIT_BLOCK
+#define GPOP_SPLIT_BLOCK 1
+#endif
+
+// Owner warps of a split block for n objects at two per thread and one block per SM: the sets of
+// 64 objects an SM carries, when that is 5 to 7 (a plain block of that many warps leaves one or
+// two schedulers with a warp less); 0 otherwise. The split needs the FP32 tail (L > 8).
+int split_owner_warps(int64_t n, int num_sms, int L)
+{
+    if (!GPOP_SPLIT_BLOCK || L <= kMixedSplit || num_sms <= 0)
+        return 0;
+    const int64_t per_sm = (n + num_sms - 1) / num_sms;
+    const int64_t sets = (per_sm + 63) / 64;
+    return sets >= 5 && sets < kSplitWarps ? (int)sets : 0;
+}
+
 template <class F, int K>
 static cudaError_t launch_gj8_k(F f, const TableSrc& ts, const PropArgs& a, int num_sms,
-    cudaStream_t s, int block_override)
+    cudaStream_t s, int block_override, bool split = true)
 {
+    if constexpr (K == 2 && F::kTable) {
+        if constexpr (!F::kComp) {
+            const int S = block_override > 0 || !split ? 0 : split_owner_warps(a.n, num_sms, ts.L);
+            if (S > 0) {
+                PropArgs b = a;
+                b.split_owners = S;
+                const size_t staged = stage_offset(ts) + (size_t)kStageDoubles * K * 8 * kSplitBlock;
+                const size_t optin = max_smem_optin();
+                cudaError_t e;
+                if (stage_corrector<F>() && staged + kSplitSmemBytes <= optin) {
+                    // mixed at 70x70: table, corrector state and exchange all in shared memory
+                    const size_t bytes = staged + kSplitSmemBytes;
+                    if ((e = set_smem(gj8_kernel<F, K, true, kSplitSmem>, bytes)) != cudaSuccess)
+                        return e;
+                    gj8_kernel<F, K, true, kSplitSmem><<<num_sms, kSplitBlock, bytes, s>>>(f, ts, b);
+                } else if (stage_corrector<F>() && staged <= optin) {
+                    // FP64 at 70x70: the exchange goes through the state arrays (L2)
+                    if ((e = set_smem(gj8_kernel<F, K, true, kSplitGlobal>, staged)) != cudaSuccess)
+                        return e;
+                    gj8_kernel<F, K, true, kSplitGlobal><<<num_sms, kSplitBlock, staged, s>>>(f, ts, b);
+                } else {
+                    const size_t bytes = table_smem_bytes(ts);
+                    if ((e = set_smem(gj8_kernel<F, K, false, kSplitGlobal>, bytes)) != cudaSuccess)
+                        return e;
+                    gj8_kernel<F, K, false, kSplitGlobal><<<num_sms, kSplitBlock, bytes, s>>>(f, ts, b);
+                }
+                return cudaGetLastError();
+            }
+        }
+    }
     const int64_t threads = (a.n + K - 1) / K;
     LaunchShape ls = pick_shape(threads, K == 1 ? kOneObjectBlock : 256, num_sms);
     if (block_override > 0) {
@@ -714,8 +976,8 @@ template <class F>
 static cudaError_t launch_gj8_f(F f, const TableSrc& ts, const PropArgs& a, int num_sms,
     cudaStream_t s, int block_override, int walk)
 {
-    if (walk == kWalkTwoObjects)
-        return launch_gj8_k<F, 2>(f, ts, a, num_sms, s, block_override);
+    if (walk == kWalkTwoObjects || walk == kWalkTwoPlain)
+        return launch_gj8_k<F, 2>(f, ts, a, num_sms, s, block_override, walk == kWalkTwoObjects);
     return launch_gj8_k<F, 1>(f, ts, a, num_sms, s, block_override);
 }
 
@@ -820,7 +1082,7 @@ cudaError_t launch_gj8(const TableSrc& ts, const PropArgs& a, int num_sms, cudaS
         f.gen_m = a.gen_m;
         f.prop_m = a.prop_m;
         return launch_gj8_f(f, ts, a, num_sms, s, block_override,
-            walk == kWalkTwoObjects ? walk : kWalkOneObject);
+            walk == kWalkTwoObjects || walk == kWalkTwoPlain ? walk : kWalkOneObject);
     }
     if ((walk == kWalkLanes || walk == kWalkLanesTwo) && a.kind == 0 && lane_ts) {
         const int K = walk == kWalkLanesTwo ? 2 : 1;

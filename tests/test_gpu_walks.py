@@ -54,3 +54,34 @@ def test_lane_walks_match_oracle(oracle_data):
     for walk in (3, 4):
         rr, vv = _run(walk, 0, r, v, steps)
         assert np.abs(rr - ro).max() < 1e-6 and np.abs(vv - vo).max() < 1e-9
+
+
+@pytest.mark.parametrize("n", [40000, 50000, 65536])
+@pytest.mark.parametrize("precision", [0, 1])
+def test_split_block_agrees_with_plain_block_and_oracle(n, precision, oracle_data):
+    """Two objects per thread at 5 to 7 sets of 64 objects per SM run in the split block (owner
+    warps carry the objects and walk the gravity columns m >= 4, the other warps walk columns
+    0..3 of the owners' objects). The low and high column totals are formed apart and added, so
+    the propagation matches the plain two-object block to rounding, not bit for bit; objects
+    taken across the whole range (first and second slot of a thread, block ends, the last
+    object) match the CPU oracle."""
+    import torch
+    import opengpop_b200 as G
+    from opengpop_b200 import orbits
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    per_sm = -(-n // sms)
+    assert G.split_block(n, sms) == (-(-per_sm // 64) if 4 < -(-per_sm // 64) < 8 else 0)
+    r, v = orbits.mixed_population(n, seed=80 + n % 7)
+    steps = 12
+    ref_r, ref_v = _run(5, precision, r, v, steps)  # plain block
+    rr, vv = _run(2, precision, r, v, steps)  # split block where the sizes call for it
+    assert np.abs(rr - ref_r).max() < 1e-6, np.abs(rr - ref_r).max()
+    assert np.abs(vv - ref_v).max() < 1e-9
+    if precision == 0:
+        gown = sms * 32 * max(G.split_block(n, sms), 1)
+        pick = np.unique(np.clip(np.r_[0, 1, 31, 32, 223, 224, gown - 1, gown, gown + 1,
+                                       n // 3, n // 2, n - 2, n - 1,
+                                       np.linspace(0, n - 1, 24).astype(int)], 0, n - 1))
+        ro, vo = O.propagate(oracle_data, "gravity", START, 30.0, steps, r[pick], v[pick])
+        assert np.abs(rr[pick] - ro).max() < 1e-6, np.abs(rr[pick] - ro).max()
+        assert np.abs(vv[pick] - vo).max() < 1e-9

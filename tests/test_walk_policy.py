@@ -24,6 +24,23 @@ def test_walk_bands():
     assert W(65536, SMS, G.MIXED) == (2, 1) and W(65536, SMS, G.FP64) == (2, 1)
 
 
+def test_split_block_bands():
+    # two objects per thread with 5 to 7 sets of 64 objects per SM take the split block (owner
+    # warps = sets); 8 sets fill the plain block, and degree 8 or less has no FP32 tail to split
+    import opengpop_b200 as G
+    per = lambda k: k * SMS
+    assert G.split_block(per(256), SMS) == 0
+    assert G.split_block(per(256) + 1, SMS) == 5
+    assert G.split_block(per(320), SMS) == 5 and G.split_block(per(320) + 1, SMS) == 6
+    assert G.split_block(per(384), SMS) == 6 and G.split_block(per(384) + 1, SMS) == 7
+    assert G.split_block(65536, SMS) == 7 and G.split_block(per(448), SMS) == 7
+    assert G.split_block(per(448) + 1, SMS) == 0
+    assert G.split_block(65536, SMS, degree=8) == 0 and G.split_block(65536, SMS, degree=9) == 7
+    for args in ((0, SMS, 70), (10, 0, 70), (10, SMS, -1)):
+        with pytest.raises(G.GpopError):
+            G.split_block(*args)
+
+
 def test_lane_blocks_fit_the_register_variant():
     # wherever the default walk takes lanes, one block of at most 384 threads per SM holds them
     import opengpop_b200 as G
