@@ -118,8 +118,8 @@ gpop_status gpop_propagator_step(gpop_propagator* p, int32_t steps, double* traj
 int32_t gpop_propagator_steps_done(const gpop_propagator* p);
 /* No counterpart in the reference. The gravity walk the propagation calls take for n objects on a
  * GPU of num_sms SMs at the given precision: 1 = one object per thread, 2 = two objects per
- * thread, 3 = lanes (*lanes_out = lanes per object, else 1); -1 for invalid arguments. Host
- * arithmetic only, no CUDA call. */
+ * thread, 3 = lanes per object, 4 = lanes per group of two objects (*lanes_out = the lanes for 3
+ * and 4, else 1); -1 for invalid arguments. Host arithmetic only, no CUDA call. */
 int32_t gpop_walk_policy(int64_t n, int32_t num_sms, int32_t precision, int32_t* lanes_out);
 /* No counterpart in the reference. Where the walk is two objects per thread: the owner warps of
  * the split block it launches (8 warps per SM, of which the owners carry the objects and the

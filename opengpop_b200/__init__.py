@@ -146,7 +146,8 @@ def load_library(path=LIB_PATH):
     return lib
 
 
-WALKS = {1: "one object per thread", 2: "two objects per thread", 3: "lanes"}
+WALKS = {1: "one object per thread", 2: "two objects per thread", 3: "lanes",
+         4: "lanes per group of two objects"}
 
 
 def walk_policy(n, num_sms=148, precision=FP64):

@@ -458,7 +458,9 @@ int32_t gpop_walk_policy(int64_t n, int32_t num_sms, int32_t precision, int32_t*
         return -1;
     const int walk = default_walk(n, num_sms, true, precision == GPOP_FP64);
     if (lanes_out)
-        *lanes_out = walk == kWalkLanes ? lanes_per_object(n, num_sms) : 1;
+        *lanes_out = walk == kWalkLanes ? lanes_per_object(n, num_sms)
+            : walk == kWalkLanesTwo     ? lane_pair_lanes(n, num_sms, precision == GPOP_FP64)
+                                        : 1;
     return walk;
 }
 

@@ -73,8 +73,8 @@ size_t max_smem_optin();
 cudaError_t launch_startup(const TableSrc& ts, const PropArgs& a, int num_sms, cudaStream_t s);
 // How many objects a GJ8 thread carries through the gravity triangle walk (0 = by problem size).
 // kWalkLanes: P lanes per object split the gravity columns (few objects; P from lanes_per_object).
-// kWalkLanesTwo: two lanes per group of two objects (only when forced; the default walks take
-// kWalkLanes where they would have taken it).
+// kWalkLanesTwo: P lanes per group of two objects (P from lane_pair_lanes, else 2), the default
+// in the bands lane_pair_lanes names.
 // kWalkTwoPlain: two objects per thread in a plain block, never the split block (for comparisons).
 enum WalkMode : int {
     kWalkOneObject = 1, kWalkTwoObjects = 2, kWalkLanes = 3, kWalkLanesTwo = 4, kWalkTwoPlain = 5
@@ -82,6 +82,9 @@ enum WalkMode : int {
 // Lanes per object (1..32, a power of 2): the most that keep n objects in one wave of blocks of at
 // most 384 threads, one per SM.
 int lanes_per_object(int64_t n, int num_sms);
+// Lanes per group of two objects (a power of 2 up to 32) where the default walk carries two objects
+// per lane group, 0 elsewhere.
+int lane_pair_lanes(int64_t n, int num_sms, bool fp64_gravity);
 // The walk launch_gj8 takes for n objects when none is forced (lanes: a lane-layout table is at
 // hand and the force is the gravity model; fp64_gravity: the FP64 build of it).
 int default_walk(int64_t n, int num_sms, bool lanes, bool fp64_gravity);

@@ -999,6 +999,42 @@ int lanes_per_object(int64_t n, int num_sms)
     return P;
 }
 
+// Two objects per lane group (K = 2) share every table entry a lane loads and give each lane two
+// independent recursions; measured on B200 at 70x70 (LEO objects, M object-steps/s, against the
+// one-object lane walk of lanes_per_object or, above 128 objects per SM, the default then):
+//   FP64   2,048: 25.8 (P 32) / 22.9    4,096: 36.1 (16) / 28.7    6,000: 34.4 (8) / 29.5
+//          8,000: 45.4 (8) / 31.2      9,472: 52.4 (8) / 33.9    12,000: 41.6 (8) / 31.9
+//         14,000: 47.4 (8) / 34.3     16,000: 50.9 (4) / 44.2    18,944: 58.8 (4) / 51.7
+//         20,000: 51.8 (4) / 46.7     22,000: 51.1 (4) / 48.0    24,000: 48.5 (4) / 52.1
+//          1,024: 15.3 (32) / 17.2
+//   mixed  4,096: 41.8 (16) / 37.5     8,000: 53.3 (8) / 44.3     9,472: 61.6 (8) / 50.0
+//         14,000: 59.2 (4) / 55.3     16,000: 66.9 (4) / 62.1    18,944: 77.5 (4) / 73.0
+//          2,048: 25.3 (32) / 28.9     6,000: 40.3 (8) / 42.8    12,000: 50.4 (4) / 50.9
+//         20,000: 63.6 (4) / 68.2
+// FP64 gains from about 10 to 150 objects per SM, with P the most lanes that keep the groups within
+// one and a half waves of 8 warps per SM (the groups past one wave run in a second launch with more
+// lanes). Mixed precision gains only where P lanes fill most of one wave (from 0.7 of it) between
+// 27 and 128 objects per SM.
+int lane_pair_lanes(int64_t n, int num_sms, bool fp64_gravity)
+{
+    const int64_t sms = num_sms;
+    if (n <= 0 || sms <= 0)
+        return 0;
+    int P = 2;
+    if (fp64_gravity) {
+        if (n < sms * 10 || n > sms * 150)
+            return 0;
+        while (P < 32 && n * 2 * P <= sms * 768)
+            P *= 2;
+        return P;
+    }
+    if (n < sms * 27 || n > sms * 128)
+        return 0;
+    while (P < 32 && n * 2 * P <= sms * 512)
+        P *= 2;
+    return n * P >= sms * 358 ? P : 0;
+}
+
 // Default walk (measured on B200 at 70x70, LEO objects, mixed / FP64 M object-steps/s):
 // - up to 128 objects per SM, lanes (P from lanes_per_object, blocks of at most 384 threads):
 //   18,900 objects 74.7 / 49.4 against 65.0 / 47.0 with two lanes per pair of objects; 9,472:
@@ -1012,6 +1048,8 @@ int lanes_per_object(int64_t n, int num_sms)
 // One or two objects per thread when no lane-layout table is at hand.
 int default_walk(int64_t n, int num_sms, bool lanes, bool fp64_gravity)
 {
+    if (lanes && lane_pair_lanes(n, num_sms, fp64_gravity) > 0)
+        return kWalkLanesTwo;
     if (lanes && (n <= (int64_t)num_sms * 128 || (fp64_gravity && 2 * n <= (int64_t)num_sms * kLanesBlockMid)))
         return kWalkLanes;
     if (n >= (int64_t)num_sms * 128)
@@ -1086,7 +1124,21 @@ cudaError_t launch_gj8(const TableSrc& ts, const PropArgs& a, int num_sms, cudaS
     }
     if ((walk == kWalkLanes || walk == kWalkLanesTwo) && a.kind == 0 && lane_ts) {
         const int K = walk == kWalkLanesTwo ? 2 : 1;
-        const int P = walk == kWalkLanesTwo ? 2 : lanes_per_object(a.n, num_sms);
+        if (K == 2) {
+            // the groups of one wave of 8 warps per SM, then the rest with more lanes each
+            const int pp = lane_pair_lanes(a.n, num_sms, !lane_ts->mixed);
+            const int P = pp > 0 ? pp : 2;
+            const int64_t main_objects = std::min<int64_t>(a.n, (int64_t)num_sms * 256 / P * 2);
+            cudaError_t e = launch_lanes_range(*lane_ts, a, 2, P, 0, main_objects, num_sms, s);
+            if (e != cudaSuccess || main_objects >= a.n)
+                return e;
+            const int64_t rest_groups = (a.n - main_objects + 1) / 2;
+            int P2 = 1; // the fewest lanes that give the rest over half a wave of threads (<= 32)
+            while (P2 < 32 && rest_groups * 2 * P2 <= (int64_t)num_sms * 256)
+                P2 *= 2;
+            return launch_lanes_range(*lane_ts, a, 2, P2, main_objects, a.n, num_sms, s);
+        }
+        const int P = lanes_per_object(a.n, num_sms);
         if (K == 1) {
             // A block of 8 warps and a bit leaves three warps on one scheduler of every SM: the
             // objects of 8 warps per SM run in one launch, the rest, with more lanes each, in a

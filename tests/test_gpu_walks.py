@@ -85,3 +85,27 @@ def test_split_block_agrees_with_plain_block_and_oracle(n, precision, oracle_dat
         ro, vo = O.propagate(oracle_data, "gravity", START, 30.0, steps, r[pick], v[pick])
         assert np.abs(rr[pick] - ro).max() < 1e-6, np.abs(rr[pick] - ro).max()
         assert np.abs(vv[pick] - vo).max() < 1e-9
+
+
+@pytest.mark.parametrize("n,precision", [(4096, 0), (20000, 0), (9472, 1), (18944, 1)])
+def test_lane_pair_walk(n, precision, oracle_data):
+    """Lanes per group of two objects, the default walk in its bands: 20,000 FP64 objects run as
+    18,944 in a wave of 8 warps per SM with four lanes per group and the other 1,056 in a second
+    launch with more lanes. The propagation matches the one-object lane walk to rounding, and
+    FP64 objects from both launches match the CPU oracle."""
+    import opengpop_b200 as G
+    from opengpop_b200 import orbits
+    assert G.walk_policy(n, 148, precision)[0] == 4
+    r, v = orbits.mixed_population(n, seed=90 + n % 11)
+    steps = 12
+    ref_r, ref_v = _run(3, precision, r, v, steps)  # lanes per object
+    rr, vv = _run(0, precision, r, v, steps)  # default: lanes per group of two objects
+    tol_r, tol_v = (1e-6, 1e-9) if precision == 0 else (1e-3, 1e-6)
+    assert np.abs(rr - ref_r).max() < tol_r, np.abs(rr - ref_r).max()
+    assert np.abs(vv - ref_v).max() < tol_v
+    if precision == 0:
+        pick = np.unique(np.clip(np.r_[0, 1, 2, 3, n // 2, 18943, 18944, 18945, n - 2, n - 1,
+                                       np.linspace(0, n - 1, 20).astype(int)], 0, n - 1))
+        ro, vo = O.propagate(oracle_data, "gravity", START, 30.0, steps, r[pick], v[pick])
+        assert np.abs(rr[pick] - ro).max() < 1e-6, np.abs(rr[pick] - ro).max()
+        assert np.abs(vv[pick] - vo).max() < 1e-9
