@@ -225,17 +225,18 @@ constexpr int kXchValues = 12;
 constexpr size_t kSplitSmemBytes = (size_t)kXchValues * 2 * kSplitBlock * sizeof(double);
 static_assert(kXchValues == kStateArrays - kX0, "the state carries one exchange array per value");
 
-// Owner thread t of a split launch carries objects t and t + (owner threads in the grid); an idle
-// slot shadows the thread's first object (or object n - 1) and never stores.
-__device__ __forceinline__ void split_objects(int64_t t, int64_t gown, int64_t n, int64_t (&obj)[2],
-    bool (&live)[2])
+// Owner thread t of a split launch over objects [lo, lo + cnt) carries objects lo + t and
+// lo + t + (owner threads in the grid); an idle slot shadows the thread's first object (or the
+// last one) and never stores.
+__device__ __forceinline__ void split_objects(int64_t t, int64_t gown, int64_t lo, int64_t cnt,
+    int64_t (&obj)[2], bool (&live)[2])
 {
-    const int64_t shadow = t < n ? t : n - 1;
+    const int64_t shadow = t < cnt ? t : cnt - 1;
 #pragma unroll
     for (int k = 0; k < 2; ++k) {
         const int64_t o = t + k * gown;
-        live[k] = o < n;
-        obj[k] = live[k] ? o : shadow;
+        live[k] = o < cnt;
+        obj[k] = lo + (live[k] ? o : shadow);
     }
 }
 
@@ -269,7 +270,8 @@ __device__ __forceinline__ void split_eval(const GravSmem& g, const double* __re
 {
     constexpr int K = 2;
     const int S = a.split_owners;
-    const int64_t n = a.n;
+    const int64_t n = a.n; // the state's stride
+    const int64_t cnt = (a.obj_hi < 0 ? n : a.obj_hi) - a.obj_lo; // objects of this launch
     const int tau = (int)threadIdx.x; // owner thread of the block (owners only)
     Exchange<SPLIT> X;
     if constexpr (SPLIT == kSplitSmem) {
@@ -339,7 +341,7 @@ __device__ __forceinline__ void split_eval(const GravSmem& g, const double* __re
             const int t = w * 32 + lane; // the owner thread whose objects this lane walks
             int64_t o[K];
             bool lv[K];
-            split_objects((int64_t)blockIdx.x * 32 * S + t, gown, n, o, lv);
+            split_objects((int64_t)blockIdx.x * 32 * S + t, gown, a.obj_lo, cnt, o, lv);
             if (!lv[0])
                 continue; // no object (then the second slot is empty too)
             WalkStart ws;
@@ -409,7 +411,8 @@ __global__ void __launch_bounds__(K == 1 ? kOneObjectBlock : 256, 1) gj8_kernel(
     }
     // staged value q (0..4: s1, s2, prev, a7, S) of object k, axis j
     auto slot = [&](int q, int k, int j) { return stage + (size_t)((q * K + k) * 3 + j) * blockDim.x; };
-    const int64_t n = a.n;
+    const int64_t n = a.n; // the state's stride; this launch runs objects [lo, lo + cnt)
+    const int64_t lo = a.obj_lo, cnt = (a.obj_hi < 0 ? n : a.obj_hi) - lo;
     int64_t obj[K];
     bool live[K];
     // split block: owner warps carry objects; the other warps walk low columns and run the step on
@@ -423,19 +426,20 @@ __global__ void __launch_bounds__(K == 1 ? kOneObjectBlock : 256, 1) gj8_kernel(
         const int S = a.split_owners;
         owner = (int)(threadIdx.x >> 5) < S;
         const int64_t gown = (int64_t)gridDim.x * 32 * S;
-        split_objects((int64_t)blockIdx.x * 32 * S + (owner ? threadIdx.x : 0), gown, n, obj, live);
+        split_objects((int64_t)blockIdx.x * 32 * S + (owner ? threadIdx.x : 0), gown, lo, cnt, obj,
+            live);
         if (!owner)
             live[0] = live[1] = false;
     } else {
         const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
         const int64_t G = (int64_t)gridDim.x * blockDim.x;
-        if (g >= n)
+        if (g >= cnt)
             return;
 #pragma unroll
         for (int k = 0; k < K; ++k) {
             const int64_t o = g + k * G;
-            live[k] = o < n;
-            obj[k] = live[k] ? o : g; // idle slots shadow object g and never store
+            live[k] = o < cnt;
+            obj[k] = lo + (live[k] ? o : g); // idle slots shadow object lo + g and never store
         }
     }
     double* st = a.state;
@@ -915,9 +919,10 @@ template <class F, int K>
 static cudaError_t launch_gj8_k(F f, const TableSrc& ts, const PropArgs& a, int num_sms,
     cudaStream_t s, int block_override, bool split = true)
 {
+    const int64_t cnt = (a.obj_hi < 0 ? a.n : a.obj_hi) - a.obj_lo; // objects of this launch
     if constexpr (K == 2 && F::kTable) {
         if constexpr (!F::kComp) {
-            const int S = block_override > 0 || !split ? 0 : split_owner_warps(a.n, num_sms, ts.L);
+            const int S = block_override > 0 || !split ? 0 : split_owner_warps(cnt, num_sms, ts.L);
             if (S > 0) {
                 PropArgs b = a;
                 b.split_owners = S;
@@ -945,7 +950,7 @@ static cudaError_t launch_gj8_k(F f, const TableSrc& ts, const PropArgs& a, int 
             }
         }
     }
-    const int64_t threads = (a.n + K - 1) / K;
+    const int64_t threads = (cnt + K - 1) / K;
     LaunchShape ls = pick_shape(threads, K == 1 ? kOneObjectBlock : 256, num_sms);
     if (block_override > 0) {
         ls.block = block_override;
@@ -1110,11 +1115,14 @@ static cudaError_t launch_lanes_range(const TableSrc& lt, const PropArgs& a0, in
 cudaError_t launch_gj8(const TableSrc& ts, const PropArgs& a, int num_sms, cudaStream_t s,
     int block_override, int walk, const TableSrc* lane_ts)
 {
-    if (a.n <= 0 || a.step_end <= a.step_begin)
+    // objects [lo, hi) of the n the state holds
+    const int64_t lo = a.obj_lo, hi = a.obj_hi < 0 ? a.n : a.obj_hi, cnt = hi - lo;
+    if (cnt <= 0 || lo < 0 || hi > a.n || a.step_end <= a.step_begin)
         return cudaSuccess;
+    const bool forced = walk > 0;
     const bool comp = a.kind == 0 && ts.mixed && (a.flags & kFlagMixedCompensated);
     if (walk <= 0)
-        walk = default_walk(a.n, num_sms, lane_ts && a.kind == 0 && !comp, a.kind == 0 && !ts.mixed);
+        walk = default_walk(cnt, num_sms, lane_ts && a.kind == 0 && !comp, a.kind == 0 && !ts.mixed);
     if (comp) { // compensated sums: the plain walks only
         ForceGravity<true, true> f {};
         f.gen_m = a.gen_m;
@@ -1122,38 +1130,53 @@ cudaError_t launch_gj8(const TableSrc& ts, const PropArgs& a, int num_sms, cudaS
         return launch_gj8_f(f, ts, a, num_sms, s, block_override,
             walk == kWalkTwoObjects || walk == kWalkTwoPlain ? walk : kWalkOneObject);
     }
+    if (walk == kWalkTwoObjects && a.kind == 0 && block_override <= 0) {
+        // More objects than one wave of 8 warps per SM holds at two per thread: whole waves of
+        // 256-thread blocks, then the rest with the walk its own size takes (100,000 objects ran as
+        // two waves of 169-thread blocks, 6 warps per SM spread 2-2-1-1).
+        const int64_t wave = (int64_t)num_sms * 512;
+        if (cnt > wave) {
+            const int64_t full = cnt / wave * wave;
+            PropArgs b = a;
+            b.obj_hi = lo + full;
+            cudaError_t e = launch_gj8(ts, b, num_sms, s, block_override, kWalkTwoPlain, lane_ts);
+            if (e != cudaSuccess || full == cnt)
+                return e;
+            PropArgs c = a;
+            c.obj_lo = lo + full;
+            return launch_gj8(ts, c, num_sms, s, block_override, forced ? walk : 0, lane_ts);
+        }
+    }
     if ((walk == kWalkLanes || walk == kWalkLanesTwo) && a.kind == 0 && lane_ts) {
         const int K = walk == kWalkLanesTwo ? 2 : 1;
         if (K == 2) {
             // the groups of one wave of 8 warps per SM, then the rest with more lanes each
-            const int pp = lane_pair_lanes(a.n, num_sms, !lane_ts->mixed);
+            const int pp = lane_pair_lanes(cnt, num_sms, !lane_ts->mixed);
             const int P = pp > 0 ? pp : 2;
-            const int64_t main_objects = std::min<int64_t>(a.n, (int64_t)num_sms * 256 / P * 2);
-            cudaError_t e = launch_lanes_range(*lane_ts, a, 2, P, 0, main_objects, num_sms, s);
-            if (e != cudaSuccess || main_objects >= a.n)
+            const int64_t main_objects = std::min<int64_t>(cnt, (int64_t)num_sms * 256 / P * 2);
+            cudaError_t e = launch_lanes_range(*lane_ts, a, 2, P, lo, lo + main_objects, num_sms, s);
+            if (e != cudaSuccess || main_objects >= cnt)
                 return e;
-            const int64_t rest_groups = (a.n - main_objects + 1) / 2;
+            const int64_t rest_groups = (cnt - main_objects + 1) / 2;
             int P2 = 1; // the fewest lanes that give the rest over half a wave of threads (<= 32)
             while (P2 < 32 && rest_groups * 2 * P2 <= (int64_t)num_sms * 256)
                 P2 *= 2;
-            return launch_lanes_range(*lane_ts, a, 2, P2, main_objects, a.n, num_sms, s);
+            return launch_lanes_range(*lane_ts, a, 2, P2, lo + main_objects, hi, num_sms, s);
         }
-        const int P = lanes_per_object(a.n, num_sms);
-        if (K == 1) {
-            // A block of 8 warps and a bit leaves three warps on one scheduler of every SM: the
-            // objects of 8 warps per SM run in one launch, the rest, with more lanes each, in a
-            // second one (20,000 objects, FP64: 4.69e7 object-steps/s against 4.38e7 in one).
-            const int64_t per_sm = ((a.n * P + num_sms - 1) / num_sms + P - 1) / P * P;
-            const int64_t main_objects = (int64_t)num_sms * 256 / P;
-            if (per_sm > 256 && per_sm <= 288 && main_objects < a.n) {
-                cudaError_t e = launch_lanes_range(*lane_ts, a, 1, P, 0, main_objects, num_sms, s);
-                if (e != cudaSuccess)
-                    return e;
-                const int P2 = lanes_per_object(a.n - main_objects, num_sms);
-                return launch_lanes_range(*lane_ts, a, 1, P2, main_objects, a.n, num_sms, s);
-            }
+        const int P = lanes_per_object(cnt, num_sms);
+        // A block of 8 warps and a bit leaves three warps on one scheduler of every SM: the
+        // objects of 8 warps per SM run in one launch, the rest, with more lanes each, in a second
+        // one (20,000 objects, FP64: 4.69e7 object-steps/s against 4.38e7 in one).
+        const int64_t per_sm = ((cnt * P + num_sms - 1) / num_sms + P - 1) / P * P;
+        const int64_t main_objects = (int64_t)num_sms * 256 / P;
+        if (per_sm > 256 && per_sm <= 288 && main_objects < cnt) {
+            cudaError_t e = launch_lanes_range(*lane_ts, a, 1, P, lo, lo + main_objects, num_sms, s);
+            if (e != cudaSuccess)
+                return e;
+            const int P2 = lanes_per_object(cnt - main_objects, num_sms);
+            return launch_lanes_range(*lane_ts, a, 1, P2, lo + main_objects, hi, num_sms, s);
         }
-        return launch_lanes_range(*lane_ts, a, K, P, 0, a.n, num_sms, s);
+        return launch_lanes_range(*lane_ts, a, K, P, lo, hi, num_sms, s);
     }
     if (walk == kWalkLanes || walk == kWalkLanesTwo)
         walk = kWalkOneObject;

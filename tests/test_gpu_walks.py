@@ -109,3 +109,30 @@ def test_lane_pair_walk(n, precision, oracle_data):
         ro, vo = O.propagate(oracle_data, "gravity", START, 30.0, steps, r[pick], v[pick])
         assert np.abs(rr[pick] - ro).max() < 1e-6, np.abs(rr[pick] - ro).max()
         assert np.abs(vv[pick] - vo).max() < 1e-9
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_more_objects_than_one_wave(precision, oracle_data):
+    """100,000 objects: one wave of 8 warps per SM at two objects per thread (75,776 objects on 148
+    SMs), then the other 24,224 with the walk their own number takes (FP64: two lanes per object;
+    mixed: two objects per thread). Matches the plain two-object block over all objects to
+    rounding, and FP64 objects on both sides of the boundary match the CPU oracle."""
+    import torch
+    from opengpop_b200 import orbits
+    n = 100000
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    r, v = orbits.mixed_population(n, seed=97)
+    steps = 12
+    ref_r, ref_v = _run(5, precision, r, v, steps)  # plain block over all objects
+    rr, vv = _run(0, precision, r, v, steps)
+    tol_r, tol_v = (1e-6, 1e-9) if precision == 0 else (1e-3, 1e-6)
+    assert np.abs(rr - ref_r).max() < tol_r, np.abs(rr - ref_r).max()
+    assert np.abs(vv - ref_v).max() < tol_v
+    if precision == 0:
+        wave = sms * 512
+        pick = np.unique(np.clip(np.r_[0, 1, wave // 2, wave - 2, wave - 1, wave, wave + 1,
+                                       n - 2, n - 1, np.linspace(0, n - 1, 16).astype(int)],
+                                 0, n - 1))
+        ro, vo = O.propagate(oracle_data, "gravity", START, 30.0, steps, r[pick], v[pick])
+        assert np.abs(rr[pick] - ro).max() < 1e-6, np.abs(rr[pick] - ro).max()
+        assert np.abs(vv[pick] - vo).max() < 1e-9
