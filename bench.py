@@ -54,9 +54,10 @@ def fp32_flops_per_object_step(L=DEGREE):
     return 7 * 24 * (terms(L) - terms(8))
 
 
-# DRAM bytes (read + write) of one mixed GJ8 launch over 65,536 objects, from an ncu capture
-# (dram__bytes_read.sum 20.6 MB, dram__bytes_write.sum 0).
-MIXED_GJ8_DRAM_BYTES = 20.6e6
+# DRAM bytes (read + write) of one mixed GJ8 launch over 65,536 objects (the split block), from an
+# ncu capture (dram__bytes_read.sum 20.66 MB, dram__bytes_write.sum 0;
+# profiles/gj8_kernels_65536obj_70x70.md).
+MIXED_GJ8_DRAM_BYTES = 20.66e6
 
 
 def env_int(k, d):

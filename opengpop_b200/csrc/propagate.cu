@@ -592,13 +592,22 @@ __global__ void __launch_bounds__(K == 1 ? kOneObjectBlock : 256, 1) gj8_kernel(
 // of group g is g + k * (groups in the grid). Used when the objects alone leave most warp slots of
 // the GPU empty. MAXT bounds the block (and so the registers a thread may hold): 512 for the many
 // lanes of few objects, 384 for two lanes per object, which then keeps its table loads in flight.
-template <bool MIXED, int K, int MAXT = (K == 1 ? 512 : 256)>
+// STAGE: the corrector's constants of a step (s1, s2, prev, a7, S) wait in shared memory during
+// the gravity walks, one copy per lane group written by its lead lane, as in gj8_kernel (two
+// objects per lane group, FP64, 18,944 objects at four lanes: the walk at 254 registers waited on
+// its table loads, short_scoreboard 1.43 per issued instruction, FP64 pipe 59 % busy).
+template <bool MIXED, int K, int MAXT = (K == 1 ? 512 : 256), bool STAGE = false>
 __global__ void __launch_bounds__(MAXT, 1) gj8_lanes_kernel(TableSrc ts, PropArgs a, int P)
 {
     extern __shared__ __align__(128) uint8_t smem[];
     GravSmem g;
     if (!bind_lane_table(smem, ts, a.err, g))
         return;
+    double* stage = nullptr;
+    if constexpr (STAGE)
+        stage = reinterpret_cast<double*>(smem + stage_offset(ts)) + threadIdx.x / P;
+    // staged value q (0..4: s1, s2, prev, a7, S) of object k, axis j, of this lane's group
+    auto slot = [&](int q, int k, int j) { return stage + (size_t)((q * K + k) * 3 + j) * (blockDim.x / P); };
     const int64_t grp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / P;
     const int64_t groups = ((int64_t)gridDim.x * blockDim.x) / P;
     const int lane = (int)(threadIdx.x & 31);
@@ -675,8 +684,19 @@ __global__ void __launch_bounds__(MAXT, 1) gj8_lanes_kernel(TableSrc ts, PropArg
                     s2[k][j] = c2;
                     prev[k][j] = s[k][j];
                     a7[k][j] = hist[8][j];
+                    if constexpr (STAGE) {
+                        if (lead) {
+                            st_stage(slot(0, k, j), s1[k][j]);
+                            st_stage(slot(1, k, j), s2[k][j]);
+                            st_stage(slot(2, k, j), prev[k][j]);
+                            st_stage(slot(3, k, j), a7[k][j]);
+                            st_stage(slot(4, k, j), S[k][j]);
+                        }
+                    }
                 }
             }
+            if constexpr (STAGE)
+                __syncwarp(mask); // the lead's stores precede the group's loads
             const double* M = a.prop_m + (size_t)(step + 4) * 9;
             for (int it = 0; it < a.ncorr; ++it) {
                 gravity_gcrs_lk<MIXED, K>(g, l, P, M, r, a8, mask);
@@ -684,6 +704,13 @@ __global__ void __launch_bounds__(MAXT, 1) gj8_lanes_kernel(TableSrc ts, PropArg
                 for (int k = 0; k < K; ++k)
 #pragma unroll
                     for (int j = 0; j < 3; ++j) {
+                        if constexpr (STAGE) {
+                            s1[k][j] = ld_stage(slot(0, k, j));
+                            s2[k][j] = ld_stage(slot(1, k, j));
+                            prev[k][j] = ld_stage(slot(2, k, j));
+                            a7[k][j] = ld_stage(slot(3, k, j));
+                            S[k][j] = ld_stage(slot(4, k, j));
+                        }
                         s[k][j] = prev[k][j] + (a8[k][j] + a7[k][j]) / 2;
                         v[k][j] = h * (s1[k][j] + a8[k][j] * c_SA[8][8] + s[k][j]);
                         r[k][j] = h * h * (s2[k][j] + a8[k][j] * c_GJ[8][8] + S[k][j]);
@@ -1005,39 +1032,33 @@ int lanes_per_object(int64_t n, int num_sms)
 }
 
 // Two objects per lane group (K = 2) share every table entry a lane loads and give each lane two
-// independent recursions; measured on B200 at 70x70 (LEO objects, M object-steps/s, against the
-// one-object lane walk of lanes_per_object or, above 128 objects per SM, the default then):
-//   FP64   2,048: 25.8 (P 32) / 22.9    4,096: 36.1 (16) / 28.7    6,000: 34.4 (8) / 29.5
-//          8,000: 45.4 (8) / 31.2      9,472: 52.4 (8) / 33.9    12,000: 41.6 (8) / 31.9
-//         14,000: 47.4 (8) / 34.3     16,000: 50.9 (4) / 44.2    18,944: 58.8 (4) / 51.7
-//         20,000: 51.8 (4) / 46.7     22,000: 51.1 (4) / 48.0    24,000: 48.5 (4) / 52.1
-//          1,024: 15.3 (32) / 17.2
-//   mixed  4,096: 41.8 (16) / 37.5     8,000: 53.3 (8) / 44.3     9,472: 61.6 (8) / 50.0
-//         14,000: 59.2 (4) / 55.3     16,000: 66.9 (4) / 62.1    18,944: 77.5 (4) / 73.0
-//          2,048: 25.3 (32) / 28.9     6,000: 40.3 (8) / 42.8    12,000: 50.4 (4) / 50.9
-//         20,000: 63.6 (4) / 68.2
-// FP64 gains from about 10 to 150 objects per SM, with P the most lanes that keep the groups within
-// one and a half waves of 8 warps per SM (the groups past one wave run in a second launch with more
-// lanes). Mixed precision gains only where P lanes fill most of one wave (from 0.7 of it) between
-// 27 and 128 objects per SM.
+// independent recursions. Measured on B200 at 70x70 (LEO objects, M object-steps/s, the corrector
+// constants staged per group), lanes per group in brackets, against the walk taken before (one
+// object per lane group; in mixed precision above 128 objects per SM two objects per thread):
+//   FP64   1,200: 15.6 (32) / 11.4     4,096: 38.4 (16) / 28.7    9,472: 53.4 (8) / 33.9
+//         14,000: 48.7 (8) / 34.3     18,944: 60.1 (4) / 51.7    20,000: 53.3 (4) / 46.7
+//         22,000: 52.6 (4) / 48.0     outside: 1,024: 17.0 (32) / 17.4; 24,000: 50.6 (8) / 52.0
+//   mixed  3,000: 35.7 (16) / 33.8     4,096: 47.9 (16) / 37.5    6,000: 47.7 (8) / 42.9
+//          8,000: 62.4 (8) / 44.3      9,472: 69.5 (8) / 50.0    12,000: 59.4 (4) / 50.9
+//         18,944: 88.3 (4) / 73.0     20,000: 73.5 (4) / 68.4
+//                                     outside: 2,048: 29.5 (16) / 29.0; 24,000: 76.0 (2) / 81.8
+// P is the most lanes whose groups fit one wave of 8 warps per SM, doubled once, up to 8 lanes,
+// when the groups still fit one and a half waves (FP64) or 1.2 waves (mixed); the groups past one
+// wave run in a second launch with more lanes. Before the staging, FP64 12,000 objects ran at 41.6
+// with 8 lanes against 38.7 with 4, and 6,000 at 34.4 with 8 against 31.4 with 16; staged, mixed
+// 12,000 runs at 59.4 with 4 against 54.9 with 8.
 int lane_pair_lanes(int64_t n, int num_sms, bool fp64_gravity)
 {
     const int64_t sms = num_sms;
-    if (n <= 0 || sms <= 0)
+    if (n <= 0 || sms <= 0 || n < sms * (fp64_gravity ? 8 : 16) || n > sms * 150)
         return 0;
+    const int64_t wave = sms * 512; // objects of one wave of 8 warps per SM at one lane per group
     int P = 2;
-    if (fp64_gravity) {
-        if (n < sms * 10 || n > sms * 150)
-            return 0;
-        while (P < 32 && n * 2 * P <= sms * 768)
-            P *= 2;
-        return P;
-    }
-    if (n < sms * 27 || n > sms * 128)
-        return 0;
-    while (P < 32 && n * 2 * P <= sms * 512)
+    while (P < 32 && n * 2 * P <= wave)
         P *= 2;
-    return n * P >= sms * 358 ? P : 0;
+    if (2 * P <= 8 && n * 2 * P * 10 <= wave * (fp64_gravity ? 15 : 12))
+        P *= 2;
+    return P;
 }
 
 // Default walk (measured on B200 at 70x70, LEO objects, mixed / FP64 M object-steps/s):
@@ -1079,6 +1100,13 @@ static cudaError_t launch_lanes_range(const TableSrc& lt, const PropArgs& a0, in
     const int block = (int)std::min<int64_t>(cap, std::max<int64_t>(32, ((per_sm + P - 1) / P) * P));
     const unsigned grid = (unsigned)((threads + block - 1) / block);
     const size_t smem = table_smem_bytes(lt);
+    // two objects per lane group: the corrector's constants parked in shared memory, one copy per
+    // group (gj8_lanes_kernel STAGE), when they fit beside the table
+#ifndef GPOP_STAGE_LANES
+#define GPOP_STAGE_LANES 1
+#endif
+    const size_t staged = GPOP_STAGE_LANES ? stage_offset(lt) + (size_t)kStageDoubles * K * 8 * (block / P)
+                                           : (size_t)1 << 40;
     cudaError_t e;
     if (lt.mixed) {
         if (K == 1 && block <= kLanesBlockMid) {
@@ -1090,9 +1118,15 @@ static cudaError_t launch_lanes_range(const TableSrc& lt, const PropArgs& a0, in
                 return e;
             gj8_lanes_kernel<true, 1><<<grid, block, smem, s>>>(lt, a, P);
         } else {
-            if ((e = set_smem(gj8_lanes_kernel<true, 2>, smem)) != cudaSuccess)
-                return e;
-            gj8_lanes_kernel<true, 2><<<grid, block, smem, s>>>(lt, a, P);
+            if (staged <= max_smem_optin()) {
+                if ((e = set_smem(gj8_lanes_kernel<true, 2, 256, true>, staged)) != cudaSuccess)
+                    return e;
+                gj8_lanes_kernel<true, 2, 256, true><<<grid, block, staged, s>>>(lt, a, P);
+            } else {
+                if ((e = set_smem(gj8_lanes_kernel<true, 2>, smem)) != cudaSuccess)
+                    return e;
+                gj8_lanes_kernel<true, 2><<<grid, block, smem, s>>>(lt, a, P);
+            }
         }
     } else {
         if (K == 1 && block <= kLanesBlockMid) {
@@ -1104,9 +1138,15 @@ static cudaError_t launch_lanes_range(const TableSrc& lt, const PropArgs& a0, in
                 return e;
             gj8_lanes_kernel<false, 1><<<grid, block, smem, s>>>(lt, a, P);
         } else {
-            if ((e = set_smem(gj8_lanes_kernel<false, 2>, smem)) != cudaSuccess)
-                return e;
-            gj8_lanes_kernel<false, 2><<<grid, block, smem, s>>>(lt, a, P);
+            if (staged <= max_smem_optin()) {
+                if ((e = set_smem(gj8_lanes_kernel<false, 2, 256, true>, staged)) != cudaSuccess)
+                    return e;
+                gj8_lanes_kernel<false, 2, 256, true><<<grid, block, staged, s>>>(lt, a, P);
+            } else {
+                if ((e = set_smem(gj8_lanes_kernel<false, 2>, smem)) != cudaSuccess)
+                    return e;
+                gj8_lanes_kernel<false, 2><<<grid, block, smem, s>>>(lt, a, P);
+            }
         }
     }
     return cudaGetLastError();

@@ -1,10 +1,10 @@
 """The default gravity walk by problem size (gpop_walk_policy, the function the propagation
 launches follow), checked at the boundaries of its bands on a 148-SM B200: lanes up to 128
 objects per SM (lanes per object chosen so a block has at most 384 threads), lanes per group of
-two objects where they gain (FP64 from 10 to 150 objects per SM; mixed precision between 27 and
-128 where the lanes fill most of a wave), FP64 two lanes per object up to 192 per SM, then FP64
-one object per thread up to 256 per SM, and two objects per thread above (mixed precision from 128
-per SM). Host arithmetic only: runs without a GPU."""
+two objects where they gain (FP64 from 8 to 150 objects per SM, mixed precision from 16 to 150),
+FP64 two lanes per object up to 192 per SM, then FP64 one object per thread up to 256 per SM, and
+two objects per thread above (mixed precision from 150 per SM). Host arithmetic only: runs
+without a GPU."""
 import pytest
 
 SMS = 148
@@ -17,9 +17,8 @@ def test_walk_bands():
     for prec in (G.FP64, G.MIXED):
         assert W(1, SMS, prec) == (3, 32)
         assert W(per(128), SMS, prec) == (4, 4)
-    assert W(per(128) + 1, SMS, G.MIXED) == (2, 1)
-    assert W(per(128) + 1, SMS, G.FP64) == (4, 4)
-    assert W(per(150), SMS, G.FP64) == (4, 4)
+        assert W(per(150), SMS, prec) == (4, 4)
+    assert W(per(150) + 1, SMS, G.MIXED) == (2, 1)
     assert W(per(150) + 1, SMS, G.FP64) == (3, 2)
     assert W(per(192), SMS, G.FP64) == (3, 2)
     assert W(per(192) + 1, SMS, G.FP64) == (1, 1)
@@ -29,19 +28,19 @@ def test_walk_bands():
 
 
 def test_lane_pair_bands():
-    # two objects per lane group: FP64 with the most lanes whose groups fit one and a half waves
-    # of 8 warps per SM; mixed precision with the most lanes that fit one wave, where they fill at
-    # least 0.7 of it
+    # two objects per lane group: the most lanes whose groups fit one wave of 8 warps per SM,
+    # doubled once up to 8 lanes when the groups still fit 1.5 waves (FP64) or 1.2 waves (mixed)
     import opengpop_b200 as G
     W = G.walk_policy
     per = lambda k: k * SMS
-    assert W(per(10) - 1, SMS, G.FP64)[0] == 3 and W(per(10), SMS, G.FP64) == (4, 32)
-    assert W(4096, SMS, G.FP64) == (4, 16) and W(6000, SMS, G.FP64) == (4, 16)
-    assert W(9472, SMS, G.FP64) == (4, 8) and W(14000, SMS, G.FP64) == (4, 8)
-    assert W(16000, SMS, G.FP64) == (4, 4) and W(20000, SMS, G.FP64) == (4, 4)
-    assert W(per(27) - 1, SMS, G.MIXED)[0] == 3 and W(per(27), SMS, G.MIXED) == (4, 16)
-    assert W(6000, SMS, G.MIXED)[0] == 3 and W(12000, SMS, G.MIXED)[0] == 3
-    assert W(9472, SMS, G.MIXED) == (4, 8) and W(14000, SMS, G.MIXED) == (4, 4)
+    assert W(per(8) - 1, SMS, G.FP64)[0] == 3 and W(per(8), SMS, G.FP64) == (4, 32)
+    assert W(4096, SMS, G.FP64) == (4, 16) and W(6000, SMS, G.FP64) == (4, 8)
+    assert W(9472, SMS, G.FP64) == (4, 8) and W(12000, SMS, G.FP64) == (4, 8)
+    assert W(14000, SMS, G.FP64) == (4, 8) and W(16000, SMS, G.FP64) == (4, 4)
+    assert W(20000, SMS, G.FP64) == (4, 4) and W(22000, SMS, G.FP64) == (4, 4)
+    assert W(per(16) - 1, SMS, G.MIXED)[0] == 3 and W(per(16), SMS, G.MIXED) == (4, 32)
+    assert W(6000, SMS, G.MIXED) == (4, 8) and W(12000, SMS, G.MIXED) == (4, 4)
+    assert W(9472, SMS, G.MIXED) == (4, 8) and W(20000, SMS, G.MIXED) == (4, 4)
     for prec in (G.FP64, G.MIXED):
         for n in range(1, per(200), 37):
             w, P = W(n, SMS, prec)
