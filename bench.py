@@ -539,7 +539,8 @@ def run_adjoint(args, torch, G, dev):
 
 def accuracy_7d(G, n_sample):
     """Mixed vs FP64 position error after 7 days (20,160 steps) on n_sample objects spread over
-    the population."""
+    the population, propagated together (at the default, the whole population: the kernels and
+    launch shapes of the headline)."""
     from opengpop_b200 import orbits
     r, v = orbits.mixed_population(N_OBJECTS, SEED)
     idx = np.linspace(0, N_OBJECTS - 1, n_sample).astype(int)
@@ -711,7 +712,7 @@ def main():
     ap.add_argument("--adjoint-pairs", type=int, default=10000)
     ap.add_argument("--adjoint-steps", type=int, default=2880)
     ap.add_argument("--stm-objects", type=int, default=8192)
-    ap.add_argument("--accuracy-objects", type=int, default=8192,
+    ap.add_argument("--accuracy-objects", type=int, default=N_OBJECTS,
                     help="objects of the 7-day mixed-vs-FP64 error sample (0 = skip)")
     ap.add_argument("--no-screen", action="store_true",
                     help="headline: skip the closest-approach job (conj pairs/s)")

@@ -2,7 +2,8 @@
 
 - The 65,536-object mixed population over 7 days (30 s steps, 20,160 steps, 70x70), on 64 objects
   spread over LEO, MEO and GEO, against the FP64 CPU oracle: the FP64 build within 1 cm, the
-  mixed-precision build (two-level and compensated FP32 sums) within 1 m.
+  mixed-precision build (two-level and compensated FP32 sums) within 1 m; both propagated alone
+  and inside the whole 65,536-object propagation.
 - The 1,024-object configuration in full (20x20, 60 s, 24 h) against the oracle: within 1 cm.
 - The closest-approach configuration (20,000 LEO objects, 2,000 seed-chosen objects against all,
   3 days, 5 km) screened by the CUDA path, against the oracle's screen of the very same GPU
@@ -51,6 +52,27 @@ def test_seven_days_against_oracle(week, precision, flags, bound_m):
           "%.3e m/s" % ({0: "FP64", 1: "mixed"}[precision] + (", compensated" if flags else ""),
                         err.max(), int(err.argmax()), np.median(err), verr.max()))
     assert err.max() <= bound_m
+
+
+@pytest.mark.parametrize("precision,bound_m", [(0, 1e-2), (1, 1.0)], ids=["fp64", "mixed"])
+def test_seven_days_all_objects_against_oracle(week, precision, bound_m):
+    """The configuration itself: all 65,536 objects propagated together for 7 days (the split
+    block: 7 owner warps per SM and one walking the low gravity columns), the same 64 objects
+    against the oracle."""
+    import opengpop_b200 as G
+    from opengpop_b200 import orbits
+    r0, v0, ro, vo = week
+    r, v = orbits.mixed_population(65536, SEED)
+    idx = np.linspace(0, 65535, 64).astype(int)
+    assert np.array_equal(r[idx], r0)
+    assert G.split_block(65536) == 7
+    ctx = G.Context(precision=precision)
+    rr, vv = ctx.propagate(START, 30.0, 20160, r, v)
+    ctx.close()
+    err = np.linalg.norm(rr[idx] - ro, axis=1)
+    print("\n7 days, all 65,536 objects, %s: position error max %.3e m (object %d), median %.3e m"
+          % ({0: "FP64", 1: "mixed"}[precision], err.max(), int(idx[err.argmax()]), np.median(err)))
+    assert np.isfinite(rr).all() and err.max() <= bound_m
 
 
 def test_thousand_objects_20x20_one_day_against_oracle():
