@@ -586,6 +586,105 @@ __global__ void __launch_bounds__(K == 1 ? kOneObjectBlock : 256, 1) gj8_kernel(
     }
 }
 
+// ---- RK8 startup in the split block (the sizes where the GJ8 steps take it) ----
+// run_startup2 over two objects per owner thread; each of its 145 gravity evaluations per object
+// is one split_eval, so the walk-only warps take the low columns here too. Outputs and the
+// bad-input flag as startup_kernel.
+template <bool MIXED, int SPLIT> struct SplitForce2 {
+    const ForceGravity<MIXED>& f;
+    const PropArgs& a;
+    bool owner;
+    const bool (&live)[2];
+    const int64_t (&obj)[2];
+    double* xsmem;
+    __device__ __forceinline__ void gen2(const double (&r)[2][3], const double (&)[2][3], int step,
+        int k, double (&acc)[2][3]) const
+    {
+        const int st = step > 0 ? step - 1 : step; // ForceModel::ComputeGenerationAcceleration
+        split_eval<MIXED, SPLIT>(f.g, f.gen_m + (size_t)((st + 4) * 10 + k) * 9, a, owner, live, obj,
+            r, acc, xsmem);
+    }
+    __device__ __forceinline__ void prop2(const double (&r)[2][3], const double (&)[2][3], int idx,
+        double (&acc)[2][3]) const
+    {
+        split_eval<MIXED, SPLIT>(f.g, f.prop_m + (size_t)idx * 9, a, owner, live, obj, r, acc, xsmem);
+    }
+};
+
+template <bool MIXED, int SPLIT>
+__global__ void __launch_bounds__(kSplitBlock, 1) startup_split_kernel(ForceGravity<MIXED> f, TableSrc ts,
+    PropArgs a)
+{
+    extern __shared__ __align__(128) uint8_t smem[];
+    bool ok = bind_table<MIXED>(smem, ts, a.err, f.g);
+    ok = __syncthreads_and(ok); // the block leaves as one: barriers follow
+    if (!ok)
+        return;
+    double* xsmem = SPLIT == kSplitSmem ? reinterpret_cast<double*>(smem + stage_offset(ts)) : nullptr;
+    const int S = a.split_owners;
+    const bool owner = (int)(threadIdx.x >> 5) < S;
+    const int64_t n = a.n;
+    int64_t obj[2];
+    bool live[2];
+    split_objects((int64_t)blockIdx.x * 32 * S + (owner ? threadIdx.x : 0), (int64_t)gridDim.x * 32 * S,
+        0, n, obj, live);
+    if (!owner)
+        live[0] = live[1] = false;
+    double r0[2][3], v0[2][3];
+    for (int k = 0; k < 2; ++k)
+        for (int j = 0; j < 3; ++j) {
+            r0[k][j] = a.r0[obj[k] * 3 + j];
+            v0[k][j] = a.v0[obj[k] * 3 + j];
+        }
+    for (int k = 0; k < 2; ++k) { // as startup_kernel: the call fails, the object still runs
+        if (!live[k])
+            continue;
+        bool usable = true;
+        for (int j = 0; j < 3; ++j)
+            usable = usable && isfinite(r0[k][j]) && isfinite(v0[k][j]);
+        if (r0[k][0] == 0.0 && r0[k][1] == 0.0 && r0[k][2] == 0.0)
+            usable = false;
+        if (!usable && a.err)
+            atomicOr(a.err, kErrBadInput);
+    }
+    StartupMats m[2];
+    const SplitForce2<MIXED, SPLIT> F { f, a, owner, live, obj, xsmem };
+    run_startup2(F, a.h, a.ncorr, r0, v0, m);
+    const bool fix_q3 = (a.flags & 2u) != 0;
+    double* st = a.state;
+    for (int k = 0; k < 2; ++k) {
+        if (!live[k])
+            continue;
+        const int64_t i = obj[k];
+        if (a.out27[0]) {
+            for (int c = 0; c < 9; ++c)
+                for (int j = 0; j < 3; ++j) {
+                    const int64_t o = i * 27 + c * 3 + j;
+                    a.out27[0][o] = m[k].r[c][j];
+                    a.out27[1][o] = m[k].v[c][j];
+                    a.out27[2][o] = m[k].a[c][j];
+                    a.out27[3][o] = m[k].s[c][j];
+                    a.out27[4][o] = m[k].S[c][j];
+                }
+        }
+        if (st) {
+            for (int j = 0; j < 3; ++j) {
+                st[(kR + j) * n + i] = m[k].r[8][j];
+                st[(kV + j) * n + i] = m[k].v[8][j];
+                st[(kSs + j) * n + i] = m[k].s[8][j];
+                st[(kSb + j) * n + i] = m[k].S[8][j];
+                for (int c = 0; c < 9; ++c)
+                    st[(kHist + c * 3 + j) * n + i] = m[k].a[c][j];
+                for (int q = 0; q < 4; ++q) {
+                    st[(kRep + q * 6 + j) * n + i] = m[k].r[5 + q][j];
+                    st[(kRep + q * 6 + 3 + j) * n + i] = m[k].v[5 + q][j];
+                    st[(kRepA + q * 3 + j) * n + i] = fix_q3 ? m[k].a[5 + q][j] : m[k].a[8][j];
+                }
+            }
+        }
+    }
+}
+
 // ---- GJ8 step with P lanes per group of K objects (few objects) ----
 // Same step as gj8_kernel; the P lanes of a group split the gravity columns of its K objects
 // (lanes.cuh, lane-layout table) and hold identical state; lane 0 of the group stores. Object k
@@ -887,10 +986,44 @@ template <class K> static cudaError_t set_smem(K kernel, size_t bytes)
     return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
+template <bool MIXED>
+static cudaError_t launch_startup_split(const TableSrc& ts, const PropArgs& a, int S, int num_sms,
+    cudaStream_t s)
+{
+    PropArgs b = a;
+    b.split_owners = S;
+    b.obj_lo = 0;
+    b.obj_hi = -1;
+    ForceGravity<MIXED> f {};
+    f.gen_m = a.gen_m;
+    f.prop_m = a.prop_m;
+    cudaError_t e;
+    const size_t xbytes = stage_offset(ts) + kSplitSmemBytes;
+    if (xbytes <= max_smem_optin()) { // the exchange in shared memory beside the table
+        if ((e = set_smem(startup_split_kernel<MIXED, kSplitSmem>, xbytes)) != cudaSuccess)
+            return e;
+        startup_split_kernel<MIXED, kSplitSmem><<<num_sms, kSplitBlock, xbytes, s>>>(f, ts, b);
+    } else {
+        const size_t bytes = table_smem_bytes(ts);
+        if ((e = set_smem(startup_split_kernel<MIXED, kSplitGlobal>, bytes)) != cudaSuccess)
+            return e;
+        startup_split_kernel<MIXED, kSplitGlobal><<<num_sms, kSplitBlock, bytes, s>>>(f, ts, b);
+    }
+    return cudaGetLastError();
+}
+
 cudaError_t launch_startup(const TableSrc& ts, const PropArgs& a, int num_sms, cudaStream_t s)
 {
     if (a.n <= 0)
         return cudaSuccess;
+    // the sizes whose GJ8 steps take the split block start in it too (the exchange may use the
+    // state arrays, so only when the state is there)
+    if (a.kind == 0 && a.state && !(ts.mixed && (a.flags & kFlagMixedCompensated))) {
+        const int S = split_owner_warps(a.n, num_sms, ts.L);
+        if (S > 0)
+            return ts.mixed ? launch_startup_split<true>(ts, a, S, num_sms, s)
+                            : launch_startup_split<false>(ts, a, S, num_sms, s);
+    }
     LaunchShape ls = pick_shape(a.n, 256, num_sms);
     if (a.kind == 0) {
         size_t smem = table_smem_bytes(ts);

@@ -75,6 +75,31 @@ def test_device_inputs_with_bad_states_fail_alone():
         ctx.close()
 
 
+def test_bad_state_fails_alone_in_the_split_block():
+    """At 40,000 objects the startup and the GJ8 steps run in the split block (5 owner warps per
+    SM): a bad state still fails the call, and every other object matches a clean run bit for
+    bit."""
+    import opengpop_b200 as G
+    from opengpop_b200 import orbits
+    n = 40000
+    assert G.split_block(n) == 5
+    r0, v0 = orbits.mixed_population(n, 6)
+    for precision in (G.FP64, G.MIXED):
+        ctx = G.Context(precision=precision)
+        rc, vc = dev(r0), dev(v0)
+        ctx.propagate_device(START, 30.0, 12, rc, vc)
+        rb = r0.copy()
+        rb[23456] = 0.0
+        rd, vd = dev(rb), dev(v0)
+        with pytest.raises(G.GpopError) as e:
+            ctx.propagate_device(START, 30.0, 12, rd, vd)
+        assert e.value.status == 1
+        keep = np.arange(n) != 23456
+        assert np.array_equal(host(rd)[keep], host(rc)[keep])
+        assert np.array_equal(host(vd)[keep], host(vc)[keep])
+        ctx.close()
+
+
 def test_poisoned_request_fails_alone_in_a_batch():
     import opengpop_b200 as G
     from opengpop_b200 import orbits
