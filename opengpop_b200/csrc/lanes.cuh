@@ -44,6 +44,37 @@ __device__ __forceinline__ void cmul(double ac, double as, double bc, double bs,
     rs = s;
 }
 
+#ifndef GPOP_LANE_PAIR_COLUMNS
+#define GPOP_LANE_PAIR_COLUMNS 1
+#endif
+constexpr bool kLanePairColumns = GPOP_LANE_PAIR_COLUMNS != 0;
+
+// Eq. 4-11 for column m of a lane walk, then the lane's cos/sin(m lambda) and q^m recursions step
+// P columns on (z^P; from column 0 the m - 1 values jump to z^(P-1)).
+template <int K>
+__device__ __forceinline__ void lane_combine(int m, const ColSums64<K>& s, const double (&CP)[K],
+    const double (&SP)[K], const double (&CPm1)[K], const double (&SPm1)[K], const double (&qP)[K],
+    double (&Cm)[K], double (&Sm)[K], double (&Cp)[K], double (&Sp)[K], double (&qm)[K],
+    double (&G)[K], double (&H)[K], double (&J)[K], double (&KK)[K])
+{
+    const double dm = (double)m;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        G[k] += Cm[k] * s.g1[k] + Sm[k] * s.g2[k];
+        J[k] += dm * (Cp[k] * s.j1[k] + Sp[k] * s.j2[k]);
+        KK[k] -= dm * (Sp[k] * s.j1[k] - Cp[k] * s.j2[k]);
+        H[k] += Cp[k] * s.h1[k] + Sp[k] * s.h2[k];
+        if (m == 0) {
+            Cp[k] = CPm1[k];
+            Sp[k] = SPm1[k];
+        } else {
+            cmul(Cp[k], Sp[k], CP[k], SP[k], Cp[k], Sp[k]);
+        }
+        cmul(Cm[k], Sm[k], CP[k], SP[k], Cm[k], Sm[k]);
+        qm[k] *= qP[k];
+    }
+}
+
 // (C1 + i S1)^p by binary powering (p >= 0).
 __device__ __forceinline__ void cpow(double c1, double s1, int p, double& rc, double& rs)
 {
@@ -63,8 +94,10 @@ __device__ __forceinline__ void cpow(double c1, double s1, int p, double& rc, do
 // object's group (lane l takes columns l, l + P, ...); the per-object totals are added across the
 // P lanes. As gravity_itrs in mixed mode: the head columns m <= 8 are combined in FP64 (their
 // terms of degree > 8 summed in FP32 per column), the columns m > 8 are walked, combined and
-// summed in FP32 and added to the FP64 totals once.
-template <bool MIXED, int K>
+// summed in FP32 and added to the FP64 totals once. PAIRS: FP64 lanes walk two of their columns
+// side by side (the one-object GJ8 lane kernel; kernels with fewer registers to spare keep one at a
+// time).
+template <bool MIXED, int K, bool PAIRS = false>
 __device__ __forceinline__ void gravity_itrs_lk(const GravSmem& gs, int l, int P, const double (&x)[K],
     const double (&y)[K], const double (&z)[K], double (&ax)[K], double (&ay)[K], double (&az)[K],
     unsigned mask)
@@ -132,6 +165,36 @@ __device__ __forceinline__ void gravity_itrs_lk(const GravSmem& gs, int l, int P
     // loads the walk's first table read depends on)
     int b64 = gs.cb64[l], b32 = gs.cb32[l];
     int m = l;
+    if constexpr (!MIXED && PAIRS && kLanePairColumns) {
+        // FP64: two of this lane's columns (m and m + P) side by side, so each object carries two
+        // independent recursions; each column's sums, and their combination, in the order of the
+        // one-column loop below (bit-identical accelerations)
+        for (; m + P <= Lhead; m += 2 * P) {
+            const int mb = m + P;
+            const int mn = mb + P < 127 ? mb + P : 127;
+            const int bb64 = gs.cb64[mb], nb64 = gs.cb64[mn];
+            ColSums64<K> sa, sb;
+            sa.zero();
+            sb.zero();
+            double Qa1[K], Qa2[K], Qb1[K], Qb2[K];
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                Qa1[k] = qm[k];
+                Qa2[k] = 0.0;
+                Qb1[k] = qm[k] * qP[k]; // the q^m the one-column loop carries into column m + P
+                Qb2[k] = 0.0;
+            }
+            const GravEntry64* ea = reinterpret_cast<const GravEntry64*>(reinterpret_cast<const uint4*>(gs.t64) + b64);
+            const GravEntry64* eb = reinterpret_cast<const GravEntry64*>(reinterpret_cast<const uint4*>(gs.t64) + bb64);
+            sa.add(ea, Qa1);
+            sb.add(eb, Qb1);
+            column64_pair<K>(ea + 1, eb + 1, Lhead - mb, u, w, Qa1, Qa2, sa, Qb1, Qb2, sb);
+            column64<K>(ea, Lhead - mb + 1, Lhead - m, u, w, Qa1, Qa2, sa);
+            lane_combine<K>(m, sa, CP, SP, CPm1, SPm1, qP, Cm, Sm, Cp, Sp, qm, G, H, J, KK);
+            lane_combine<K>(mb, sb, CP, SP, CPm1, SPm1, qP, Cm, Sm, Cp, Sp, qm, G, H, J, KK);
+            b64 = nb64;
+        }
+    }
     for (; m <= Lhead; m += P) {
         const int mn = m + P < 127 ? m + P : 127;
         const int nb64 = gs.cb64[mn], nb32 = gs.cb32[mn];
@@ -277,7 +340,7 @@ __device__ __forceinline__ void gravity_itrs_lanes(const GravSmem& gs, int l, in
 }
 
 // K objects: GCRS positions r[k] with the ITRS<-GCRS matrix M of gravity_gcrs.
-template <bool MIXED, int K>
+template <bool MIXED, int K, bool PAIRS = false>
 __device__ __forceinline__ void gravity_gcrs_lk(const GravSmem& gs, int l, int P, const double* __restrict__ M,
     const double (&r)[K][3], double (&a)[K][3], unsigned mask)
 {
@@ -292,7 +355,7 @@ __device__ __forceinline__ void gravity_gcrs_lk(const GravSmem& gs, int l, int P
         py[k] = m[3] * r[k][0] + m[4] * r[k][1] + m[5] * r[k][2];
         pz[k] = m[6] * r[k][0] + m[7] * r[k][1] + m[8] * r[k][2];
     }
-    gravity_itrs_lk<MIXED, K>(gs, l, P, px, py, pz, ax, ay, az, mask);
+    gravity_itrs_lk<MIXED, K, PAIRS>(gs, l, P, px, py, pz, ax, ay, az, mask);
 #pragma unroll
     for (int k = 0; k < K; ++k) {
         a[k][0] = m[0] * ax[k] + m[3] * ay[k] + m[6] * az[k];

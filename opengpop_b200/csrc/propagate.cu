@@ -798,7 +798,10 @@ __global__ void __launch_bounds__(MAXT, 1) gj8_lanes_kernel(TableSrc ts, PropArg
                 __syncwarp(mask); // the lead's stores precede the group's loads
             const double* M = a.prop_m + (size_t)(step + 4) * 9;
             for (int it = 0; it < a.ncorr; ++it) {
-                gravity_gcrs_lk<MIXED, K>(g, l, P, M, r, a8, mask);
+                // two columns at a time for one object per group at up to 384 threads a block (FP64
+                // 1,024 objects: 18.8 against 17.4 M object-steps/s); with two objects per group,
+                // or the 128 registers of 512-thread blocks, that spills (-9 %)
+                gravity_gcrs_lk<MIXED, K, K == 1 && MAXT <= 384>(g, l, P, M, r, a8, mask);
 #pragma unroll
                 for (int k = 0; k < K; ++k)
 #pragma unroll
