@@ -131,7 +131,7 @@ void gpop_propagator_destroy(gpop_propagator* p);
 /* No counterpart in the reference. gpop_propagate_device for callers that may not allocate device
  * memory while running (services that reserve their memory budget at start-up and forbid later
  * allocation; hosts whose device memory is held by another allocator's pool). The scratch lives in
- * one fixed device array of the library (about 4.1 MB on every GPU that loads it, until exit), so
+ * one fixed device array of the library (about 4.5 MB on every GPU that loads it, until exit), so
  * calls are limited to GPOP_NOALLOC_MAX_OBJECTS objects and GPOP_NOALLOC_MAX_STEPS steps; larger
  * requests return GPOP_ERR_INVALID_ARG. All calls share that array: calls that overlap on the GPU
  * race. Every call looks the array's device address up (cudaGetSymbolAddress, which allocates

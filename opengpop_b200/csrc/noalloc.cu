@@ -9,7 +9,7 @@
 // file-scope device array instead, so a call never allocates.
 //
 // Limits: at most GPOP_NOALLOC_MAX_OBJECTS objects and GPOP_NOALLOC_MAX_STEPS steps per call
-// (about 4.1 MB of device memory, held by every GPU that loads the library until the process
+// (about 4.5 MB of device memory, held by every GPU that loads the library until the process
 // exits). Every call shares the one array and finds the previous call's contents in it; calls that
 // overlap on the GPU (several streams, threads or contexts at once) race on it.
 //
