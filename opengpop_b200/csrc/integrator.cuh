@@ -139,14 +139,16 @@ __device__ void run_startup(const F& f, double h, int ncorr, const T* r0, const 
 // F2 provides gen2(r, v, step, k, a) and prop2(r, v, idx, a) over both objects at once
 // ([2][3] arrays); those may hold block-wide barriers, so every thread of a block makes the same
 // calls in the same order (the control flow below depends on no data). Per object the arithmetic
-// is that of rk8_step, corrector_correct and run_startup.
-template <class F2> __device__ void rk8_step2(const F2& f, double h, int step, StartupMats (&m)[2])
+// is that of rk8_step, corrector_correct and run_startup. A thread that carries no objects
+// (active false) makes the same force calls and skips the arithmetic around them.
+template <class F2>
+__device__ void rk8_step2(const F2& f, double h, int step, StartupMats (&m)[2], bool active)
 {
     const double hh = step > 0 ? h : -h;
     const int base = 4 + step + (step > 0 ? -1 : 1);
     double Kx[2][10][3], Kv[2][10][3];
-    double tx[2][3], tv[2][3];
-    for (int o = 0; o < 2; ++o)
+    double tx[2][3] = {}, tv[2][3] = {};
+    for (int o = 0; o < 2 && active; ++o)
         for (int j = 0; j < 3; ++j) {
             tx[o][j] = m[o].r[base][j];
             tv[o][j] = m[o].v[base][j];
@@ -155,12 +157,12 @@ template <class F2> __device__ void rk8_step2(const F2& f, double h, int step, S
     {
         double acc[2][3];
         f.gen2(tx, tv, step, 0, acc);
-        for (int o = 0; o < 2; ++o)
+        for (int o = 0; o < 2 && active; ++o)
             for (int j = 0; j < 3; ++j)
                 Kv[o][0][j] = acc[o][j];
     }
     for (int k = 1; k <= 9; ++k) {
-        for (int o = 0; o < 2; ++o)
+        for (int o = 0; o < 2 && active; ++o)
             for (int j = 0; j < 3; ++j) {
                 double sx = 0.0, sv = 0.0;
                 for (int i = 0; i < k; ++i) {
@@ -172,14 +174,14 @@ template <class F2> __device__ void rk8_step2(const F2& f, double h, int step, S
             }
         double acc[2][3];
         f.gen2(tx, tv, step, k, acc);
-        for (int o = 0; o < 2; ++o)
+        for (int o = 0; o < 2 && active; ++o)
             for (int j = 0; j < 3; ++j) {
                 Kv[o][k][j] = acc[o][j];
                 Kx[o][k][j] = tv[o][j];
             }
     }
     const int col = 4 + step;
-    for (int o = 0; o < 2; ++o)
+    for (int o = 0; o < 2 && active; ++o)
         for (int j = 0; j < 3; ++j) {
             double sx = 0.0, sv = 0.0;
             for (int k = 0; k < 10; ++k) {
@@ -191,28 +193,30 @@ template <class F2> __device__ void rk8_step2(const F2& f, double h, int step, S
         }
 }
 
-template <class F2> __device__ void corrector_accel2(const F2& f, StartupMats (&m)[2], bool epoch)
+template <class F2>
+__device__ void corrector_accel2(const F2& f, StartupMats (&m)[2], bool epoch, bool active)
 {
     for (int i = 0; i < 9; ++i) {
         if (i == 4 && !epoch)
             continue; // the same for every thread: no evaluation, no barrier
-        double r[2][3], v[2][3], acc[2][3];
-        for (int o = 0; o < 2; ++o)
+        double r[2][3] = {}, v[2][3] = {}, acc[2][3];
+        for (int o = 0; o < 2 && active; ++o)
             for (int j = 0; j < 3; ++j) {
                 r[o][j] = m[o].r[i][j];
                 v[o][j] = m[o].v[i][j];
             }
         f.prop2(r, v, i, acc);
-        for (int o = 0; o < 2; ++o)
+        for (int o = 0; o < 2 && active; ++o)
             for (int j = 0; j < 3; ++j)
                 m[o].a[i][j] = acc[o][j];
     }
 }
 
-template <class F2> __device__ void corrector_correct2(const F2& f, double h, StartupMats (&m)[2])
+template <class F2>
+__device__ void corrector_correct2(const F2& f, double h, StartupMats (&m)[2], bool active)
 {
     const double h2 = h * h;
-    for (int o = 0; o < 2; ++o) {
+    for (int o = 0; o < 2 && active; ++o) {
         corrector_s0(h, m[o]);
         corrector_all_s(m[o]);
         for (int c = 0; c < 9; ++c) {
@@ -229,14 +233,14 @@ template <class F2> __device__ void corrector_correct2(const F2& f, double h, St
             }
         }
     }
-    corrector_accel2(f, m, false);
+    corrector_accel2(f, m, false, active);
 }
 
 template <class F2>
 __device__ void run_startup2(const F2& f, double h, int ncorr, const double (&r0)[2][3],
-    const double (&v0)[2][3], StartupMats (&m)[2])
+    const double (&v0)[2][3], StartupMats (&m)[2], bool active)
 {
-    for (int o = 0; o < 2; ++o) {
+    for (int o = 0; o < 2 && active; ++o) {
         for (int c = 0; c < 9; ++c)
             for (int j = 0; j < 3; ++j)
                 m[o].r[c][j] = m[o].v[c][j] = m[o].a[c][j] = m[o].s[c][j] = m[o].S[c][j] = 0.0;
@@ -246,14 +250,14 @@ __device__ void run_startup2(const F2& f, double h, int ncorr, const double (&r0
         }
     }
     for (int i = 1; i <= 4; ++i) {
-        rk8_step2(f, h, i, m);
-        rk8_step2(f, h, -i, m);
+        rk8_step2(f, h, i, m, active);
+        rk8_step2(f, h, -i, m, active);
     }
     if (ncorr <= 0)
         return;
-    corrector_accel2(f, m, true);
+    corrector_accel2(f, m, true, active);
     for (int i = 0; i < ncorr; ++i)
-        corrector_correct2(f, h, m);
+        corrector_correct2(f, h, m, active);
 }
 
 } // namespace gpop

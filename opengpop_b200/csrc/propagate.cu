@@ -649,7 +649,7 @@ __global__ void __launch_bounds__(kSplitBlock, 1) startup_split_kernel(ForceGrav
     }
     StartupMats m[2];
     const SplitForce2<MIXED, SPLIT> F { f, a, owner, live, obj, xsmem };
-    run_startup2(F, a.h, a.ncorr, r0, v0, m);
+    run_startup2(F, a.h, a.ncorr, r0, v0, m, owner); // the walk-only warps skip the arithmetic
     const bool fix_q3 = (a.flags & 2u) != 0;
     double* st = a.state;
     for (int k = 0; k < 2; ++k) {
