@@ -136,3 +136,30 @@ def test_more_objects_than_one_wave(precision, oracle_data):
         ro, vo = O.propagate(oracle_data, "gravity", START, 30.0, steps, r[pick], v[pick])
         assert np.abs(rr[pick] - ro).max() < 1e-6, np.abs(rr[pick] - ro).max()
         assert np.abs(vv[pick] - vo).max() < 1e-9
+
+
+def test_split_block_trajectory():
+    """The trajectory outputs of the split block (positions, velocities and accelerations of
+    every step, [step][xyz][object]) match the plain two-object block's to rounding at 40,000
+    objects (5 owner warps per SM)."""
+    import torch
+    import opengpop_b200 as G
+    from opengpop_b200 import orbits
+    n, steps = 40000, 10
+    r0, v0 = orbits.mixed_population(n, seed=41)
+    out = {}
+    for walk in (5, 2):
+        os.environ["GPOP_WALK_MODE"] = str(walk)
+        try:
+            c = G.Context(precision=G.FP64)
+        finally:
+            del os.environ["GPOP_WALK_MODE"]
+        r = torch.tensor(r0, dtype=torch.float64, device="cuda")
+        v = torch.tensor(v0, dtype=torch.float64, device="cuda")
+        tr, tv, ta = (torch.zeros(steps, 3, n, dtype=torch.float64, device="cuda") for _ in range(3))
+        c.propagate_trajectory(START, 30.0, steps, r, v, tr, tv, ta)
+        torch.cuda.synchronize()
+        out[walk] = [t.cpu().numpy() for t in (tr, tv, ta)]
+        c.close()
+    for a, b, tol in zip(out[5], out[2], (1e-6, 1e-9, 1e-12)):
+        assert np.isfinite(b).all() and np.abs(a - b).max() < tol, np.abs(a - b).max()
