@@ -163,3 +163,45 @@ def test_split_block_trajectory():
         c.close()
     for a, b, tol in zip(out[5], out[2], (1e-6, 1e-9, 1e-12)):
         assert np.isfinite(b).all() and np.abs(a - b).max() < tol, np.abs(a - b).max()
+
+
+def test_trajectory_over_more_than_one_wave():
+    """80,000 FP64 objects (one wave of 75,776 at two objects per thread, then 4,224 in lanes per
+    group of two objects): every step's trajectory row matches the plain two-object block over all
+    objects to rounding."""
+    import torch
+    import opengpop_b200 as G
+    from opengpop_b200 import orbits
+    n, steps = 80000, 8
+    r0, v0 = orbits.mixed_population(n, seed=43)
+    out = {}
+    for walk in (5, 0):
+        os.environ["GPOP_WALK_MODE"] = str(walk)
+        try:
+            c = G.Context(precision=G.FP64)
+        finally:
+            del os.environ["GPOP_WALK_MODE"]
+        r = torch.tensor(r0, dtype=torch.float64, device="cuda")
+        v = torch.tensor(v0, dtype=torch.float64, device="cuda")
+        tr = torch.zeros(steps, 3, n, dtype=torch.float64, device="cuda")
+        c.propagate_trajectory(START, 30.0, steps, r, v, tr)
+        torch.cuda.synchronize()
+        out[walk] = tr.cpu().numpy()
+        c.close()
+    assert np.isfinite(out[0]).all() and np.abs(out[0] - out[5]).max() < 1e-6
+
+
+def test_compensated_sums_at_split_sizes():
+    """The compensated mixed walk has no split-block form: at 40,000 objects it runs the plain
+    block and agrees with the default mixed walk (split block) within the FP32 rounding of the
+    degree > 8 sums."""
+    import opengpop_b200 as G
+    from opengpop_b200 import orbits
+    r0, v0 = orbits.mixed_population(40000, seed=44)
+    ref = G.Context(precision=G.MIXED)
+    rr, vr = ref.propagate(START, 30.0, 12, r0, v0)
+    ref.close()
+    comp = G.Context(precision=G.MIXED, flags=G.MIXED_COMPENSATED)
+    rc, vc = comp.propagate(START, 30.0, 12, r0, v0)
+    comp.close()
+    assert np.abs(rc - rr).max() < 1e-3 and np.abs(vc - vr).max() < 1e-6
