@@ -83,3 +83,21 @@ def test_walk_policy_rejects_bad_arguments():
     for args in ((0, SMS, G.FP64), (10, 0, G.FP64), (10, SMS, 7)):
         with pytest.raises(G.GpopError):
             G.walk_policy(*args)
+
+
+@pytest.mark.parametrize("sms", [1, 7, 132, 148, 160])
+def test_policy_invariants_for_any_sm_count(sms):
+    # whatever the GPU: a split block holds every object of its launch in its owner warps, lane
+    # groups have a power-of-two lane count, and the first lane-pair launch fits one wave
+    import opengpop_b200 as G
+    for prec in (G.FP64, G.MIXED):
+        for n in list(range(1, 4000, 13)) + list(range(4000, sms * 700, max(1, sms * 3))):
+            w, P = G.walk_policy(n, sms, prec)
+            assert w in (1, 2, 3, 4) and P >= 1 and P & (P - 1) == 0 and P <= 32
+            S = G.split_block(n, sms)
+            assert S == 0 or 5 <= S <= 7
+            if S:
+                assert 2 * sms * 32 * S >= n
+            if w == 4:
+                main = min(n, sms * 256 // P * 2)
+                assert -(-main // 2) * P <= sms * 256
